@@ -1,0 +1,387 @@
+"""Benchmark: ns/day of the 64 000-ion LJ + PME melt on B200 (one process per GPU).
+
+Workload (plain form): 32 000 Na+ / 32 000 Cl- ions at 0.0375 per cubic Angstrom
+(L = 119.5 A), LJ eps = 0.01 eV, sigma = 2.8 A, r_c = 9 A; SPME r_c = 9 A,
+erfc(alpha r_c) = 1e-5, mesh spacing 1 A (120^3), order 5; FP32 forces;
+velocity-Verlet NVE at dt = 1 fs from a 1200 K Maxwell-Boltzmann start.
+Inputs are seeded synthetic (no dataset exists for this path).
+
+One step = one captured CUDA-graph replay of the full MD step (kick + drift,
+device list decision, conditional build / prune, pair pass beside the mesh
+transform, gather + scatter + kick).  Each timed step is bracketed by CUDA
+events on the launching stream and preceded by an L2 flush (a 256 MiB write);
+the timed region is bracketed by a barrier and device synchronisation, and the
+max over ranks is reported.  With several GPUs every rank runs its own replica
+(the system does not shard; no collective in the step).
+
+--impl reference times the CPU restatement of the same step (the reference has
+no CPU force path) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "ns/day @64k-ion LJ+PME: learned-coarse vs plain, equal force error, 1 B200"
+N_IONS = 64000
+RHO = 0.0375
+RC = 9.0
+DT_FS = 1.0
+T_INIT = 1200.0
+BUFFER, PRUNE = 1.0, 0.3
+SEED = 2026
+
+
+def ns_per_day(ms_per_step: float, dt_fs: float = DT_FS) -> float:
+    return (1000.0 / ms_per_step) * dt_fs * 86400.0 * 1e-6
+
+
+def make_system(pd):
+    L = (N_IONS / RHO) ** (1.0 / 3.0)
+    pos, q, box = pd.synthetic.ionic_melt(N_IONS, L, 2.2, seed=SEED)
+    m = pd.synthetic.melt_masses(q)
+    v = pd.synthetic.maxwell_boltzmann(m, T_INIT, seed=SEED + 1, kB=pd.synthetic.KB_EV)
+    return pos, q, m, v, box
+
+
+def forces(pd):
+    lj = pd.LennardJones(epsilon=0.01, sigma=2.8, cutoff=RC, pairs="neighborlist",
+                         neighborlist=pd.ClusterPairList(buffer=BUFFER, prune_buffer=PRUNE))
+    el = pd.PME(coulomb_prefactor=pd.synthetic.COULOMB_EV_A, real_cutoff=RC, real_space_tolerance=1e-5,
+                mesh_spacing=1.0, order=5)
+    return [lj, el]
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            import tempfile
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        for line in open(self.path):
+            p = [s.strip() for s in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                rows.append((float(p[1]), float(p[2]), float(p[3]) if p[3] not in ("[N/A]", "") else 0.0, p[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[3][k].lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": reasons}
+
+
+def dist_setup():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, v: float) -> float:
+    if world <= 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def time_pairs_kernel(pd, st, reps=50):
+    """Pair pass alone (same stream, warm): average launch time and the algorithmic work per launch."""
+    import torch
+    s = st.stream
+    eng = st.cluster
+    with torch.cuda.stream(s):
+        for _ in range(3):
+            eng.pairs(energy=False, stream=s)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        for _ in range(reps):
+            eng.pairs(energy=False, stream=s)
+        b.record(s)
+    b.synchronize()
+    ms = a.elapsed_time(b) / reps
+    # clear the accumulated slot forces (a kick-free evaluation restores the state)
+    st.evaluate_forces_into_f(False)
+    return ms
+
+
+def pair_count(pos, box, rc):
+    """Pairs inside r_c (Newton-3, counted once) from a cell grid on the host."""
+    L = np.asarray(box, float)
+    n = len(pos)
+    nc = np.maximum((L // rc).astype(int), 3)
+    cell = np.floor((pos / L + 0.5) % 1.0 * nc).astype(int) % nc
+    cid = cell[:, 0] + nc[0] * (cell[:, 1] + nc[1] * cell[:, 2])
+    order = np.argsort(cid, kind="stable")
+    starts = np.searchsorted(cid[order], np.arange(nc.prod() + 1))
+    total = 0
+    for c in range(nc.prod()):
+        ia = order[starts[c]:starts[c + 1]]
+        if len(ia) == 0:
+            continue
+        cx, cy, cz = c % nc[0], (c // nc[0]) % nc[1], c // (nc[0] * nc[1])
+        nb = []
+        for dz in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dx in (-1, 0, 1):
+                    cc = ((cx + dx) % nc[0]) + nc[0] * (((cy + dy) % nc[1]) + nc[1] * ((cz + dz) % nc[2]))
+                    nb.append(order[starts[cc]:starts[cc + 1]])
+        jb = np.concatenate(nb)
+        d = pos[ia][:, None, :] - pos[jb][None, :, :]
+        d -= L * np.round(d / L)
+        r2 = (d * d).sum(-1)
+        total += int(((r2 < rc * rc) & (r2 > 0)).sum())
+    return total // 2
+
+
+def cpu_baseline_run(pd, ora, steps_budget_s=15.0, max_steps=None):
+    """The CPU restatement of the step (FP64, all host cores): ms per step on a bounded number of steps."""
+    pos, q, m, v, box = make_system(pd)
+    alpha = pd.splits.alpha_from_tolerance(RC, 1e-5)
+    K = pd.splits.resolve_mesh(None, 1.0, box, 5)
+    cpu = ora.CpuMelt(pos, v, q, m, box, C=pd.synthetic.COULOMB_EV_A, alpha=alpha, rc=RC, K=K, P=5,
+                      lj=dict(sigma=2.8, eps=0.01, rc=RC), workers=-1)
+    dt = DT_FS / pd.synthetic.TIME_UNIT_FS
+    t0 = time.perf_counter()
+    cpu.step(dt)   # warm-up step
+    first = time.perf_counter() - t0
+    nsteps = max(1, int(steps_budget_s / max(first, 1e-3)))
+    if max_steps is not None:
+        nsteps = max(1, min(nsteps, max_steps))
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        cpu.step(dt)
+    el = time.perf_counter() - t0
+    ms = 1000.0 * el / nsteps
+    return ms, nsteps, os.cpu_count()
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the CPU restatement on the host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    import __graft_entry__ as ge
+    pd = ge.load_package()
+    ora = ge.load_oracle()
+    budget = 120.0
+    pos, q, m, v, box = make_system(pd)
+    alpha = pd.splits.alpha_from_tolerance(RC, 1e-5)
+    K = pd.splits.resolve_mesh(None, 1.0, box, 5)
+    cpu = ora.CpuMelt(pos, v, q, m, box, C=pd.synthetic.COULOMB_EV_A, alpha=alpha, rc=RC, K=K, P=5,
+                      lj=dict(sigma=2.8, eps=0.01, rc=RC), workers=-1)
+    dt = DT_FS / pd.synthetic.TIME_UNIT_FS
+    t0 = time.perf_counter()
+    for _ in range(max(1, min(args.warmup, 2))):
+        cpu.step(dt)
+    per = (time.perf_counter() - t0) / max(1, min(args.warmup, 2))
+    steps = max(1, min(args.steps, int(budget / max(per, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        cpu.step(dt)
+    ms = 1000.0 * (time.perf_counter() - t0) / steps
+    val = ns_per_day(ms)
+    cores = os.cpu_count()
+    out = {"impl": "reference", "metric": METRIC, "value": val, "unit": "ns/day", "n_gpus": args.gpus,
+           "steps": steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded ionic melt)",
+           "config": {"workload": "ionic melt N=64000 LJ+SPME 120^3 order 5, NVE dt=1 fs", "form": "plain"},
+           "cpu_baseline": {"value": val, "unit": "ns/day", "cores": cores, "kind": "port",
+                            "sample": f"{steps} full MD steps of the 64k-ion melt on the CPU restatement "
+                                      f"(requested {args.steps}; capped to ~{int(budget)} s)"},
+           "e2e": {"value": val, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="pdb200", choices=["pdb200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-flush", action="store_true", help="(diagnostic) do not flush L2 between steps")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+    import __graft_entry__ as ge
+    pd = ge.load_package()
+    pd.build()
+    L = pd._native.lib()
+    pos, q, m, v, box = make_system(pd)
+    system = pd.ParticleSystem(pos, box, types=["Na", "Cl"], typeids=np.where(q > 0, 1, 2), masses=m, charges=q,
+                               velocities=v)
+    dt = DT_FS / pd.synthetic.TIME_UNIT_FS
+    sim = pd.Simulation(system, pd.Integrator(dt=dt, forces=forces(pd)))
+    st = sim.state
+    s = st.stream
+    pd.evaluate_forces_into_f(sim, energy=False)
+    # kernels one step launches (eager launch count of the same sequence the graph holds)
+    c0 = L.pd_launch_count()
+    st.step(1, use_graph=False)
+    st.synchronize()
+    kernels_per_step = int(L.pd_launch_count() - c0)
+    # warm-up (graph capture on the first replay)
+    st.step(args.warmup, use_graph=True)
+    st.synchronize()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(s):
+            for k in range(args.steps):
+                if not args.no_flush:
+                    flush.fill_(float(k))
+                starts[k].record(s)
+                st.engine.step(1, dt, energy_last=False, use_graph=True, stream=s)
+                ends[k].record(s)
+        torch.cuda.synchronize()
+    barrier(world)
+    total_ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
+    total_ms = max_over_ranks(world, total_ms)
+    ms_step = total_ms / args.steps
+    value = world * ns_per_day(ms_step)
+    stats = st.cluster.statistics()
+    if stats["error"]:
+        raise RuntimeError(f"cluster list error {stats['error']} during the run")
+    clocks = clk.summary()
+
+    # end to end through the C ABI with pinned host buffers (H2D state in, D2H state and energy out per step)
+    n = st.n
+    hx = torch.empty(3 * n, dtype=torch.float32, pin_memory=True).numpy()
+    hv = torch.empty(3 * n, dtype=torch.float32, pin_memory=True).numpy()
+    hx[:] = torch.cat([st.x, st.y, st.z]).cpu().numpy()
+    hv[:] = torch.cat([st.vx, st.vy, st.vz]).cpu().numpy()
+    e2e_steps = max(20, args.steps // 4)
+    for _ in range(3):
+        st.engine.step_host(hx, hv, 1, dt, stream=s)
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        st.engine.step_host(hx, hv, 1, dt, stream=s)
+    e2e_ms = 1000.0 * (time.perf_counter() - t0) / e2e_steps
+    e2e_ms = max_over_ranks(world, e2e_ms)
+
+    # roofline of the dominant kernel: the fused pair pass (FP32 pipe)
+    pair_ms = time_pairs_kernel(pd, st)
+    npairs = pair_count(st.positions(), box, RC)
+    nf = len(st.solver.coulomb_polynomial().pf)
+    flop_pair = 20 + 16 * 0 + (2 * (nf - 1) + 8)
+    flops = npairs * flop_pair
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    nsm = torch.cuda.get_device_properties(0).multi_processor_count
+    fp32_peak = nsm * 128 * 2 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12   # TFLOP/s (no measured FP32 figure)
+    achieved = flops / (pair_ms * 1e-3) / 1e12
+    roofline = {"kernel": "k_pairs<LJ uniform, Coulomb polynomial, force only>", "bound": "fp32",
+                "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                "traffic": None, "per_launch_ms": pair_ms, "pairs_within_rc": npairs, "flop_per_pair": flop_pair,
+                "peak_source": "nominal FP32 FMA rate at sm_max_mhz (MEASURED_PEAKS.json has no FP32 figure)"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        ora = ge.load_oracle()
+        cms, csteps, cores = cpu_baseline_run(pd, ora)
+        cpu = {"value": ns_per_day(cms), "unit": "ns/day", "cores": cores, "kind": "port",
+               "sample": f"{csteps} full MD steps of the same 64k-ion melt on the FP64 CPU restatement "
+                         f"(OpenMP pair sums, threaded FFT)"}
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ionic melt, 1200 K start)",
+               "config": {"workload": "ionic melt N=64000 (L=119.5 A) LJ+SPME r_c=9 A, 120^3 order 5, NVE dt=1 fs",
+                          "form": "plain (learned coarse-mesh form not built)", "parallelism": f"replicas x{world}",
+                          "list_buffer_A": BUFFER, "prune_buffer_A": PRUNE,
+                          "l2": "flushed (256 MiB write) before every timed step" if not args.no_flush else "warm",
+                          "builds": stats["builds"], "prunes": stats["prunes"]},
+               "roofline": roofline, "cpu_baseline": cpu,
+               "e2e": {"value": world * ns_per_day(e2e_ms), "unit": "ns/day", "h2d_bytes_per_step": 24 * n,
+                       "d2h_bytes_per_step": 24 * n + 8, "ms_per_step": e2e_ms},
+               "gpu_launches": kernels_per_step * args.steps, "kernels_per_step": kernels_per_step,
+               "clocks": clocks}
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,260 @@
+/*
+ * pdb200.h — C ABI of libpdb200.so, the B200 (sm_100a) implementation of the
+ * per-step force hot path of ParticleDynamics.jl.
+ *
+ * The ABI is what the reference's Julia host code would `ccall` in place of
+ * the bodies of its hot-path kernels.  Every entry point takes plain pointers
+ * (caller arrays are DEVICE pointers unless stated otherwise), sizes and a
+ * CUDA stream, and returns an int status (PD_OK = 0).  No C++ or torch types
+ * cross the boundary.  Handles are not thread-safe: use one handle per stream.
+ *
+ * Reference paths below are relative to the ParticleDynamics.jl project root.
+ *
+ * Ownership follows the reference (src/electrostatics/Solver.jl:68-74,
+ * src/clusterpairs/List.jl:18-27): the caller owns the particle arrays
+ * (structure-of-arrays float32 x, y, z, q, forces, energies) and passes them
+ * on every call; the library owns its workspaces, allocates them only in the
+ * *_create / *_setup / *_grow / *_set_box calls, and never allocates, frees or
+ * synchronises inside the enqueue calls, so enqueue calls can be captured in a
+ * CUDA graph.
+ *
+ * Errors: host argument errors return PD_EINVAL with a message available from
+ * pd_last_error().  In-stream failures (outer-list capacity, non-finite
+ * coordinates) latch a device error word inside the handle; every later list
+ * and pair kernel of that handle then does nothing (as the reference's
+ * counts[CL_ERR], src/clusterpairs/List.jl:25-27, Kernels.jl:51) until the
+ * host reads the status at a boundary (pd_cluster_status) and grows the list
+ * (pd_cluster_grow).  No kernel traps.
+ */
+#ifndef PDB200_H
+#define PDB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* A cudaStream_t passed as an opaque pointer (NULL = the legacy default stream). */
+typedef void *pd_stream_t;
+
+enum pd_status_code {
+    PD_OK = 0,
+    PD_EINVAL = 1,      /* bad argument (ArgumentError in the reference) */
+    PD_ENOMEM = 2,      /* device allocation failed */
+    PD_ECAPACITY = 3,   /* outer cluster list overflowed; pd_cluster_grow, then rebuild */
+    PD_ENONFINITE = 4,  /* non-finite coordinates met by a list build */
+    PD_ECUFFT = 5,      /* a cuFFT call failed */
+    PD_ECUDA = 6,       /* a CUDA runtime call failed */
+    PD_ESTATE = 7,      /* call out of order (e.g. pairs before any build) */
+    PD_ENOTSUP = 8      /* valid request this build does not support */
+};
+
+/* Library version (major*10000 + minor*100 + patch). */
+int pd_version(void);
+/* Static text for a status code. */
+const char *pd_strerror(int code);
+/* Message of the last failure on the calling thread ("" if none). */
+const char *pd_last_error(void);
+/* Number of kernel launches this library has issued on the calling process. */
+uint64_t pd_launch_count(void);
+
+/* ======================================================================
+ * Cluster-pair engine: ClusterPairEngine + ClusterPairList
+ * (src/clusterpairs/Engine.jl:15-97, src/clusterpairs/List.jl:112-179).
+ *
+ * Particles are clustered into x-y columns of about one super-cluster edge,
+ * sorted by z, cut into super-clusters of 64 and split 2x2x2 into clusters of
+ * up to 8.  The outer list holds, per super-cluster, the j-clusters
+ * (index >= the i-cluster's) whose bounding-box gap is below r_list = rmax +
+ * skin; pruning keeps the 8x8 tiles with a pair inside rmax + prune_buffer.
+ * ====================================================================== */
+typedef struct pd_cluster pd_cluster;
+
+enum pd_lj_kind {
+    PD_LJ_NONE = 0,     /* no van der Waals term */
+    PD_LJ_UNIFORM = 1,  /* one (c6, c12, rc2, esh) for every pair */
+    PD_LJ_TABLE = 2     /* per type-pair table, ntypes <= 16 (LJ_TABLE_SHARED) */
+};
+
+#define PD_MAX_POLY 32
+#define PD_MAX_TYPES 16
+
+typedef struct {
+    int n;                  /* particles */
+    double rmax;            /* largest interaction cutoff */
+    double skin;            /* list buffer: r_list = rmax + skin */
+    double prune_buffer;    /* r_prune = rmax + prune_buffer, 0 <= prune_buffer <= skin */
+    /* Lennard-Jones, pair_force() of src/clusterpairs/PairFunctor.jl:127-156:
+     * f = (12 c12 ir6 - 6 c6) ir6 ir2 and e = (c12 ir6 - c6) ir6 - esh inside rc2. */
+    int lj_kind;
+    float lj_c6, lj_c12, lj_rc2, lj_esh;      /* PD_LJ_UNIFORM */
+    int ntypes;                               /* PD_LJ_TABLE: type ids 1..ntypes */
+    float lj_table[PD_MAX_TYPES * PD_MAX_TYPES * 4]; /* row-major (c6, c12, rc2, esh), lj_type_table() PairFunctor.jl:166-179 */
+    /* Real-space Coulomb as CoulombPolynomial (PairFunctor.jl:21-29): inside rc2,
+     * f/r = C qq (1/r^3 - P_f(x)), e = C qq (1/r + P_e(x) - eshift), x = r^2 sx - 1.
+     * Monomial coefficients, constant term first (horner(), PairFunctor.jl:104-110). */
+    int coulomb;
+    float coul_C, coul_rc2, coul_sx, coul_eshift;
+    int coul_has_mesh;
+    int coul_ne, coul_nf;
+    float coul_pe[PD_MAX_POLY], coul_pf[PD_MAX_POLY];
+    float selfc;            /* self coefficient: the scatter subtracts 0.5*C*selfc*q^2 */
+    /* fixed list intervals (nstlist, nstprune) instead of displacement triggers; 0 = triggers
+     * (_decide_kernel!, src/clusterpairs/Engine.jl:301-324) */
+    int nstlist, nstprune;
+} pd_cluster_params;
+
+typedef struct {
+    int superclusters;      /* counts[CL_NS] */
+    int outer_entries;      /* counts[CL_NE] */
+    int working_entries;    /* entries of the pruned list */
+    int error;              /* 0, PD_ECAPACITY or PD_ENONFINITE */
+    int required;           /* outer entries needed after PD_ECAPACITY (counts[CL_REQ]) */
+    int capacity;           /* outer-entry capacity (necap) */
+    int builds, prunes;     /* device-decided totals (CL_NBUILD, CL_NPRUNE) */
+    int nsmax, nslot;       /* super-cluster bound and slot count of this geometry */
+    int last_build, last_prune; /* decision flags of the last pd_cluster_decide */
+    long long tile_bits;    /* live (i-atom, j-half) tile bits of the working list */
+} pd_cluster_stats;
+
+/* ClusterPairEngine(T, N, box; ...) + setup! (Engine.jl:54-97, 130-139).  Copies *p. */
+int pd_cluster_create(pd_cluster **out, const pd_cluster_params *p, const double box[3]);
+int pd_cluster_destroy(pd_cluster *c);
+/* setup!(list, box, rlist, npmax) (List.jl:874-937): size every buffer for this box and
+ * request a build.  Host boundary: may reallocate (captured graphs must be recaptured). */
+int pd_cluster_setup(pd_cluster *c, const double box[3]);
+/* ensure_capacity!(list) (List.jl:959-969): after PD_ECAPACITY grow the outer-entry storage to
+ * 1.5x (first growth) or 1.25x the required entries plus 1024, and request a build. */
+int pd_cluster_grow(pd_cluster *c);
+/* request_build!(list) (List.jl:1077): the next decision rebuilds. */
+int pd_cluster_request_build(pd_cluster *c, pd_stream_t s);
+/* enqueue_decide! (Engine.jl:328-335): displacement maxima since the last build/prune and the
+ * device decision (build, prune) written to the handle's device flags.  fixed = 1 follows
+ * nstlist/nstprune when they are set. */
+int pd_cluster_decide(pd_cluster *c, const float *x, const float *y, const float *z, int fixed, pd_stream_t s);
+/* build!(list, rx, ry, rz) (List.jl:979-1051) followed by the pack of the force coordinates
+ * (_pack!, Engine.jl:117-127) and the first pruning pass.  q and type may be NULL.
+ * conditional = 1: every kernel of the build runs only when the device build flag is set
+ * (the CL_BUILD conditional graph body of ClusterBackend.jl:110-143). */
+int pd_cluster_build(pd_cluster *c, const float *x, const float *y, const float *z,
+                     const float *q, const int *type, int conditional, pd_stream_t s);
+/* _pack! (Engine.jl:117-127): cluster-ordered force coordinates (centred image) and charges. */
+int pd_cluster_pack(pd_cluster *c, const float *x, const float *y, const float *z,
+                    const float *q, const int *type, pd_stream_t s);
+/* enqueue_prune! (Engine.jl:353-364): distance-only pruning of the outer list to the prune
+ * radius (_prune_only_kernel!, Kernels.jl:349-394) and compaction into the working list.
+ * conditional = 1: only when the device prune flag is set. */
+int pd_cluster_prune(pd_cluster *c, const float *x, const float *y, const float *z, int conditional, pd_stream_t s);
+/* enqueue_pairs!(eng, energy, Val(false)) (Engine.jl:213-223): fused LJ + Coulomb pass over the
+ * working list (_cluster_pair_kernel!, Kernels.jl:38-202) into the slot accumulators. */
+int pd_cluster_pairs(pd_cluster *c, int energy, pd_stream_t s);
+/* enqueue_scatter! (Engine.jl:227-257, _scatter_kernel! Kernels.jl:207-240): slot accumulators to
+ * storage order, minus the Coulomb self energy, then zero the accumulators.  add = 1 adds to
+ * fx/fy/fz/epot (a mesh gather in set mode ran first); vir6 is N x 6 row-major
+ * (xx, yy, zz, xy, xz, yz) and is always overwritten.  q may be NULL (uncharged). */
+int pd_cluster_scatter(pd_cluster *c, float *fx, float *fy, float *fz, float *epot, float *vir6,
+                       const float *q, int energy, int add, pd_stream_t s);
+/* compute!(eng, ...) (Engine.jl:185-190): eager update_list! + pairs + scatter.  Reads the
+ * device counts on the host after a build and grows/rebuilds on overflow (not capturable). */
+int pd_cluster_compute(pd_cluster *c, const float *x, const float *y, const float *z,
+                       const float *q, const int *type, float *fx, float *fy, float *fz,
+                       float *epot, float *vir6, int energy, pd_stream_t s);
+/* statistics(eng) (Engine.jl:402-412): host read of the device counts (synchronises s). */
+int pd_cluster_status(pd_cluster *c, pd_cluster_stats *out, pd_stream_t s);
+/* mesh_order(eng) (Engine.jl:394): device pointer to the particles in slot order (n entries). */
+const int *pd_cluster_order(pd_cluster *c);
+/* Device pointers into the list for tests: perm (nslot, -1 = padding), packed xyzq (nslot x 4),
+ * outer offsets (nsmax + 1), outer entries ((cj << 8) | i-cluster mask), working entries
+ * (cj, two 8-bit warp masks in bits 0-15 of the second word), working counts (nsmax). */
+int pd_cluster_buffers(pd_cluster *c, const int **perm, const float **xq, const int **scio,
+                       const uint32_t **cjo, const uint32_t **cjw, const int **nw);
+
+/* ======================================================================
+ * Mesh engine: ElectrostaticsSolver / MeshWorkspace (src/electrostatics/Solver.jl:17-158)
+ * for SPME (B-spline window, exact deconvolution) and P3M with the optimal influence
+ * function for analytic (AD) or ik differentiation.  cuFFT does the transforms.
+ * ====================================================================== */
+typedef struct pd_mesh pd_mesh;
+
+enum pd_mesh_kind { PD_MESH_SPME = 1, PD_MESH_P3M_AD = 2, PD_MESH_P3M_IK = 3 };
+
+typedef struct {
+    int kind;               /* pd_mesh_kind (influence :spme, :p3m_ad, :p3m_ik, Spec.jl:5) */
+    int order;              /* B-spline order P, 3..12 (BSplineWindow, Windows.jl:18-24) */
+    int alias_order;        /* P3M alias sums |n| <= alias_order, 0..6 */
+    int mesh[3];            /* K1, K2, K3 (resolve_mesh, Spec.jl:141-146) */
+    double alpha;           /* Gaussian split parameter */
+    double C;               /* coulomb_prefactor / relative_permittivity */
+    int background;         /* net_charge = :background (Solver.jl:179-185) */
+    double qtotal;          /* total charge (background term) */
+    int nmax;               /* largest particle count passed to pd_mesh_transform / pd_mesh_gather */
+} pd_mesh_params;
+
+int pd_mesh_create(pd_mesh **out, const pd_mesh_params *p, const double box[3]);
+int pd_mesh_destroy(pd_mesh *m);
+/* refresh_geometry!(solver, box) (Solver.jl:193-209): FP64 influence function and virial
+ * coefficients on the device for a new box (compute_influence!, Influence.jl:190-227). */
+int pd_mesh_set_box(pd_mesh *m, const double box[3]);
+/* mesh_transform!(solver, rx, ry, rz, q, energy, order) (Solver.jl:305-339): spread the n
+ * particles order[0..n) (0-based ids; NULL = identity), forward R2C, influence multiply with the
+ * FP64 mesh energy/virial reduction, inverse C2R (ik: three field transforms). */
+int pd_mesh_transform(pd_mesh *m, const float *x, const float *y, const float *z, const float *q,
+                      const int *order, int n, int energy, pd_stream_t s);
+/* mesh_gather!(solver, ..., energy, order; set) (Solver.jl:360-378): reciprocal forces (and
+ * energies 0.5 q phi + bg q) of the particles of order, added (set = 0) or stored (set = 1, AD
+ * only); with energy, vglobal6 (device, 6 floats) receives the mesh virial plus background. */
+int pd_mesh_gather(pd_mesh *m, const float *x, const float *y, const float *z, const float *q,
+                   const int *order, int n, float *fx, float *fy, float *fz, float *epot,
+                   float *vglobal6, int energy, int set, pd_stream_t s);
+/* Host read of the FP64 accumulator acc[0..7): mesh energy and the six virial sums. */
+int pd_mesh_energy(pd_mesh *m, double out7[7], pd_stream_t s);
+/* Copies of the FP32 influence function (nmodes) and virial coefficients (6 x nmodes) to host
+ * memory; either pointer may be NULL.  nmodes = (K1/2+1)*K2*K3. */
+int pd_mesh_influence(pd_mesh *m, float *G, float *Vc);
+/* Mesh dimensions and mode count. */
+int pd_mesh_dims(pd_mesh *m, int mesh[3], int *nmodes);
+
+/* ======================================================================
+ * Device step engine: the captured per-step graph of the reference's device engine
+ * (cluster_step_parts, src/engine/ClusterBackend.jl:90-220): kick + drift (+ list decision),
+ * conditional build and prune, the pair pass in parallel with the mesh transform, then the
+ * gather fused with the slot scatter and the closing half kick.
+ * ====================================================================== */
+typedef struct pd_md pd_md;
+
+typedef struct {
+    int n;
+    float *x, *y, *z;          /* positions (centred image, wrapped into [-L/2, L/2) by the drift) */
+    float *vx, *vy, *vz;
+    float *fx, *fy, *fz;       /* forces of the current positions */
+    const float *q;            /* charges or NULL */
+    const int *type;           /* type ids 1..ntypes or NULL */
+    const float *inv_mass;     /* per particle 1/m (device) or NULL: use inv_mass_uniform */
+    float inv_mass_uniform;
+    float *epot;               /* per-particle potential energy (energy steps) */
+    float *vir6;               /* per-particle pair virial, N x 6 (energy steps) */
+    float *vglobal6;           /* mesh virial (energy steps), 6 floats */
+} pd_md_state;
+
+/* The engine borrows c, m (may be NULL) and the state arrays for its lifetime. */
+int pd_md_create(pd_md **out, pd_cluster *c, pd_mesh *m, const pd_md_state *st, double box[3]);
+int pd_md_destroy(pd_md *md);
+/* evaluate_forces_into_f!(st, energy) (src/simulation/ForceEvaluation.jl:40-44): forces (and
+ * energies, virials) of the current positions; the list is kept valid (host boundary). */
+int pd_md_evaluate(pd_md *md, int energy, pd_stream_t s);
+/* nsteps velocity-Verlet NVE steps (NVEFusion.jl:3-27, SimulationCore.jl:581-592) with time
+ * step dt; energies on the last step when energy_last = 1.  use_graph = 1 replays one captured
+ * CUDA graph per step (captured on the first call); 0 launches the kernels directly. */
+int pd_md_step(pd_md *md, int nsteps, float dt, int energy_last, int use_graph, pd_stream_t s);
+/* Steps through the C ABI with host buffers: copies x, v (pinned host, 3n floats each,
+ * [x..., y..., z...]) to the device, runs nsteps, copies them back with the potential energy
+ * sum (double) of the last step.  Used for end-to-end timing. */
+int pd_md_step_host(pd_md *md, float *host_xyz, float *host_v, int nsteps, float dt,
+                    double *epot_sum, pd_stream_t s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PDB200_H */

@@ -1,0 +1,21 @@
+"""B200 (sm_100a) implementation of ParticleDynamics.jl's per-step force hot path.
+
+The compute path is libpdb200.so (CUDA, built in-tree by ``build.py``); this
+package holds the host side above its C ABI: ctypes bindings, the FP64 setup
+math, the engine objects and the workflow API.  Importing the package does
+not require a GPU; creating an engine does, and there is no CPU fallback.
+"""
+from . import _native, splits, synthetic  # noqa: F401
+from .engine import ClusterPairEngine, DeviceEngine, ElectrostaticsSolver, ElectrostaticsSpec  # noqa: F401
+from .workflow import (  # noqa: F401
+    PME, PPPM, WCA, CellList, ClusterPairList, ConstantVolume, Integrator, LennardJones, ParticleSystem, Simulation,
+    SimulationState, Stage, electrostatics_spec, evaluate_forces_into_f, run, state, step,
+)
+
+__version__ = "0.1.0"
+
+
+def build(force: bool = False):
+    """Compile libpdb200.so for sm_100a (in-tree)."""
+    from ._build import build as _b
+    return _b(force=force)

@@ -1,0 +1,155 @@
+"""ctypes binding of libpdb200.so (declarations mirror include/pdb200.h).
+
+The shared object is built in-tree by ``build.py``.  Loading fails loudly when
+it is missing: there is no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libpdb200.so"
+
+PD_OK, PD_EINVAL, PD_ENOMEM, PD_ECAPACITY, PD_ENONFINITE, PD_ECUFFT, PD_ECUDA, PD_ESTATE, PD_ENOTSUP = range(9)
+PD_LJ_NONE, PD_LJ_UNIFORM, PD_LJ_TABLE = 0, 1, 2
+PD_MESH_SPME, PD_MESH_P3M_AD, PD_MESH_P3M_IK = 1, 2, 3
+PD_MAX_POLY = 32
+PD_MAX_TYPES = 16
+
+_p = C.c_void_p
+_fp = C.c_void_p   # device pointers are passed as integers
+
+
+class ClusterParams(C.Structure):
+    _fields_ = [
+        ("n", C.c_int),
+        ("rmax", C.c_double), ("skin", C.c_double), ("prune_buffer", C.c_double),
+        ("lj_kind", C.c_int),
+        ("lj_c6", C.c_float), ("lj_c12", C.c_float), ("lj_rc2", C.c_float), ("lj_esh", C.c_float),
+        ("ntypes", C.c_int),
+        ("lj_table", C.c_float * (PD_MAX_TYPES * PD_MAX_TYPES * 4)),
+        ("coulomb", C.c_int),
+        ("coul_C", C.c_float), ("coul_rc2", C.c_float), ("coul_sx", C.c_float), ("coul_eshift", C.c_float),
+        ("coul_has_mesh", C.c_int),
+        ("coul_ne", C.c_int), ("coul_nf", C.c_int),
+        ("coul_pe", C.c_float * PD_MAX_POLY), ("coul_pf", C.c_float * PD_MAX_POLY),
+        ("selfc", C.c_float),
+        ("nstlist", C.c_int), ("nstprune", C.c_int),
+    ]
+
+
+class ClusterStats(C.Structure):
+    _fields_ = [
+        ("superclusters", C.c_int), ("outer_entries", C.c_int), ("working_entries", C.c_int),
+        ("error", C.c_int), ("required", C.c_int), ("capacity", C.c_int),
+        ("builds", C.c_int), ("prunes", C.c_int), ("nsmax", C.c_int), ("nslot", C.c_int),
+        ("last_build", C.c_int), ("last_prune", C.c_int),
+        ("tile_bits", C.c_longlong),
+    ]
+
+
+class MeshParams(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int), ("order", C.c_int), ("alias_order", C.c_int),
+        ("mesh", C.c_int * 3),
+        ("alpha", C.c_double), ("C", C.c_double),
+        ("background", C.c_int), ("qtotal", C.c_double),
+        ("nmax", C.c_int),
+    ]
+
+
+class MDState(C.Structure):
+    _fields_ = [
+        ("n", C.c_int),
+        ("x", _fp), ("y", _fp), ("z", _fp),
+        ("vx", _fp), ("vy", _fp), ("vz", _fp),
+        ("fx", _fp), ("fy", _fp), ("fz", _fp),
+        ("q", _fp), ("type", _fp), ("inv_mass", _fp),
+        ("inv_mass_uniform", C.c_float),
+        ("epot", _fp), ("vir6", _fp), ("vglobal6", _fp),
+    ]
+
+
+# name: (restype, argtypes)
+_SIGS = {
+    "pd_version": (C.c_int, []),
+    "pd_strerror": (C.c_char_p, [C.c_int]),
+    "pd_last_error": (C.c_char_p, []),
+    "pd_launch_count": (C.c_uint64, []),
+    "pd_cluster_create": (C.c_int, [C.POINTER(_p), C.POINTER(ClusterParams), C.POINTER(C.c_double)]),
+    "pd_cluster_destroy": (C.c_int, [_p]),
+    "pd_cluster_setup": (C.c_int, [_p, C.POINTER(C.c_double)]),
+    "pd_cluster_grow": (C.c_int, [_p]),
+    "pd_cluster_request_build": (C.c_int, [_p, _p]),
+    "pd_cluster_decide": (C.c_int, [_p, _fp, _fp, _fp, C.c_int, _p]),
+    "pd_cluster_build": (C.c_int, [_p, _fp, _fp, _fp, _fp, _fp, C.c_int, _p]),
+    "pd_cluster_pack": (C.c_int, [_p, _fp, _fp, _fp, _fp, _fp, _p]),
+    "pd_cluster_prune": (C.c_int, [_p, _fp, _fp, _fp, C.c_int, _p]),
+    "pd_cluster_pairs": (C.c_int, [_p, C.c_int, _p]),
+    "pd_cluster_scatter": (C.c_int, [_p, _fp, _fp, _fp, _fp, _fp, _fp, C.c_int, C.c_int, _p]),
+    "pd_cluster_compute": (C.c_int, [_p, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, C.c_int, _p]),
+    "pd_cluster_status": (C.c_int, [_p, C.POINTER(ClusterStats), _p]),
+    "pd_cluster_order": (_fp, [_p]),
+    "pd_cluster_buffers": (C.c_int, [_p, C.POINTER(_p), C.POINTER(_p), C.POINTER(_p), C.POINTER(_p),
+                                     C.POINTER(_p), C.POINTER(_p)]),
+    "pd_mesh_create": (C.c_int, [C.POINTER(_p), C.POINTER(MeshParams), C.POINTER(C.c_double)]),
+    "pd_mesh_destroy": (C.c_int, [_p]),
+    "pd_mesh_set_box": (C.c_int, [_p, C.POINTER(C.c_double)]),
+    "pd_mesh_transform": (C.c_int, [_p, _fp, _fp, _fp, _fp, _fp, C.c_int, C.c_int, _p]),
+    "pd_mesh_gather": (C.c_int, [_p, _fp, _fp, _fp, _fp, _fp, C.c_int, _fp, _fp, _fp, _fp, _fp, C.c_int,
+                                 C.c_int, _p]),
+    "pd_mesh_energy": (C.c_int, [_p, C.POINTER(C.c_double), _p]),
+    "pd_mesh_influence": (C.c_int, [_p, _p, _p]),
+    "pd_mesh_dims": (C.c_int, [_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "pd_md_create": (C.c_int, [C.POINTER(_p), _p, _p, C.POINTER(MDState), C.POINTER(C.c_double)]),
+    "pd_md_destroy": (C.c_int, [_p]),
+    "pd_md_evaluate": (C.c_int, [_p, C.c_int, _p]),
+    "pd_md_step": (C.c_int, [_p, C.c_int, C.c_float, C.c_int, C.c_int, _p]),
+    "pd_md_step_host": (C.c_int, [_p, _p, _p, C.c_int, C.c_float, C.POINTER(C.c_double), _p]),
+}
+
+EXPORTED = tuple(_SIGS)
+
+_lib = None
+
+
+class NativeError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        super().__init__(f"{where}: {msg} (status {code})")
+        self.code = code
+
+
+def lib() -> C.CDLL:
+    """The loaded library (raises if libpdb200.so was not built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python {HERE / '_build.py'}` (there is no CPU fallback)")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(code: int, where: str) -> None:
+    if code != PD_OK:
+        L = lib()
+        msg = L.pd_last_error().decode() or L.pd_strerror(code).decode()
+        raise NativeError(code, where, msg)
+
+
+def call(name: str, *args) -> int:
+    f = getattr(lib(), name)
+    code = f(*args)
+    if f.restype is C.c_int:
+        check(code, name)
+    return code
+
+
+def dbl3(v) -> C.Array:
+    return (C.c_double * 3)(*[float(a) for a in v])

@@ -1,0 +1,377 @@
+// Fused cluster-pair force kernel and slot scatter of libpdb200.
+//
+// Semantics: _cluster_pair_kernel! and _scatter_kernel! of
+// src/clusterpairs/Kernels.jl (ParticleDynamics.jl) with the pair physics of
+// pair_force (src/clusterpairs/PairFunctor.jl:127-156).  Layout of this
+// library: one 64-thread CTA (two warps) per super-cluster part; thread
+// (ti, tj) = (tid & 7, tid >> 3) pairs i-atom ti of each of the 8 i-clusters
+// with j-atom tj of the current j-cluster.  The 64 i-atoms live in shared
+// memory as packed float4 (x, y, z, q); j-atoms are read as one float4 each,
+// with the next entry's j-atom prefetched into registers while the current
+// entry is evaluated.  j-forces are reduced over the 8 ti lanes by shuffles and
+// added with three fence-free reductions; i-forces stay in registers and are
+// reduced once per CTA.
+#include "common.cuh"
+#include "internal.hpp"
+
+using namespace pdb;
+
+namespace pdb {
+
+// (x, y, z) summed over the 8 lanes of a ti group; lanes ti = 0, 1, 2 return the
+// x, y, z totals (_reduce3, Kernels.jl:20-30).
+__device__ __forceinline__ float reduce3(float fx, float fy, float fz, int ti) {
+    fx += __shfl_down_sync(0xffffffffu, fx, 1);
+    fy += __shfl_up_sync(0xffffffffu, fy, 1);
+    fz += __shfl_down_sync(0xffffffffu, fz, 1);
+    fx = (ti & 1) ? fy : fx;
+    fx += __shfl_down_sync(0xffffffffu, fx, 2);
+    fz += __shfl_up_sync(0xffffffffu, fz, 2);
+    fx = (ti & 2) ? fz : fx;
+    fx += __shfl_down_sync(0xffffffffu, fx, 4);
+    return fx;
+}
+
+__device__ __forceinline__ float sum8(float v) {
+    v += __shfl_down_sync(0xffffffffu, v, 4);
+    v += __shfl_down_sync(0xffffffffu, v, 2);
+    v += __shfl_down_sync(0xffffffffu, v, 1);
+    return v;
+}
+
+__device__ __forceinline__ float reduce_i(float v) {
+    v += __shfl_down_sync(0xffffffffu, v, 16);
+    v += __shfl_down_sync(0xffffffffu, v, 8);
+    return v;
+}
+
+__device__ __forceinline__ float horner(const float *c, int n, float x) {
+    float acc = c[n - 1];
+    for (int k = n - 2; k >= 0; --k) acc = fmaf(acc, x, c[k]);
+    return acc;
+}
+
+template <int LJK, bool COUL, bool ENERGY>
+__global__ void __launch_bounds__(64) k_pairs(const float4 *__restrict__ xq, const int *__restrict__ ts,
+                                              const uint2 *__restrict__ cjw, const int *__restrict__ scio,
+                                              const int *__restrict__ nw, const int *__restrict__ counts,
+                                              const float *__restrict__ lj_table, float4 *__restrict__ fc,
+                                              float *__restrict__ vc, int nslot, int nsplit, const PairParams pp) {
+    const int tid = threadIdx.x;
+    const int ti = tid & 7, tj = tid >> 3, w = tid >> 5;
+    const int S = blockIdx.x / nsplit, part = blockIdx.x % nsplit;
+    if (S >= counts[W_NS] || counts[W_ERR] != 0) return;
+    __shared__ float4 sxq[SUPER];
+    __shared__ int sty[SUPER];
+    __shared__ float4 stab[LJK == PD_LJ_TABLE ? PD_MAX_TYPES * PD_MAX_TYPES : 1];
+    sxq[tid] = xq[S * SUPER + tid];
+    if (LJK == PD_LJ_TABLE) {
+        sty[tid] = (ts[S * SUPER + tid] - 1) * pp.ntypes;
+        for (int k = tid; k < pp.ntypes * pp.ntypes; k += SUPER)
+            stab[k] = reinterpret_cast<const float4 *>(lj_table)[k];
+    }
+    __syncthreads();
+    const float Lx = pp.Lx, Ly = pp.Ly, Lz = pp.Lz;
+    const float hx = 0.5f * Lx, hy = 0.5f * Ly, hz = 0.5f * Lz;
+    const float inf = __int_as_float(0x7f800000);
+    float fxi[8], fyi[8], fzi[8];
+    float ei[8], w1i[8], w2i[8], w3i[8], w4i[8], w5i[8], w6i[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        fxi[a] = fyi[a] = fzi[a] = 0.f;
+        if (ENERGY) ei[a] = w1i[a] = w2i[a] = w3i[a] = w4i[a] = w5i[a] = w6i[a] = 0.f;
+    }
+    const int e0 = scio[S], ne = nw[S];
+    const int ea = e0 + (int)(((long long)ne * part) / nsplit);
+    const int eb = e0 + (int)(((long long)ne * (part + 1)) / nsplit);
+    // software pipeline: the entry and j-atom of the next iteration are loaded ahead
+    uint2 ent = ea < eb ? cjw[ea] : make_uint2(0u, 0u);
+    float4 pj = ea < eb ? xq[(int)ent.x * 8 + tj] : make_float4(0.f, 0.f, 0.f, 0.f);
+    int tyj = (LJK == PD_LJ_TABLE && ea < eb) ? ts[(int)ent.x * 8 + tj] : 1;
+    for (int e = ea; e < eb; ++e) {
+        const uint2 cur = ent;
+        const float4 cpj = pj;
+        const int ctyj = tyj;
+        if (e + 1 < eb) {
+            ent = cjw[e + 1];
+            pj = xq[(int)ent.x * 8 + tj];
+            if (LJK == PD_LJ_TABLE) tyj = ts[(int)ent.x * 8 + tj];
+        }
+        const uint32_t imask = (cur.y >> (8 * w)) & 0xffu;
+        if (imask == 0) continue;   // uniform per warp
+        const int cj = (int)cur.x;
+        const int js = cj * 8 + tj;
+        float fjx = 0.f, fjy = 0.f, fjz = 0.f;
+        float ej = 0.f, vj1 = 0.f, vj2 = 0.f, vj3 = 0.f, vj4 = 0.f, vj5 = 0.f, vj6 = 0.f;
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            if ((imask >> a) & 1u) {
+                const float4 pi = sxq[a * 8 + ti];
+                float dx = pi.x - cpj.x, dy = pi.y - cpj.y, dz = pi.z - cpj.z;
+                // compensated periodic difference only when a lane of this warp needs it
+                if (__any_sync(0xffffffffu, (fabsf(dx) > hx) | (fabsf(dy) > hy) | (fabsf(dz) > hz))) {
+                    dx = periodic_delta(pi.x, cpj.x, hx, Lx);
+                    dy = periodic_delta(pi.y, cpj.y, hy, Ly);
+                    dz = periodic_delta(pi.z, cpj.z, hz, Lz);
+                }
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const bool ok = ((cj != S * 8 + a) || (tj > ti)) && (r2 < inf);
+                const float rinv = rsqrtf(r2);
+                const float rinv2 = rinv * rinv;
+                float f = 0.f, en = 0.f;
+                if (LJK != PD_LJ_NONE) {
+                    float c6, c12, lrc2, esh;
+                    if (LJK == PD_LJ_TABLE) {
+                        const float4 tb = stab[sty[a * 8 + ti] + (ctyj - 1)];
+                        c6 = tb.x;
+                        c12 = tb.y;
+                        lrc2 = tb.z;
+                        esh = tb.w;
+                    } else {
+                        c6 = pp.c6;
+                        c12 = pp.c12;
+                        lrc2 = pp.lrc2;
+                        esh = pp.esh;
+                    }
+                    const bool use = r2 < lrc2;
+                    const float ir6 = rinv2 * rinv2 * rinv2;
+                    f += use ? (12.f * c12 * ir6 - 6.f * c6) * ir6 * rinv2 : 0.f;
+                    if (ENERGY) en += use ? (c12 * ir6 - c6) * ir6 - esh : 0.f;
+                }
+                if (COUL) {
+                    const bool inr = r2 < pp.rc2;
+                    const float x = fmaf(r2, pp.sx, -1.f);
+                    const float pf = horner(pp.pf, pp.nf, x);
+                    const float rinv3 = rinv * rinv2;
+                    const float cq = pp.C * (pi.w * cpj.w);
+                    f += cq * (inr ? rinv3 - pf : 0.f);
+                    if (ENERGY) {
+                        const float pe = horner(pp.pe, pp.ne, x);
+                        en += cq * (inr ? rinv + pe - pp.eshift : 0.f);
+                    }
+                }
+                f = ok ? f : 0.f;
+                dx = ok ? dx : 0.f;
+                dy = ok ? dy : 0.f;
+                dz = ok ? dz : 0.f;
+                const float fxp = f * dx, fyp = f * dy, fzp = f * dz;
+                fxi[a] += fxp;
+                fyi[a] += fyp;
+                fzi[a] += fzp;
+                fjx -= fxp;
+                fjy -= fyp;
+                fjz -= fzp;
+                if (ENERGY) {
+                    en = ok ? 0.5f * en : 0.f;
+                    const float w1 = 0.5f * fxp * dx, w2 = 0.5f * fyp * dy, w3 = 0.5f * fzp * dz;
+                    const float w4 = 0.5f * fxp * dy, w5 = 0.5f * fxp * dz, w6 = 0.5f * fyp * dz;
+                    ei[a] += en;
+                    w1i[a] += w1;
+                    w2i[a] += w2;
+                    w3i[a] += w3;
+                    w4i[a] += w4;
+                    w5i[a] += w5;
+                    w6i[a] += w6;
+                    ej += en;
+                    vj1 += w1;
+                    vj2 += w2;
+                    vj3 += w3;
+                    vj4 += w4;
+                    vj5 += w5;
+                    vj6 += w6;
+                }
+            }
+        }
+        const float r = reduce3(fjx, fjy, fjz, ti);
+        if (ti < 3) red_add(reinterpret_cast<float *>(&fc[js]) + ti, r);
+        if (ENERGY) {
+            const float rv1 = reduce3(vj1, vj2, vj3, ti);
+            const float rv2 = reduce3(vj4, vj5, vj6, ti);
+            ej = sum8(ej);
+            if (ti < 3) {
+                red_add(&vc[(size_t)ti * nslot + js], rv1);
+                red_add(&vc[(size_t)(ti + 3) * nslot + js], rv2);
+            }
+            if (ti == 0) red_add(reinterpret_cast<float *>(&fc[js]) + 3, ej);
+        }
+    }
+    const int lane = tid & 31;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        fxi[a] = reduce_i(fxi[a]);
+        fyi[a] = reduce_i(fyi[a]);
+        fzi[a] = reduce_i(fzi[a]);
+        if (ENERGY) {
+            ei[a] = reduce_i(ei[a]);
+            w1i[a] = reduce_i(w1i[a]);
+            w2i[a] = reduce_i(w2i[a]);
+            w3i[a] = reduce_i(w3i[a]);
+            w4i[a] = reduce_i(w4i[a]);
+            w5i[a] = reduce_i(w5i[a]);
+            w6i[a] = reduce_i(w6i[a]);
+        }
+    }
+    if (lane < 8) {
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            const int ai = S * SUPER + a * 8 + lane;
+            if (ENERGY) {
+                red_add_v4(reinterpret_cast<float *>(&fc[ai]), fxi[a], fyi[a], fzi[a], ei[a]);
+                red_add(&vc[(size_t)0 * nslot + ai], w1i[a]);
+                red_add(&vc[(size_t)1 * nslot + ai], w2i[a]);
+                red_add(&vc[(size_t)2 * nslot + ai], w3i[a]);
+                red_add(&vc[(size_t)3 * nslot + ai], w4i[a]);
+                red_add(&vc[(size_t)4 * nslot + ai], w5i[a]);
+                red_add(&vc[(size_t)5 * nslot + ai], w6i[a]);
+            } else {
+                red_add_v4(reinterpret_cast<float *>(&fc[ai]), fxi[a], fyi[a], fzi[a], 0.f);
+            }
+        }
+    }
+}
+
+// Slot buffers to storage order, self energy, zeroing (_scatter_kernel!, Kernels.jl:207-240).
+template <bool ENERGY, bool ADD>
+__global__ void k_scatter(const int *__restrict__ perm, int nslot, const int *__restrict__ counts,
+                          float4 *__restrict__ fc, float *__restrict__ vc, const float *__restrict__ q,
+                          float half_c_self, float *__restrict__ fx, float *__restrict__ fy, float *__restrict__ fz,
+                          float *__restrict__ epot, float *__restrict__ vir6) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslot) return;
+    const int used = counts[W_NS] * SUPER;
+    if (s >= used) return;   // slots past the super-cluster count hold nothing
+    const int i = perm[s];
+    const float4 f = fc[s];
+    if (i >= 0) {
+        if (ADD) {
+            fx[i] += f.x;
+            fy[i] += f.y;
+            fz[i] += f.z;
+        } else {
+            fx[i] = f.x;
+            fy[i] = f.y;
+            fz[i] = f.z;
+        }
+        if (ENERGY) {
+            float e = f.w;
+            if (q) {
+                const float qi = q[i];
+                e -= half_c_self * qi * qi;
+            }
+            epot[i] = ADD ? epot[i] + e : e;
+            if (vir6) {
+#pragma unroll
+                for (int k = 0; k < 6; ++k) vir6[(size_t)i * 6 + k] = vc[(size_t)k * nslot + s];
+            }
+        }
+    }
+    fc[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (ENERGY) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) vc[(size_t)k * nslot + s] = 0.f;
+    }
+}
+
+int cluster_pairs_launch(pd_cluster *c, int energy, cudaStream_t s) {
+    const int grid = c->nsmax * c->nsplit;
+    const PairParams &pp = c->pp;
+#define PD_PAIRS(LJK, COUL, EN)                                                                            \
+    k_pairs<LJK, COUL, EN><<<grid, 64, 0, s>>>(c->xq, c->ts, c->cjw, c->scio, c->nw, c->counts, c->lj_table, \
+                                               c->fc, c->vc, c->nslot, c->nsplit, pp)
+#define PD_PAIRS_E(LJK, COUL) \
+    do {                      \
+        if (energy)           \
+            PD_PAIRS(LJK, COUL, true); \
+        else                  \
+            PD_PAIRS(LJK, COUL, false); \
+    } while (0)
+    const bool coul = pp.coulomb != 0;
+    switch (pp.lj_kind) {
+        case PD_LJ_NONE:
+            if (coul) PD_PAIRS_E(PD_LJ_NONE, true);
+            else PD_PAIRS_E(PD_LJ_NONE, false);
+            break;
+        case PD_LJ_UNIFORM:
+            if (coul) PD_PAIRS_E(PD_LJ_UNIFORM, true);
+            else PD_PAIRS_E(PD_LJ_UNIFORM, false);
+            break;
+        default:
+            if (coul) PD_PAIRS_E(PD_LJ_TABLE, true);
+            else PD_PAIRS_E(PD_LJ_TABLE, false);
+            break;
+    }
+#undef PD_PAIRS_E
+#undef PD_PAIRS
+    PD_LAUNCHED();
+    return PD_OK;
+}
+
+}  // namespace pdb
+
+extern "C" {
+
+int pd_cluster_pairs(pd_cluster *c, int energy, pd_stream_t s) {
+    PD_CHECK(c, PD_EINVAL, "pd_cluster_pairs: null handle");
+    PD_CHECK(c->have_build, PD_ESTATE, "pd_cluster_pairs: the list has not been built");
+    return cluster_pairs_launch(c, energy, (cudaStream_t)s);
+}
+
+int pd_cluster_scatter(pd_cluster *c, float *fx, float *fy, float *fz, float *epot, float *vir6, const float *q,
+                       int energy, int add, pd_stream_t s) {
+    PD_CHECK(c && fx && fy && fz, PD_EINVAL, "pd_cluster_scatter: null argument");
+    PD_CHECK(!energy || epot, PD_EINVAL, "pd_cluster_scatter: energy needs epot");
+    const float hcs = 0.5f * c->p.coul_C * c->p.selfc;
+    const float *qq = c->p.coulomb ? q : nullptr;
+    cudaStream_t st = (cudaStream_t)s;
+    const int blocks = (c->nslot + 255) / 256;
+    if (energy) {
+        if (add)
+            k_scatter<true, true><<<blocks, 256, 0, st>>>(c->perm, c->nslot, c->counts, c->fc, c->vc, qq, hcs, fx, fy, fz,
+                                                          epot, vir6);
+        else
+            k_scatter<true, false><<<blocks, 256, 0, st>>>(c->perm, c->nslot, c->counts, c->fc, c->vc, qq, hcs, fx, fy,
+                                                           fz, epot, vir6);
+    } else {
+        if (add)
+            k_scatter<false, true><<<blocks, 256, 0, st>>>(c->perm, c->nslot, c->counts, c->fc, c->vc, qq, hcs, fx, fy,
+                                                           fz, epot, vir6);
+        else
+            k_scatter<false, false><<<blocks, 256, 0, st>>>(c->perm, c->nslot, c->counts, c->fc, c->vc, qq, hcs, fx,
+                                                            fy, fz, epot, vir6);
+    }
+    PD_LAUNCHED();
+    return PD_OK;
+}
+
+int pd_cluster_compute(pd_cluster *c, const float *x, const float *y, const float *z, const float *q, const int *type,
+                       float *fx, float *fy, float *fz, float *epot, float *vir6, int energy, pd_stream_t s) {
+    PD_CHECK(c && x && y && z && fx && fy && fz, PD_EINVAL, "pd_cluster_compute: null argument");
+    cudaStream_t st = (cudaStream_t)s;
+    int rc;
+    int h[W_LEN];
+    // update_list! (Engine.jl:160-176): decision at the current coordinates
+    if ((rc = cluster_decide_launch(c, x, y, z, 0, st))) return rc;
+    if ((rc = cluster_read_counts(c, h, st))) return rc;
+    if (h[W_BUILD] || !c->have_build) {
+        for (int attempt = 0; attempt < 8; ++attempt) {
+            if ((rc = cluster_build_launch(c, x, y, z, q, type, 0, st))) return rc;
+            if ((rc = cluster_read_counts(c, h, st))) return rc;
+            if (h[W_ERR] == 0) break;
+            if (h[W_ERR] == PD_ENONFINITE) {
+                set_error("Cluster-pair list: non-finite coordinates");
+                return PD_ENONFINITE;
+            }
+            if ((rc = pd_cluster_grow(c))) return rc;
+        }
+        PD_CHECK(h[W_ERR] == 0, PD_ECAPACITY, "outer list still overflows after growth");
+        c->have_build = true;
+        if ((rc = cluster_set_word(c, W_PRUNE, 1, st))) return rc;
+    } else {
+        if ((rc = pd_cluster_pack(c, x, y, z, q, type, s))) return rc;
+    }
+    if ((rc = cluster_prune_launch(c, 1, st))) return rc;
+    if ((rc = cluster_pairs_launch(c, energy, st))) return rc;
+    return pd_cluster_scatter(c, fx, fy, fz, epot, vir6, q, energy, 0, s);
+}
+
+}  // extern "C"

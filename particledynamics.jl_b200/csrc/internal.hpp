@@ -1,0 +1,160 @@
+// Host-side structures of libpdb200 shared by its translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+#include <string>
+
+#include "../../include/pdb200.h"
+
+namespace pdb {
+
+// Thread-local message of the last failure (pd_last_error).
+void set_error(const char *fmt, ...);
+void count_launch(int n = 1);
+
+#define PD_CUDA(call)                                                                   \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess) {                                                        \
+            ::pdb::set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),     \
+                             __FILE__, __LINE__);                                       \
+            return e_ == cudaErrorMemoryAllocation ? PD_ENOMEM : PD_ECUDA;              \
+        }                                                                               \
+    } while (0)
+
+#define PD_LAUNCHED()                                                                   \
+    do {                                                                                \
+        ::pdb::count_launch();                                                          \
+        cudaError_t e_ = cudaGetLastError();                                            \
+        if (e_ != cudaSuccess) {                                                        \
+            ::pdb::set_error("kernel launch failed: %s (%s:%d)", cudaGetErrorString(e_), \
+                             __FILE__, __LINE__);                                       \
+            return PD_ECUDA;                                                            \
+        }                                                                               \
+    } while (0)
+
+#define PD_CHECK(cond, code, ...)        \
+    do {                                 \
+        if (!(cond)) {                   \
+            ::pdb::set_error(__VA_ARGS__); \
+            return (code);               \
+        }                                \
+    } while (0)
+
+template <typename T>
+int dalloc(T **p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        set_error("cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+        *p = nullptr;
+        return PD_ENOMEM;
+    }
+    return PD_OK;
+}
+template <typename T>
+void dfree(T *&p) {
+    if (p) cudaFree((void *)p);
+    p = nullptr;
+}
+
+// Parameters of the fused pair kernel, passed by value (kernel parameter space).
+struct PairParams {
+    float Lx, Ly, Lz;
+    int lj_kind;
+    float c6, c12, lrc2, esh;     // uniform LJ
+    int ntypes;
+    int coulomb;
+    float C, rc2, sx, eshift;
+    int ne, nf;
+    float pe[PD_MAX_POLY];
+    float pf[PD_MAX_POLY];
+};
+
+}  // namespace pdb
+
+struct pd_cluster {
+    pd_cluster_params p;
+    int n = 0;
+    double box[3] = {0, 0, 0};
+    float L[3] = {0, 0, 0};
+    double rlist = 0;
+    // geometry of the last setup (List.jl:874-937)
+    int ncx = 0, ncy = 0, nzb = 0, mx = 0, my = 0, ncol = 0, nbin = 0, nsmax = 0, nslot = 0, ncs = 0;
+    int necap = 0;
+    bool grown = false;
+    bool have_build = false;
+    int nsplit = 1;
+    int num_sms = 148;
+    // device buffers
+    int *counts = nullptr;     // W_LEN words
+    int *bin = nullptr;        // N
+    int *bcnt = nullptr;       // nbin, zero between builds
+    int *bstart = nullptr;     // nbin + 1
+    int *cursor = nullptr;     // nbin
+    int *sorted = nullptr;     // N
+    int *col_sc_off = nullptr; // ncol + 1
+    int *sc_first = nullptr, *sc_n = nullptr, *sc_col = nullptr;  // nsmax
+    int *perm = nullptr;       // nslot (-1 padding)
+    int *slot_of = nullptr;    // N
+    int *order = nullptr;      // N
+    float4 *xq = nullptr;      // nslot
+    int *ts = nullptr;         // nslot
+    float4 *cbc = nullptr, *cbh = nullptr;   // 8 nsmax cluster boxes (centre, half width)
+    float4 *sbc = nullptr, *sbh = nullptr;   // nsmax super-cluster boxes
+    int *cnt_sc = nullptr;     // nsmax
+    int *scio = nullptr;       // nsmax + 1
+    uint32_t *cjo = nullptr;   // necap
+    uint2 *cjw = nullptr;      // necap
+    int *nw = nullptr;         // nsmax
+    float4 *fc = nullptr;      // nslot: force xyz + energy
+    float *vc = nullptr;       // 6 nslot
+    float4 *ref_build = nullptr, *ref_prune = nullptr;  // N
+    float *lj_table = nullptr; // ntypes^2 x 4 (device)
+    pdb::PairParams pp;
+};
+
+struct pd_mesh {
+    pd_mesh_params p;
+    int K1 = 0, K2 = 0, K3 = 0, K1h = 0;
+    int nmodes = 0, nnodes = 0;
+    double box[3] = {0, 0, 0};
+    double ubg = 0.0;          // background energy
+    float bg = 0.0f;           // background potential per unit charge
+    int nmax_packed = 0;
+    float *gridA = nullptr;    // charge grid (kept zero between transforms)
+    float *gridB = nullptr;    // potential grid
+    float *field[3] = {nullptr, nullptr, nullptr};  // ik field grids
+    cufftComplex *spec = nullptr;
+    cufftComplex *scratch = nullptr;                // ik
+    float *G = nullptr;        // nmodes
+    float *Vc = nullptr;       // 6 nmodes (row c: c * nmodes + m)
+    double *acc = nullptr;     // 7
+    float4 *packed = nullptr;  // particles packed in the caller's order (SoA entry points)
+    cufftHandle fwd = 0, bwd = 0;
+    bool plans = false;
+    void *work = nullptr;
+    size_t work_size = 0;
+    cudaStream_t plan_stream = nullptr;
+};
+
+namespace pdb {
+// Mesh internals used by the step engine.
+int mesh_transform_packed(pd_mesh *m, const float4 *xq, int nchunks, const int *ns_dev, int energy, cudaStream_t s);
+int mesh_gather_join(pd_mesh *m, pd_cluster *c, const float4 *xq, const int *perm, const int *ns_dev, int nchunks,
+                     float *fx, float *fy, float *fz, float *vx, float *vy, float *vz, const float *inv_mass,
+                     float inv_mass_uniform, float half_dt, float *epot, float *vir6, float *vglobal6, const float *q,
+                     float half_c_self, int energy, cudaStream_t s);
+int mesh_store_virial(pd_mesh *m, float *vglobal6, cudaStream_t s);
+// Cluster internals used by the step engine.
+int cluster_decide_launch(pd_cluster *c, const float *x, const float *y, const float *z, int fixed, cudaStream_t s);
+int cluster_pairs_launch(pd_cluster *c, int energy, cudaStream_t s);
+int cluster_build_launch(pd_cluster *c, const float *x, const float *y, const float *z, const float *q,
+                         const int *type, int conditional, cudaStream_t s);
+int cluster_prune_launch(pd_cluster *c, int conditional, cudaStream_t s);
+int cluster_read_counts(pd_cluster *c, int *host, cudaStream_t s);
+int cluster_set_word(pd_cluster *c, int word, int value, cudaStream_t s);
+}  // namespace pdb

@@ -1,0 +1,381 @@
+// Device step engine of libpdb200: one velocity-Verlet NVE step as a fixed
+// sequence of kernels that is captured once into a CUDA graph and replayed.
+//
+// The reference's device engine (src/engine/ClusterBackend.jl:90-220,
+// src/engine/Run.jl:247-294, src/simulation/NVEFusion.jl:3-27) runs
+// kick+drift, the list decision, conditional build / prune bodies, the pair
+// pass beside the mesh transform, a scatter and the closing kick.  Here:
+//   1. k_kick_drift: half kick, drift, wrap, pack of the cluster-ordered force
+//      coordinates and the displacement maxima for the list decision, fused;
+//   2. the one-thread decision;
+//   3. build and prune kernels that run only when the device flags ask for them;
+//   4. the pair pass on the main stream and the mesh transform (spread, R2C,
+//      solve, C2R) on a second stream;
+//   5. the join: mesh gather + slot pair forces + store in storage order +
+//      closing half kick, one kernel per super-cluster (k_gather, mesh.cu), or
+//      k_scatter_kick without a mesh.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "internal.hpp"
+
+using namespace pdb;
+
+struct pd_md {
+    pd_cluster *c = nullptr;
+    pd_mesh *m = nullptr;
+    pd_md_state st;
+    float L[3] = {0, 0, 0};
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};   // [energy]
+    float exec_dt[2] = {0.f, 0.f};
+    cudaStream_t exec_stream[2] = {nullptr, nullptr};
+    double *esum = nullptr;   // device FP64 energy sum
+    float half_c_self = 0.f;
+};
+
+namespace pdb {
+
+// _nve_kick_drift3_kernel! (NVEFusion.jl:3-27) fused with the pack of the force
+// coordinates (_pack_kernel!, List.jl:377-413) and the displacement maxima of
+// _displacement_kernel! (List.jl:787-819).
+__global__ void __launch_bounds__(256) k_kick_drift(int n, float *__restrict__ x, float *__restrict__ y,
+                                                    float *__restrict__ z, float *__restrict__ vx,
+                                                    float *__restrict__ vy, float *__restrict__ vz,
+                                                    const float *__restrict__ fx, const float *__restrict__ fy,
+                                                    const float *__restrict__ fz, const float *__restrict__ inv_mass,
+                                                    float inv_mass_uniform, float dt, float Lx, float Ly, float Lz,
+                                                    const float *__restrict__ q, const int *__restrict__ slot_of,
+                                                    float4 *__restrict__ xq, const float4 *__restrict__ rb,
+                                                    const float4 *__restrict__ rp, float tb2, float tp2,
+                                                    int *__restrict__ counts) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float ra = 0.f, rbv = 0.f;
+    if (i < n) {
+        const float c = 0.5f * dt * (inv_mass ? inv_mass[i] : inv_mass_uniform);
+        const float ux = fmaf(c, fx[i], vx[i]), uy = fmaf(c, fy[i], vy[i]), uz = fmaf(c, fz[i], vz[i]);
+        vx[i] = ux;
+        vy[i] = uy;
+        vz[i] = uz;
+        float xi = fmaf(dt, ux, x[i]), yi = fmaf(dt, uy, y[i]), zi = fmaf(dt, uz, z[i]);
+        xi -= (xi >= 0.5f * Lx) ? Lx : 0.f;
+        xi += (xi < -0.5f * Lx) ? Lx : 0.f;
+        yi -= (yi >= 0.5f * Ly) ? Ly : 0.f;
+        yi += (yi < -0.5f * Ly) ? Ly : 0.f;
+        zi -= (zi >= 0.5f * Lz) ? Lz : 0.f;
+        zi += (zi < -0.5f * Lz) ? Lz : 0.f;
+        x[i] = xi;
+        y[i] = yi;
+        z[i] = zi;
+        xq[slot_of[i]] = make_float4(force_coordinate(xi, Lx), force_coordinate(yi, Ly), force_coordinate(zi, Lz),
+                                     q ? q[i] : 0.f);
+        const float4 b = rb[i];
+        float dx = mic(xi - b.x, Lx), dy = mic(yi - b.y, Ly), dz = mic(zi - b.z, Lz);
+        float d2 = dx * dx + dy * dy + dz * dz;
+        rbv = tb2 > 0.f ? d2 / tb2 : (d2 > 0.f ? __int_as_float(0x7f800000) : 0.f);
+        if (!isfinite(rbv)) rbv = __int_as_float(0x7f800000);
+        const float4 p = rp[i];
+        dx = mic(xi - p.x, Lx);
+        dy = mic(yi - p.y, Ly);
+        dz = mic(zi - p.z, Lz);
+        d2 = dx * dx + dy * dy + dz * dz;
+        const float rpv = tp2 > 0.f ? d2 / tp2 : (d2 > 0.f ? __int_as_float(0x7f800000) : 0.f);
+        ra = fmaxf(rbv, rpv);
+    }
+    ra = warp_max(ra);
+    rbv = warp_max(rbv);
+    __shared__ float sh[2][8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        sh[0][w] = ra;
+        sh[1][w] = rbv;
+    }
+    __syncthreads();
+    if (w == 0) {
+        float a = lane < 8 ? sh[0][lane] : 0.f;
+        float c = lane < 8 ? sh[1][lane] : 0.f;
+        a = warp_max(a);
+        c = warp_max(c);
+        if (lane == 0) {
+            atomicMax(&counts[W_FLAG_ANY], __float_as_int(a));
+            atomicMax(&counts[W_FLAG_BUILD], __float_as_int(c));
+        }
+    }
+}
+
+__global__ void k_decide_step(int *__restrict__ counts, int nstlist, int nstprune) {
+    float anyr = __int_as_float(counts[W_FLAG_ANY]);
+    float br = __int_as_float(counts[W_FLAG_BUILD]);
+    bool build, prune;
+    if (nstlist > 0) {
+        int k = counts[W_DSTEP];
+        counts[W_DSTEP] = k + 1;
+        build = (k % nstlist == 0) || (counts[W_REQUEST] != 0) || !isfinite(br);
+        prune = build || (nstprune > 0 && k % nstprune == 0);
+    } else {
+        build = (br > 1.0f) || (counts[W_REQUEST] != 0);
+        prune = build || (anyr > 1.0f);
+    }
+    counts[W_BUILD] = build ? 1 : 0;
+    counts[W_PRUNE] = prune ? 1 : 0;
+    counts[W_REQUEST] = 0;
+    counts[W_NBUILD] += build ? 1 : 0;
+    counts[W_NPRUNE] += prune ? 1 : 0;
+    counts[W_FLAG_ANY] = 0;
+    counts[W_FLAG_BUILD] = 0;
+}
+
+// Slot forces to storage order with the closing half kick (no mesh):
+// _scatter_kernel! (Kernels.jl:207-240) + _nve_kick3_kernel! (SimulationCore.jl:581-592).
+template <bool ENERGY>
+__global__ void k_scatter_kick(const int *__restrict__ perm, int nslot, const int *__restrict__ counts,
+                               float4 *__restrict__ fc, float *__restrict__ vc, const float4 *__restrict__ xq,
+                               float half_c_self, float *__restrict__ fx, float *__restrict__ fy,
+                               float *__restrict__ fz, float *__restrict__ vx, float *__restrict__ vy,
+                               float *__restrict__ vz, const float *__restrict__ inv_mass, float inv_mass_uniform,
+                               float half_dt, float *__restrict__ epot, float *__restrict__ vir6) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslot || s >= counts[W_NS] * SUPER) return;
+    const int i = perm[s];
+    const float4 f = fc[s];
+    fc[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (i >= 0) {
+        fx[i] = f.x;
+        fy[i] = f.y;
+        fz[i] = f.z;
+        const float cm = half_dt * (inv_mass ? inv_mass[i] : inv_mass_uniform);
+        vx[i] = fmaf(cm, f.x, vx[i]);
+        vy[i] = fmaf(cm, f.y, vy[i]);
+        vz[i] = fmaf(cm, f.z, vz[i]);
+        if (ENERGY) {
+            const float qi = xq[s].w;
+            epot[i] = f.w - half_c_self * qi * qi;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) vir6[(size_t)i * 6 + k] = vc[(size_t)k * nslot + s];
+        }
+    }
+    if (ENERGY) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) vc[(size_t)k * nslot + s] = 0.f;
+    }
+}
+
+__global__ void k_sum(const float *__restrict__ v, int n, double *__restrict__ out) {
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += (double)v[i];
+    s = warp_sum_d(s);
+    __shared__ double sh[8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sh[w] = s;
+    __syncthreads();
+    if (w == 0) {
+        s = lane < 8 ? sh[lane] : 0.0;
+        s = warp_sum_d(s);
+        if (lane == 0) red_add_d(out, s);
+    }
+}
+
+}  // namespace pdb
+
+// Closing part of a step: pair pass beside the mesh transform, then the join.
+static int enqueue_forces(pd_md *md, int energy, float half_dt, cudaStream_t s) {
+    pd_cluster *c = md->c;
+    pd_mesh *m = md->m;
+    pd_md_state &st = md->st;
+    int rc;
+    if (m) {
+        PD_CUDA(cudaEventRecord(md->ev_fork, s));
+        PD_CUDA(cudaStreamWaitEvent(md->side, md->ev_fork, 0));
+        if ((rc = mesh_transform_packed(m, c->xq, c->nsmax, c->counts + W_NS, energy, md->side))) return rc;
+        PD_CUDA(cudaEventRecord(md->ev_join, md->side));
+    }
+    if ((rc = cluster_pairs_launch(c, energy, s))) return rc;
+    if (m) {
+        PD_CUDA(cudaStreamWaitEvent(s, md->ev_join, 0));
+        rc = mesh_gather_join(m, c, c->xq, c->perm, c->counts + W_NS, c->nsmax, st.fx, st.fy, st.fz, st.vx, st.vy,
+                              st.vz, st.inv_mass, st.inv_mass_uniform, half_dt, st.epot, st.vir6, st.vglobal6, st.q,
+                              md->half_c_self, energy, s);
+        if (rc) return rc;
+    } else {
+        const int blocks = (c->nslot + 255) / 256;
+        if (energy)
+            k_scatter_kick<true><<<blocks, 256, 0, s>>>(c->perm, c->nslot, c->counts, c->fc, c->vc, c->xq,
+                                                        md->half_c_self, st.fx, st.fy, st.fz, st.vx, st.vy, st.vz,
+                                                        st.inv_mass, st.inv_mass_uniform, half_dt, st.epot, st.vir6);
+        else
+            k_scatter_kick<false><<<blocks, 256, 0, s>>>(c->perm, c->nslot, c->counts, c->fc, c->vc, c->xq,
+                                                         md->half_c_self, st.fx, st.fy, st.fz, st.vx, st.vy, st.vz,
+                                                         st.inv_mass, st.inv_mass_uniform, half_dt, st.epot,
+                                                         st.vir6);
+        PD_LAUNCHED();
+    }
+    return PD_OK;
+}
+
+// One full step, device-decided (capturable).
+static int enqueue_step(pd_md *md, float dt, int energy, cudaStream_t s) {
+    pd_cluster *c = md->c;
+    pd_md_state &st = md->st;
+    const float hb = (float)(0.5 * c->p.skin), hp = (float)(0.5 * c->p.prune_buffer);
+    k_kick_drift<<<(st.n + 255) / 256, 256, 0, s>>>(st.n, st.x, st.y, st.z, st.vx, st.vy, st.vz, st.fx, st.fy, st.fz,
+                                                    st.inv_mass, st.inv_mass_uniform, dt, md->L[0], md->L[1], md->L[2],
+                                                    c->p.coulomb ? st.q : nullptr, c->slot_of, c->xq, c->ref_build,
+                                                    c->ref_prune, hb * hb, hp * hp, c->counts);
+    PD_LAUNCHED();
+    k_decide_step<<<1, 1, 0, s>>>(c->counts, c->p.nstlist, c->p.nstprune);
+    PD_LAUNCHED();
+    int rc;
+    if ((rc = cluster_build_launch(c, st.x, st.y, st.z, c->p.coulomb ? st.q : nullptr, st.type, 1, s))) return rc;
+    if ((rc = cluster_prune_launch(c, 1, s))) return rc;
+    return enqueue_forces(md, energy, 0.5f * dt, s);
+}
+
+extern "C" {
+
+int pd_md_create(pd_md **out, pd_cluster *c, pd_mesh *m, const pd_md_state *st, double box[3]) {
+    PD_CHECK(out && c && st && box, PD_EINVAL, "pd_md_create: null argument");
+    *out = nullptr;
+    PD_CHECK(st->n == c->n, PD_EINVAL, "pd_md_create: state has %d particles, the list %d", st->n, c->n);
+    PD_CHECK(st->x && st->y && st->z && st->vx && st->vy && st->vz && st->fx && st->fy && st->fz, PD_EINVAL,
+             "pd_md_create: state arrays missing");
+    PD_CHECK(!m || st->q, PD_EINVAL, "pd_md_create: a mesh needs charges");
+    PD_CHECK(!m || m->p.kind != PD_MESH_P3M_IK, PD_ENOTSUP,
+             "pd_md_create: the fused step supports analytic differentiation (SPME, P3M-AD)");
+    PD_CHECK(!m || m->p.nmax >= 0, PD_EINVAL, "bad mesh");
+    pd_md *md = new pd_md();
+    md->c = c;
+    md->m = m;
+    md->st = *st;
+    for (int d = 0; d < 3; ++d) md->L[d] = (float)box[d];
+    md->half_c_self = c->p.coulomb ? 0.5f * c->p.coul_C * c->p.selfc : 0.f;
+    if (cudaStreamCreateWithFlags(&md->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&md->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&md->ev_join, cudaEventDisableTiming) != cudaSuccess ||
+        dalloc(&md->esum, 1) != PD_OK) {
+        set_error("pd_md_create: stream/event allocation failed");
+        pd_md_destroy(md);
+        return PD_ECUDA;
+    }
+    *out = md;
+    return PD_OK;
+}
+
+int pd_md_destroy(pd_md *md) {
+    if (!md) return PD_OK;
+    for (int k = 0; k < 2; ++k)
+        if (md->exec[k]) cudaGraphExecDestroy(md->exec[k]);
+    if (md->ev_fork) cudaEventDestroy(md->ev_fork);
+    if (md->ev_join) cudaEventDestroy(md->ev_join);
+    if (md->side) cudaStreamDestroy(md->side);
+    dfree(md->esum);
+    delete md;
+    return PD_OK;
+}
+
+// evaluate_forces_into_f!: eager list maintenance (host boundary) and one force pass without kicks.
+int pd_md_evaluate(pd_md *md, int energy, pd_stream_t sp) {
+    PD_CHECK(md, PD_EINVAL, "pd_md_evaluate: null handle");
+    cudaStream_t s = (cudaStream_t)sp;
+    pd_cluster *c = md->c;
+    pd_md_state &st = md->st;
+    const float *q = c->p.coulomb ? st.q : nullptr;
+    int rc, h[W_LEN];
+    if ((rc = cluster_decide_launch(c, st.x, st.y, st.z, 0, s))) return rc;
+    if ((rc = cluster_read_counts(c, h, s))) return rc;
+    if (h[W_BUILD] || !c->have_build) {
+        for (int attempt = 0; attempt < 8; ++attempt) {
+            if ((rc = cluster_build_launch(c, st.x, st.y, st.z, q, st.type, 0, s))) return rc;
+            if ((rc = cluster_read_counts(c, h, s))) return rc;
+            if (h[W_ERR] == 0) break;
+            if (h[W_ERR] == PD_ENONFINITE) {
+                set_error("Cluster-pair list: non-finite coordinates");
+                return PD_ENONFINITE;
+            }
+            if ((rc = pd_cluster_grow(c))) return rc;
+            // the graphs captured the old entry storage
+            for (int k = 0; k < 2; ++k)
+                if (md->exec[k]) {
+                    cudaGraphExecDestroy(md->exec[k]);
+                    md->exec[k] = nullptr;
+                }
+        }
+        PD_CHECK(h[W_ERR] == 0, PD_ECAPACITY, "outer list still overflows after growth");
+        c->have_build = true;
+        if ((rc = cluster_set_word(c, W_PRUNE, 1, s))) return rc;
+    } else {
+        if ((rc = pd_cluster_pack(c, st.x, st.y, st.z, q, st.type, sp))) return rc;
+    }
+    if ((rc = cluster_prune_launch(c, 1, s))) return rc;
+    return enqueue_forces(md, energy, 0.f, s);
+}
+
+int pd_md_step(pd_md *md, int nsteps, float dt, int energy_last, int use_graph, pd_stream_t sp) {
+    PD_CHECK(md, PD_EINVAL, "pd_md_step: null handle");
+    PD_CHECK(nsteps >= 0, PD_EINVAL, "pd_md_step: negative step count");
+    cudaStream_t s = (cudaStream_t)sp;
+    int rc;
+    if (!md->c->have_build) {
+        if ((rc = pd_md_evaluate(md, 0, sp))) return rc;
+    }
+    for (int k = 0; k < nsteps; ++k) {
+        const int energy = (energy_last && k == nsteps - 1) ? 1 : 0;
+        if (!use_graph) {
+            if ((rc = enqueue_step(md, dt, energy, s))) return rc;
+            continue;
+        }
+        if (!md->exec[energy] || md->exec_dt[energy] != dt || md->exec_stream[energy] != s) {
+            if (md->exec[energy]) {
+                cudaGraphExecDestroy(md->exec[energy]);
+                md->exec[energy] = nullptr;
+            }
+            PD_CHECK(s != nullptr, PD_EINVAL, "pd_md_step: graph replay needs a non-default stream");
+            cudaGraph_t g = nullptr;
+            PD_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            rc = enqueue_step(md, dt, energy, s);
+            cudaError_t e = cudaStreamEndCapture(s, &g);
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            PD_CHECK(e == cudaSuccess, PD_ECUDA, "step capture failed: %s", cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&md->exec[energy], g, 0);
+            cudaGraphDestroy(g);
+            PD_CHECK(e == cudaSuccess, PD_ECUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
+            md->exec_dt[energy] = dt;
+            md->exec_stream[energy] = s;
+        }
+        PD_CUDA(cudaGraphLaunch(md->exec[energy], s));
+    }
+    return PD_OK;
+}
+
+int pd_md_step_host(pd_md *md, float *host_xyz, float *host_v, int nsteps, float dt, double *epot_sum, pd_stream_t sp) {
+    PD_CHECK(md && host_xyz && host_v, PD_EINVAL, "pd_md_step_host: null argument");
+    cudaStream_t s = (cudaStream_t)sp;
+    pd_md_state &st = md->st;
+    const size_t nb = sizeof(float) * (size_t)st.n;
+    float *dx[3] = {st.x, st.y, st.z}, *dv[3] = {st.vx, st.vy, st.vz};
+    for (int d = 0; d < 3; ++d) {
+        PD_CUDA(cudaMemcpyAsync(dx[d], host_xyz + (size_t)d * st.n, nb, cudaMemcpyHostToDevice, s));
+        PD_CUDA(cudaMemcpyAsync(dv[d], host_v + (size_t)d * st.n, nb, cudaMemcpyHostToDevice, s));
+    }
+    int rc = pd_md_step(md, nsteps, dt, epot_sum ? 1 : 0, 1, sp);
+    if (rc) return rc;
+    if (epot_sum) {
+        PD_CUDA(cudaMemsetAsync(md->esum, 0, sizeof(double), s));
+        k_sum<<<std::min(1024, (st.n + 255) / 256), 256, 0, s>>>(st.epot, st.n, md->esum);
+        PD_LAUNCHED();
+        PD_CUDA(cudaMemcpyAsync(epot_sum, md->esum, sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    for (int d = 0; d < 3; ++d) {
+        PD_CUDA(cudaMemcpyAsync(host_xyz + (size_t)d * st.n, dx[d], nb, cudaMemcpyDeviceToHost, s));
+        PD_CUDA(cudaMemcpyAsync(host_v + (size_t)d * st.n, dv[d], nb, cudaMemcpyDeviceToHost, s));
+    }
+    PD_CUDA(cudaStreamSynchronize(s));
+    return PD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,374 @@
+"""Workflow API over the device engines.
+
+Mirrors the reference's public force/integrator/simulation API
+(src/workflow/Forces.jl:33-118, src/workflow/Electrostatics.jl:44-99,
+src/workflow/RunLoop.jl:403-457): force descriptors ``LennardJones``, ``WCA``,
+``PME``, ``PPPM``; list policies ``ClusterPairList`` and ``CellList``;
+``Integrator``, ``Stage``, ``ParticleSystem``, ``Simulation`` and the
+``run`` / ``step`` / ``evaluate_forces_into_f`` calls (``run!``, ``step!`` and
+``evaluate_forces_into_f!`` in Julia).  Every force evaluation and step runs on
+the GPU through libpdb200; there is no CPU path.
+
+Charged systems run on the cluster-pair backend (as the reference's user rule,
+src/simulation/ElectrostaticsCoupling.jl:76-86).  Uncharged 3D LJ/WCA systems
+also run on the cluster-pair list here.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import splits
+from .engine import ClusterPairEngine, DeviceEngine, ElectrostaticsSolver, ElectrostaticsSpec
+
+
+# ----------------------------------------------------------------------------- descriptors
+
+@dataclass
+class CellList:
+    """Neighbor-list policy (Forces.jl:33-44): list buffer (skin), row capacity, rebuild interval."""
+    buffer: float = 0.4
+    capacity: int = 96
+    rebuild_interval: int = 20
+
+
+@dataclass
+class ClusterPairList:
+    """Cluster-pair traversal (Forces.jl:46-57): list radius = cutoff + buffer, pruned to cutoff + prune_buffer."""
+    buffer: float = 0.1
+    prune_buffer: float | None = None
+
+
+@dataclass
+class LennardJones:
+    """Lennard-Jones force (Forces.jl:84-93); vdw_modifier 'none' truncates, 'potential_shift' shifts."""
+    epsilon: float | None = None
+    sigma: float | None = None
+    cutoff: float | None = None
+    pairs: str = "all"
+    mode: str = "standard"
+    pair_table: object = None
+    neighborlist: object = None
+    vdw_modifier: str = "none"
+
+
+@dataclass
+class WCA:
+    """Weeks-Chandler-Andersen force (Forces.jl:100-108): LJ cut at 2^(1/6) sigma, shifted by +epsilon."""
+    epsilon: float | None = None
+    sigma: float | None = None
+    cutoff: float | None = None
+    pairs: str = "all"
+    mode: str = "standard"
+    pair_table: object = None
+    neighborlist: object = None
+
+
+@dataclass
+class PME:
+    """Smooth particle-mesh Ewald with analytic differentiation (Electrostatics.jl:44-61)."""
+    coulomb_prefactor: float | None = None
+    real_cutoff: float | None = None
+    alpha: float | None = None
+    real_space_tolerance: float | None = None
+    mesh: tuple | None = None
+    mesh_spacing: float | None = None
+    order: int = 4
+    relative_permittivity: float = 1.0
+    net_charge: str = "error"
+    boundary: str = "tin_foil"
+    real_space_modifier: str = "none"
+    exclusions: object = "topology"
+    exclude_bonded: bool = False
+    scaled_pairs: tuple = ()
+    pairs: str = "neighborlist"
+    neighborlist: object = None
+
+
+@dataclass
+class PPPM:
+    """P3M with the optimal influence function, AD or ik differentiation (Electrostatics.jl:79-99)."""
+    coulomb_prefactor: float | None = None
+    real_cutoff: float | None = None
+    alpha: float | None = None
+    real_space_tolerance: float | None = None
+    mesh: tuple | None = None
+    mesh_spacing: float | None = None
+    order: int = 5
+    differentiation: str = "ad"
+    alias_order: int = 2
+    relative_permittivity: float = 1.0
+    net_charge: str = "error"
+    boundary: str = "tin_foil"
+    real_space_modifier: str = "none"
+    exclusions: object = "topology"
+    exclude_bonded: bool = False
+    scaled_pairs: tuple = ()
+    pairs: str = "neighborlist"
+    neighborlist: object = None
+
+
+def electrostatics_spec(f) -> ElectrostaticsSpec:
+    """Validated solver spec of a PME/PPPM descriptor."""
+    if f.coulomb_prefactor is None or f.real_cutoff is None:
+        raise ValueError(f"{type(f).__name__} requires coulomb_prefactor and real_cutoff.")
+    if f.boundary != "tin_foil":
+        raise ValueError(f"Only conducting (tin-foil) boundary conditions are implemented; got {f.boundary}.")
+    if (f.alpha is None) == (f.real_space_tolerance is None):
+        raise ValueError("Provide exactly one of alpha and real_space_tolerance.")
+    if f.exclusions not in ("topology", None, ()) or f.exclude_bonded or len(f.scaled_pairs) > 0:
+        raise NotImplementedError("Coulomb exceptions are not supported by this build of the cluster-pair path.")
+    alpha = float(f.alpha) if f.alpha is not None else splits.alpha_from_tolerance(f.real_cutoff,
+                                                                                    f.real_space_tolerance)
+    if isinstance(f, PME):
+        influence = "spme"
+        alias = 2
+    else:
+        if f.differentiation not in ("ad", "ik"):
+            raise ValueError("differentiation must be ad or ik.")
+        influence = "p3m_ad" if f.differentiation == "ad" else "p3m_ik"
+        alias = f.alias_order
+    return ElectrostaticsSpec(coulomb_prefactor=float(f.coulomb_prefactor), real_cutoff=float(f.real_cutoff),
+                              alpha=alpha, influence=influence, order=int(f.order), mesh=f.mesh,
+                              mesh_spacing=f.mesh_spacing, alias_order=alias,
+                              relative_permittivity=float(f.relative_permittivity), net_charge=f.net_charge,
+                              real_space_modifier=f.real_space_modifier)
+
+
+@dataclass
+class ConstantVolume:
+    """NVE velocity Verlet on a group (the whole system)."""
+    group: object = None
+
+
+@dataclass
+class Integrator:
+    dt: float
+    forces: list = field(default_factory=list)
+    methods: list = field(default_factory=lambda: [ConstantVolume()])
+
+
+@dataclass
+class Stage:
+    """A run stage (RunLoop.jl): name, steps, and how often energies are evaluated (0 = last step only)."""
+    name: str = "run"
+    steps: int = 0
+    energy_every: int = 0
+    progress: bool = False
+
+
+class ParticleSystem:
+    """Positions (N x 3), box, types, per-type masses and charges (host data)."""
+
+    def __init__(self, positions, box, types=("A",), typeids=None, masses=None, charges=None, velocities=None):
+        self.positions = np.asarray(positions, float).reshape(-1, 3)
+        n = len(self.positions)
+        self.box = tuple(float(b) for b in box)
+        if len(self.box) != 3:
+            raise ValueError("this build supports 3D periodic boxes")
+        self.types = [str(t) for t in types]
+        self.typeids = np.ones(n, np.int32) if typeids is None else np.asarray(typeids, np.int32)
+
+        def per_particle(v, default):
+            if v is None:
+                return np.full(n, default, float)
+            if isinstance(v, dict):
+                return np.array([float(v[self.types[t - 1]]) for t in self.typeids])
+            a = np.asarray(v, float)
+            return np.full(n, float(a)) if a.ndim == 0 else a.reshape(n)
+
+        self.masses = per_particle(masses, 1.0)
+        self.charges = None if charges is None else per_particle(charges, 0.0)
+        self.velocities = None if velocities is None else np.asarray(velocities, float).reshape(n, 3)
+
+    @property
+    def n(self) -> int:
+        return len(self.positions)
+
+
+# ----------------------------------------------------------------------------- state
+
+class SimulationState:
+    """Device state of one system and its engines (the SimulationState of the reference)."""
+
+    def __init__(self, system: ParticleSystem, forces, dt: float, device="cuda"):
+        if not torch.cuda.is_available():
+            raise RuntimeError("libpdb200 needs a CUDA device; there is no CPU force path")
+        self.dev = torch.device(device)
+        n = system.n
+        self.n = n
+        self.box = system.box
+        f32 = dict(dtype=torch.float32, device=self.dev)
+        L = np.array(self.box)
+        pos = system.positions - L * np.floor(system.positions / L + 0.5)   # centred image
+        self.x, self.y, self.z = (torch.tensor(pos[:, d], **f32) for d in range(3))
+        v = system.velocities if system.velocities is not None else np.zeros((n, 3))
+        self.vx, self.vy, self.vz = (torch.tensor(v[:, d], **f32) for d in range(3))
+        self.fx, self.fy, self.fz = (torch.zeros(n, **f32) for _ in range(3))
+        self.epot = torch.zeros(n, **f32)
+        self.vir6 = torch.zeros((n, 6), **f32)
+        self.vglobal = torch.zeros(6, **f32)
+        self.q = torch.tensor(system.charges, **f32) if system.charges is not None else None
+        self.typ = torch.tensor(system.typeids, dtype=torch.int32, device=self.dev)
+        self.inv_mass = torch.tensor(1.0 / system.masses, **f32)
+        self.masses = system.masses
+        self.dt = float(dt)
+        self.step_count = 0
+        self.stream = torch.cuda.Stream(device=self.dev)
+        self._compile(system, forces)
+
+    def _compile(self, system, forces):
+        vdw = [f for f in forces if isinstance(f, (LennardJones, WCA))]
+        elec = [f for f in forces if isinstance(f, (PME, PPPM))]
+        if len(vdw) > 1 or len(elec) > 1:
+            raise ValueError("at most one short-range vdW force and one electrostatics force")
+        lj = None
+        rlj = 0.0
+        nl = None
+        if vdw:
+            f = vdw[0]
+            if f.mode != "standard":
+                raise ValueError(f"Only mode=standard is supported for {type(f).__name__}.")
+            if f.epsilon is None or f.sigma is None:
+                raise ValueError(f"{type(f).__name__} requires epsilon and sigma.")
+            eps, sig = float(f.epsilon), float(f.sigma)
+            if isinstance(f, WCA):
+                rc = sig * splits.WCA_RC_FACTOR if f.cutoff is None else float(f.cutoff)
+                table = splits.lj_type_table(sig, eps, rc, wca=True)
+            else:
+                if f.cutoff is None:
+                    raise ValueError("LennardJones requires an explicit cutoff.")
+                rc = float(f.cutoff)
+                table = splits.lj_type_table(sig, eps, rc, shift=f.vdw_modifier == "potential_shift")
+            lj = dict(table=table)
+            rlj = rc
+            nl = f.neighborlist
+        self.solver = None
+        coul = None
+        selfc = 0.0
+        rcoul = 0.0
+        if elec:
+            if self.q is None:
+                raise ValueError("electrostatics requires per-particle charges")
+            spec = electrostatics_spec(elec[0])
+            self.solver = ElectrostaticsSolver(spec, self.box, system.charges, nmax=self.n)
+            coul = self.solver.coulomb_polynomial()
+            selfc = self.solver.selfc
+            rcoul = spec.real_cutoff
+            if nl is None:
+                nl = elec[0].neighborlist
+        rmax = max(rlj, rcoul)
+        if rmax <= 0:
+            raise ValueError("The cluster-pair backend needs a vdW term or an electrostatics solver.")
+        if isinstance(nl, ClusterPairList):
+            skin = nl.buffer
+            pb = nl.prune_buffer if nl.prune_buffer is not None else 0.5 * skin
+        else:
+            skin = (nl.buffer if isinstance(nl, CellList) else CellList().buffer)
+            pb = 0.5 * skin
+        # small boxes: the list radius stays below half the box (_charged_backend!, ElectrostaticsCoupling.jl:76-86)
+        skin = min(skin, max(0.999 * (min(self.box) / 2 - rmax), 0.0))
+        pb = min(pb, skin)
+        self.cluster = ClusterPairEngine(self.n, self.box, rmax=rmax, skin=skin, prune_buffer=pb, lj=lj,
+                                         coulomb=coul, selfc=selfc)
+        state = dict(x=self.x, y=self.y, z=self.z, vx=self.vx, vy=self.vy, vz=self.vz, fx=self.fx, fy=self.fy,
+                     fz=self.fz, q=self.q if coul is not None else None, type=self.typ, inv_mass=self.inv_mass,
+                     epot=self.epot, vir6=self.vir6, vglobal=self.vglobal)
+        self.engine = DeviceEngine(self.cluster, self.solver, state, self.box)
+        self.forces_valid = False
+
+    # -- force evaluation
+    def evaluate_forces_into_f(self, energy: bool = False):
+        """evaluate_forces_into_f!(st, energy) (ForceEvaluation.jl:40-44)."""
+        with torch.cuda.stream(self.stream):
+            if self.solver is None:
+                self.vglobal.zero_()
+            self.engine.evaluate(energy=energy, stream=self.stream)
+        self.stream.synchronize()
+        self.forces_valid = True
+
+    def step(self, nsteps: int = 1, energy_last: bool = False, use_graph: bool = True):
+        if not self.forces_valid:
+            self.evaluate_forces_into_f(False)
+        self.engine.step(nsteps, self.dt, energy_last=energy_last, use_graph=use_graph, stream=self.stream)
+        self.step_count += nsteps
+
+    def synchronize(self):
+        self.stream.synchronize()
+
+    # -- observables (FP64 host reductions)
+    def potential_energy(self) -> float:
+        self.synchronize()
+        return float(self.epot.double().sum())
+
+    def kinetic_energy(self) -> float:
+        self.synchronize()
+        v2 = (self.vx.double() ** 2 + self.vy.double() ** 2 + self.vz.double() ** 2).cpu().numpy()
+        return 0.5 * float((self.masses * v2).sum())
+
+    def virial_tensor(self) -> dict:
+        """Pair virial rows plus the mesh virial (xx, yy, zz, xy, xz, yz)."""
+        self.synchronize()
+        w = self.vir6.double().sum(0).cpu().numpy() + self.vglobal.double().cpu().numpy()
+        return dict(zip(("xx", "yy", "zz", "xy", "xz", "yz"), w))
+
+    def forces(self) -> np.ndarray:
+        self.synchronize()
+        return torch.stack([self.fx, self.fy, self.fz], 1).double().cpu().numpy()
+
+    def positions(self) -> np.ndarray:
+        self.synchronize()
+        return torch.stack([self.x, self.y, self.z], 1).double().cpu().numpy()
+
+
+class Simulation:
+    """System + integrator on one GPU (the reference's Simulation, src/workflow)."""
+
+    def __init__(self, system: ParticleSystem, integrator: Integrator, precision="f32", seed: int = 0):
+        if precision not in ("f32", np.float32, "Float32"):
+            raise ValueError("this build runs the Float32 force path")
+        for m in integrator.methods:
+            if not isinstance(m, ConstantVolume):
+                raise NotImplementedError(f"integration method {type(m).__name__} is not part of this build")
+        self.system = system
+        self.integrator = integrator
+        self.seed = seed
+        self.state = SimulationState(system, integrator.forces, integrator.dt)
+
+
+def state(sim: Simulation) -> SimulationState:
+    return sim.state
+
+
+def run(sim: Simulation, stage: Stage) -> Simulation:
+    """run!(sim, stage) (RunLoop.jl:403-457): stage.steps NVE steps on the device."""
+    st = sim.state
+    if stage.steps <= 0:
+        return sim
+    every = stage.energy_every
+    if every and every > 0:
+        done = 0
+        while done < stage.steps:
+            k = min(every, stage.steps - done)
+            st.step(k, energy_last=True)
+            done += k
+    else:
+        st.step(stage.steps, energy_last=True)
+    st.synchronize()
+    return sim
+
+
+def step(sim_or_state, compute_energy: bool = False):
+    """step!(st, integ, dt; compute_energy) (SteppingEngine.jl:23)."""
+    st = sim_or_state.state if isinstance(sim_or_state, Simulation) else sim_or_state
+    st.step(1, energy_last=compute_energy)
+    return st
+
+
+def evaluate_forces_into_f(sim_or_state, energy: bool = False):
+    st = sim_or_state.state if isinstance(sim_or_state, Simulation) else sim_or_state
+    st.evaluate_forces_into_f(energy)
+    return st

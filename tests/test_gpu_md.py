@@ -1,0 +1,127 @@
+"""Whole-path checks on the LJ + PME ionic melt: workflow API, step engine, CUDA graph, full size."""
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _melt_sim(pd, n, seed=7, kind="PME", buffer=1.0, prune=0.3, T=1200.0):
+    L = (n / 0.0375) ** (1 / 3)
+    pos, q, box = pd.synthetic.ionic_melt(n, L, 2.2, seed=seed)
+    m = pd.synthetic.melt_masses(q)
+    v = pd.synthetic.maxwell_boltzmann(m, T, seed=seed + 1, kB=pd.synthetic.KB_EV)
+    system = pd.ParticleSystem(pos, box, types=["Na", "Cl"], typeids=np.where(q > 0, 1, 2), masses=m, charges=q,
+                               velocities=v)
+    lj = pd.LennardJones(epsilon=0.01, sigma=2.8, cutoff=9.0, pairs="neighborlist",
+                         neighborlist=pd.ClusterPairList(buffer=buffer, prune_buffer=prune))
+    if kind == "PME":
+        el = pd.PME(coulomb_prefactor=pd.synthetic.COULOMB_EV_A, real_cutoff=9.0, real_space_tolerance=1e-5,
+                    mesh_spacing=1.0, order=5)
+    else:
+        el = pd.PPPM(coulomb_prefactor=pd.synthetic.COULOMB_EV_A, real_cutoff=9.0, real_space_tolerance=1e-5,
+                     mesh_spacing=1.0, order=5, differentiation="ad")
+    dt = 1.0 / pd.synthetic.TIME_UNIT_FS
+    sim = pd.Simulation(system, pd.Integrator(dt=dt, forces=[lj, el]))
+    return sim, q, box
+
+
+def _oracle_forces(pd, ora, sim, q, box, kind="spme"):
+    st = sim.state
+    return ora.pme_total(st.positions(), q, box, C=pd.synthetic.COULOMB_EV_A, alpha=st.solver.spec.alpha, rc=9.0,
+                         K=st.solver.mesh, P=5, kind=kind, lj=dict(sigma=2.8, eps=0.01, rc=9.0))
+
+
+@pytest.mark.parametrize("kind", ["PME", "PPPM"])
+def test_melt_forces_energy_virial(pd, ora, cuda, kind):
+    sim, q, box = _melt_sim(pd, 4000, kind=kind)
+    pd.evaluate_forces_into_f(sim, energy=True)
+    st = sim.state
+    ref = _oracle_forces(pd, ora, sim, q, box, kind="spme" if kind == "PME" else "p3m_ad")
+    F = st.forces()
+    rel = np.linalg.norm(F - ref["F"]) / np.linalg.norm(ref["F"])
+    assert rel < 1e-5, rel                              # the north-star parity bound (relative RMS)
+    E = st.potential_energy()
+    assert abs(E - ref["Etot"]) / abs(ref["Etot"]) < 1e-5
+    W = st.virial_tensor()
+    W6 = np.array([W[k] for k in ("xx", "yy", "zz", "xy", "xz", "yz")])
+    assert np.max(np.abs(W6 - ref["W"])) / abs(ref["W"][:3].sum()) < 1e-4
+
+
+def test_nve_graph_equals_eager(pd, cuda):
+    sa, q, box = _melt_sim(pd, 4000, seed=21)
+    sb, _, _ = _melt_sim(pd, 4000, seed=21)
+    sa.state.step(50, energy_last=True, use_graph=True)
+    sb.state.step(50, energy_last=True, use_graph=False)
+    Ra, Rb = sa.state.positions(), sb.state.positions()
+    D = Ra - Rb
+    D -= np.array(box) * np.round(D / np.array(box))
+    assert np.max(np.abs(D)) < 1e-3        # FP32 atomics reorder sums; trajectories agree closely
+    s = sa.state.cluster.statistics()
+    assert s["builds"] >= 1 and s["prunes"] > s["builds"] and s["error"] == 0
+
+
+def test_nve_energy_error_is_second_order(pd, cuda):
+    # The random-placement start collapses and heats the melt to ~2e4 K within 50 fs, so velocity Verlet's
+    # energy error is visible; it must shrink as dt^2 (a list or force bug would not).
+    drift = []
+    for dt_fs in (0.5, 0.25):
+        sim, q, box = _melt_sim(pd, 4000, seed=21)
+        st = sim.state
+        st.dt = dt_fs / pd.synthetic.TIME_UNIT_FS
+        pd.evaluate_forces_into_f(sim, energy=True)
+        E0 = st.potential_energy() + st.kinetic_energy()
+        st.step(int(round(30 / dt_fs)), energy_last=True)
+        drift.append(abs(st.potential_energy() + st.kinetic_energy() - E0) / abs(E0))
+    assert drift[1] < 5e-3
+    assert 2.5 < drift[0] / drift[1] < 6.0, drift
+
+
+def test_trajectory_matches_cpu_oracle(pd, ora, cuda):
+    import torch
+    sim, q, box = _melt_sim(pd, 2000, seed=5)
+    st = sim.state
+    pd.evaluate_forces_into_f(sim)
+    vel = torch.stack([st.vx, st.vy, st.vz], 1).double().cpu().numpy()
+    cpu = ora.CpuMelt(st.positions(), vel, q, pd.synthetic.melt_masses(q), box, C=pd.synthetic.COULOMB_EV_A,
+                      alpha=st.solver.spec.alpha, rc=9.0, K=st.solver.mesh, P=5, lj=dict(sigma=2.8, eps=0.01, rc=9.0))
+    for _ in range(10):
+        cpu.step(st.dt)
+    st.step(10)
+    D = st.positions() - cpu.pos
+    D -= np.array(box) * np.round(D / np.array(box))
+    assert np.max(np.abs(D)) < 1e-4
+
+
+def test_step_through_host_buffers(pd, cuda):
+    sim, q, box = _melt_sim(pd, 2000, seed=4)
+    st = sim.state
+    pd.evaluate_forces_into_f(sim)
+    xyz = np.ascontiguousarray(np.concatenate([st.x.cpu().numpy(), st.y.cpu().numpy(), st.z.cpu().numpy()]))
+    v = np.ascontiguousarray(np.concatenate([st.vx.cpu().numpy(), st.vy.cpu().numpy(), st.vz.cpu().numpy()]))
+    e = st.engine.step_host(xyz, v, 3, st.dt, stream=st.stream)
+    assert math.isfinite(e)
+    assert np.allclose(xyz[:2000], st.x.cpu().numpy())
+    assert abs(e - st.potential_energy()) < 1e-6 * abs(e)
+
+
+@pytest.mark.slow
+def test_full_size_melt(pd, ora, cuda):
+    # 64 000 ions at the benchmark shape: forces against the oracle and size-independent properties
+    sim, q, box = _melt_sim(pd, 64000, seed=2026)
+    pd.evaluate_forces_into_f(sim, energy=True)
+    st = sim.state
+    ref = _oracle_forces(pd, ora, sim, q, box)
+    F = st.forces()
+    rel = np.linalg.norm(F - ref["F"]) / np.linalg.norm(ref["F"])
+    assert rel < 1e-5, rel
+    assert abs(st.potential_energy() - ref["Etot"]) / abs(ref["Etot"]) < 1e-5
+    # net force is a mesh-convergence quantity, small against the force scale
+    assert np.linalg.norm(F.sum(0)) < 1e-3 * np.linalg.norm(F)
+    E0 = st.potential_energy() + st.kinetic_energy()
+    pd.run(sim, pd.Stage(steps=100))
+    E1 = st.potential_energy() + st.kinetic_energy()
+    assert abs(E1 - E0) / abs(E0) < 1e-3
+    s = st.cluster.statistics()
+    assert s["error"] == 0
