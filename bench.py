@@ -56,9 +56,9 @@ def make_system(pd):
     return pos, q, m, v, box
 
 
-def forces(pd):
+def forces(pd, buffer=BUFFER, prune=PRUNE):
     lj = pd.LennardJones(epsilon=0.01, sigma=2.8, cutoff=RC, pairs="neighborlist",
-                         neighborlist=pd.ClusterPairList(buffer=BUFFER, prune_buffer=PRUNE))
+                         neighborlist=pd.ClusterPairList(buffer=buffer, prune_buffer=prune))
     el = pd.PME(coulomb_prefactor=pd.synthetic.COULOMB_EV_A, real_cutoff=RC, real_space_tolerance=1e-5,
                 mesh_spacing=1.0, order=5)
     return [lj, el]
@@ -82,7 +82,7 @@ class ClockSampler:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -264,6 +264,8 @@ def main():
     ap.add_argument("--impl", default="pdb200", choices=["pdb200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-flush", action="store_true", help="(diagnostic) do not flush L2 between steps")
+    ap.add_argument("--buffer", type=float, default=BUFFER, help="cluster list buffer (Angstrom)")
+    ap.add_argument("--prune", type=float, default=PRUNE, help="prune buffer (Angstrom)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -284,18 +286,22 @@ def main():
     system = pd.ParticleSystem(pos, box, types=["Na", "Cl"], typeids=np.where(q > 0, 1, 2), masses=m, charges=q,
                                velocities=v)
     dt = DT_FS / pd.synthetic.TIME_UNIT_FS
-    sim = pd.Simulation(system, pd.Integrator(dt=dt, forces=forces(pd)))
+    sim = pd.Simulation(system, pd.Integrator(dt=dt, forces=forces(pd, args.buffer, args.prune)))
     st = sim.state
     s = st.stream
     pd.evaluate_forces_into_f(sim, energy=False)
-    # kernels one step launches (eager launch count of the same sequence the graph holds)
+    # kernels of one eager step: the always-run part plus the build and prune kernels, which the captured
+    # graph launches only inside its conditional nodes on steps that build or prune
     c0 = L.pd_launch_count()
     st.step(1, use_graph=False)
     st.synchronize()
-    kernels_per_step = int(L.pd_launch_count() - c0)
+    kernels_eager = int(L.pd_launch_count() - c0)
+    KERNELS_BUILD, KERNELS_PRUNE = 9, 1
+    kernels_always = kernels_eager - KERNELS_BUILD - KERNELS_PRUNE
     # warm-up (graph capture on the first replay)
     st.step(args.warmup, use_graph=True)
     st.synchronize()
+    pre = st.cluster.statistics()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -319,8 +325,12 @@ def main():
     if stats["error"]:
         raise RuntimeError(f"cluster list error {stats['error']} during the run")
     clocks = clk.summary()
+    timed_builds = stats["builds"] - pre["builds"]
+    timed_prunes = stats["prunes"] - pre["prunes"]
+    gpu_launches = kernels_always * args.steps + KERNELS_BUILD * timed_builds + KERNELS_PRUNE * timed_prunes
 
-    # end to end through the C ABI with pinned host buffers (H2D state in, D2H state and energy out per step)
+    # end to end through the C ABI with pinned host buffers: every step copies the state (x, v) in from
+    # pinned host memory and copies the stepped state back (the step's result)
     n = st.n
     hx = torch.empty(3 * n, dtype=torch.float32, pin_memory=True).numpy()
     hv = torch.empty(3 * n, dtype=torch.float32, pin_memory=True).numpy()
@@ -328,11 +338,11 @@ def main():
     hv[:] = torch.cat([st.vx, st.vy, st.vz]).cpu().numpy()
     e2e_steps = max(20, args.steps // 4)
     for _ in range(3):
-        st.engine.step_host(hx, hv, 1, dt, stream=s)
+        st.engine.step_host(hx, hv, 1, dt, stream=s, energy=False)
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        st.engine.step_host(hx, hv, 1, dt, stream=s)
+        st.engine.step_host(hx, hv, 1, dt, stream=s, energy=False)
     e2e_ms = 1000.0 * (time.perf_counter() - t0) / e2e_steps
     e2e_ms = max_over_ranks(world, e2e_ms)
 
@@ -369,13 +379,15 @@ def main():
                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ionic melt, 1200 K start)",
                "config": {"workload": "ionic melt N=64000 (L=119.5 A) LJ+SPME r_c=9 A, 120^3 order 5, NVE dt=1 fs",
                           "form": "plain (learned coarse-mesh form not built)", "parallelism": f"replicas x{world}",
-                          "list_buffer_A": BUFFER, "prune_buffer_A": PRUNE,
+                          "list_buffer_A": args.buffer, "prune_buffer_A": args.prune,
                           "l2": "flushed (256 MiB write) before every timed step" if not args.no_flush else "warm",
-                          "builds": stats["builds"], "prunes": stats["prunes"]},
+                          "timed_builds": timed_builds, "timed_prunes": timed_prunes},
                "roofline": roofline, "cpu_baseline": cpu,
                "e2e": {"value": world * ns_per_day(e2e_ms), "unit": "ns/day", "h2d_bytes_per_step": 24 * n,
-                       "d2h_bytes_per_step": 24 * n + 8, "ms_per_step": e2e_ms},
-               "gpu_launches": kernels_per_step * args.steps, "kernels_per_step": kernels_per_step,
+                       "d2h_bytes_per_step": 24 * n, "ms_per_step": e2e_ms},
+               "gpu_launches": gpu_launches,
+               "kernels": {"every_step": kernels_always, "per_build": KERNELS_BUILD, "per_prune": KERNELS_PRUNE,
+                           "cufft_per_step": "2 transforms (library kernels, not counted)"},
                "clocks": clocks}
         print(json.dumps(out))
     if world > 1:

@@ -56,7 +56,7 @@ def _load():
         L.ora_cluster_geometry.restype = C.c_int
         L.ora_cluster_build.argtypes = [C.c_int, _f, _f, _f, _d, C.c_double, C.c_int, _i, _i, _u]
         L.ora_cluster_build.restype = C.c_int
-        L.ora_cluster_prune.argtypes = [C.c_int, _f, _i, _u, _d, C.c_double, _u, _i]
+        L.ora_cluster_prune.argtypes = [C.c_int, _f, _i, _u, _d, C.c_double, C.c_double, _u, _i]
         L.ora_force_coordinate.argtypes = [C.c_float, C.c_float]
         L.ora_force_coordinate.restype = C.c_float
         _lib = L
@@ -296,15 +296,18 @@ def cluster_build(pos32, box, rlist):
     return dict(ns=ns, perm=perm, scio=scio[:ns + 1].copy(), cjo=cjo[:ne].copy(), geom=g)
 
 
-def cluster_prune(ns, xq, scio, cjo, box, rp):
-    """Prune + compaction (Kernels.jl:349-394, List.jl:719-759): working entries per super-cluster."""
+def cluster_prune(ns, xq, scio, cjo, box, rp, pbuf):
+    """Prune + compaction (Kernels.jl:349-394, List.jl:719-759): working entries per super-cluster.
+
+    The second word of an entry holds the two 8-bit warp masks and, in bit 16, the periodic-path
+    mark (an atom within pbuf/2 of a face or a separation component above L/2 - pbuf)."""
     L = _load()
     xq = np.ascontiguousarray(xq, np.float32)
     scio = np.ascontiguousarray(scio, np.int32)
     cjo = np.ascontiguousarray(cjo, np.uint32)
     cjw = np.zeros((max(len(cjo), 1), 2), np.uint32)
     nw = np.zeros(max(ns, 1), np.int32)
-    L.ora_cluster_prune(int(ns), _p(xq, _f), _p(scio, _i), _p(cjo, _u), _p(_box(box)), float(rp), _p(cjw, _u),
+    L.ora_cluster_prune(int(ns), _p(xq, _f), _p(scio, _i), _p(cjo, _u), _p(_box(box)), float(rp), float(pbuf), _p(cjw, _u),
                         _p(nw, _i))
     return cjw[:len(cjo)], nw[:ns]
 

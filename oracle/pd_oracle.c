@@ -890,8 +890,17 @@ float ora_force_coordinate(float x, float L) {
  * coordinates and charges (4 floats per slot, NaN padding).  cjw receives (cj, mask_lo | mask_hi << 8)
  * pairs at the super-cluster's outer offset; nw the kept count per super-cluster. */
 void ora_cluster_prune(int NS, const float *xq, const int *scio, const uint32_t *cjo, const double box[3], double rp,
-                       uint32_t *cjw, int *nw) {
+                       double pbuf, uint32_t *cjw, int *nw) {
     const float L[3] = {(float)box[0], (float)box[1], (float)box[2]};
+    /* periodic-path mark (bit 16): an atom within half the prune buffer of a face, or a separation
+     * component above L/2 - prune buffer, among the tile's atoms */
+    const float pb = (float)pbuf;
+    float wl[3], dl[3];
+    for (int k = 0; k < 3; ++k) {
+        const float hL = 0.5f * L[k], hp = 0.5f * pb;
+        wl[k] = hL - hp;
+        dl[k] = hL - pb;
+    }
     const float iL[3] = {1.0f / L[0], 1.0f / L[1], 1.0f / L[2]};
     const float Lmax = fmaxf(L[0], fmaxf(L[1], L[2]));
     const float rpf = (float)rp;
@@ -909,6 +918,19 @@ void ora_cluster_prune(int NS, const float *xq, const int *scio, const uint32_t 
             const int cj = (int)(cjo[e] >> 8);
             const uint32_t imask = cjo[e] & 0xffu;
             uint32_t m[2] = {0, 0};
+            int mark = 0;
+            for (int a = 0; a < 8; ++a) {
+                if (!((imask >> a) & 1u)) continue;
+                for (int tj = 0; tj < 8; ++tj)
+                    for (int ti = 0; ti < 8; ++ti) {
+                        const float *pi = xq + 4 * (size_t)(64 * S + 8 * a + ti);
+                        const float *pj = xq + 4 * (size_t)(8 * cj + tj);
+                        for (int k = 0; k < 3; ++k) {
+                            const float r = pi[k] - pj[k];
+                            if (fabsf(pj[k]) > wl[k] || fabsf(pi[k]) > wl[k] || fabsf(r) > dl[k]) mark = 1;
+                        }
+                    }
+            }
             for (int h = 0; h < 2; ++h)
                 for (int a = 0; a < 8; ++a) {
                     if (!((imask >> a) & 1u)) continue;
@@ -930,7 +952,7 @@ void ora_cluster_prune(int NS, const float *xq, const int *scio, const uint32_t 
                 }
             if (m[0] | m[1]) {
                 cjw[2 * (size_t)(scio[S] + keep)] = (uint32_t)cj;
-                cjw[2 * (size_t)(scio[S] + keep) + 1] = m[0] | (m[1] << 8);
+                cjw[2 * (size_t)(scio[S] + keep) + 1] = m[0] | (m[1] << 8) | ((uint32_t)mark << 16);
                 ++keep;
             }
         }

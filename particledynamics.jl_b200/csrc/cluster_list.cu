@@ -453,17 +453,22 @@ __global__ void __launch_bounds__(1024) k_entry_scan(const int *__restrict__ cnt
 // entries are written in order at the start of the super-cluster's own outer
 // segment, so no global scan is needed.  The prune reference coordinates of
 // the super-cluster's particles are refreshed here.
+//
+// Bit 16 of a kept entry's mask word marks tiles that may need the periodic
+// (compensated) difference before the next prune: an atom within half the
+// prune buffer of a box face (it can wrap before the displacement trigger
+// forces a new prune) or a separation component above L/2 - prune_buffer.
+// Unmarked tiles take the plain difference in the pair kernel.
 __global__ void __launch_bounds__(256) k_prune(const float4 *__restrict__ xq, const int *__restrict__ perm,
                                                const int *__restrict__ scio, const uint32_t *__restrict__ cjo,
                                                uint2 *__restrict__ cjw, int *__restrict__ nw,
                                                float4 *__restrict__ ref_prune, float Lx, float Ly, float Lz,
-                                               float rp2, int *__restrict__ counts, int gated) {
+                                               float rp2, float pbuf, int *__restrict__ counts, int gated) {
     if (gated && counts[W_PRUNE] == 0) return;
     if (counts[W_ERR] != 0) return;
     const int S = blockIdx.x;
     if (S >= counts[W_NS]) return;
     __shared__ float4 si[SUPER];
-    __shared__ uint32_t sm[4][2];
     const int t = threadIdx.x;
     if (t < SUPER) {
         float4 v = xq[S * SUPER + t];
@@ -480,43 +485,64 @@ __global__ void __launch_bounds__(256) k_prune(const float4 *__restrict__ xq, co
     const int w = t >> 5, lane = t & 31;
     const int g = w >> 1, h = w & 1;
     const int ti = lane & 7, tj = h * 4 + (lane >> 3);
+    const float wlx = __fsub_rn(__fmul_rn(0.5f, Lx), __fmul_rn(0.5f, pbuf));
+    const float wly = __fsub_rn(__fmul_rn(0.5f, Ly), __fmul_rn(0.5f, pbuf));
+    const float wlz = __fsub_rn(__fmul_rn(0.5f, Lz), __fmul_rn(0.5f, pbuf));
+    const float dlx = __fsub_rn(__fmul_rn(0.5f, Lx), pbuf);
+    const float dly = __fsub_rn(__fmul_rn(0.5f, Ly), pbuf);
+    const float dlz = __fsub_rn(__fmul_rn(0.5f, Lz), pbuf);
     const int e0 = scio[S], e1 = scio[S + 1];
-    int nkeep = 0;  // meaningful in thread 0
-    for (int eb = e0; eb < e1; eb += 4) {
-        const int e = eb + g;
-        uint32_t pm = 0;
-        if (e < e1) {
+    // Chunks of PCH entries: each warp pair evaluates every fourth entry of the chunk and
+    // records its j-half mask; warp 0 then compacts the chunk in order with ballots.
+    constexpr int PCH = 256;
+    __shared__ uint32_t sm_ent[PCH];
+    __shared__ uint32_t sm_half[2][PCH];
+    int nkeep = 0;  // running kept count (warp 0)
+    for (int cb = e0; cb < e1; cb += PCH) {
+        const int ce = min(e1, cb + PCH);
+        for (int e = cb + g; e < ce; e += 4) {
+            uint32_t pm = 0;
+            bool pbc = false;
             const uint32_t ent = cjo[e];
             const int cj = (int)(ent >> 8);
             const uint32_t imask = ent & 0xffu;
             const float4 pj = xq[cj * 8 + tj];
+            const bool jnear = fabsf(pj.x) > wlx || fabsf(pj.y) > wly || fabsf(pj.z) > wlz;
 #pragma unroll
             for (int a = 0; a < 8; ++a) {
                 if ((imask >> a) & 1u) {
                     const float4 p = si[a * 8 + ti];
-                    float dx = p.x - pj.x, dy = p.y - pj.y, dz = p.z - pj.z;
-                    dx = fmaf(-Lx, rintf(dx * iLx), dx);
-                    dy = fmaf(-Ly, rintf(dy * iLy), dy);
-                    dz = fmaf(-Lz, rintf(dz * iLz), dz);
+                    const float rx = p.x - pj.x, ry = p.y - pj.y, rz = p.z - pj.z;
+                    pbc = pbc || jnear || fabsf(p.x) > wlx || fabsf(p.y) > wly || fabsf(p.z) > wlz ||
+                          fabsf(rx) > dlx || fabsf(ry) > dly || fabsf(rz) > dlz;
+                    const float dx = fmaf(-Lx, rintf(rx * iLx), rx);
+                    const float dy = fmaf(-Ly, rintf(ry * iLy), ry);
+                    const float dz = fmaf(-Lz, rintf(rz * iLz), rz);
                     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                     const bool ok = ((cj != S * 8 + a) || (tj > ti)) && (r2 < __int_as_float(0x7f800000));
                     const bool keep = __any_sync(0xffffffffu, ok && r2 < rp2w);
                     pm |= keep ? (1u << a) : 0u;
                 }
             }
+            pbc = __any_sync(0xffffffffu, pbc);
+            if (lane == 0) {
+                sm_half[h][e - cb] = pm | (pbc ? 0x100u : 0u);
+                if (h == 0) sm_ent[e - cb] = (uint32_t)cj;
+            }
         }
-        if (lane == 0) sm[g][h] = pm;
         __syncthreads();
-        if (t == 0) {
-            for (int gg = 0; gg < 4; ++gg) {
-                const int ee = eb + gg;
-                if (ee < e1) {
-                    const uint32_t m = sm[gg][0] | (sm[gg][1] << 8);
-                    if (m) {
-                        cjw[e0 + nkeep] = make_uint2(cjo[ee] >> 8, m);
-                        ++nkeep;
-                    }
+        if (w == 0) {
+            for (int k = lane; k < ((ce - cb + 31) & ~31); k += 32) {
+                uint32_t m = 0, cj = 0;
+                if (k < ce - cb) {
+                    const uint32_t a0 = sm_half[0][k], a1 = sm_half[1][k];
+                    m = (a0 & 0xffu) | ((a1 & 0xffu) << 8) | (((a0 | a1) & 0x100u) << 8);
+                    cj = sm_ent[k];
                 }
+                const bool live = (m & 0xffffu) != 0;
+                const unsigned bal = __ballot_sync(0xffffffffu, live);
+                if (live) cjw[e0 + nkeep + __popc(bal & ((1u << lane) - 1u))] = make_uint2(cj, m);
+                nkeep += __popc(bal);
             }
         }
         __syncthreads();
@@ -705,7 +731,7 @@ int cluster_prune_launch(pd_cluster *c, int conditional, cudaStream_t s) {
     const double rp = c->p.rmax + c->p.prune_buffer;
     const float rp2 = (float)rp * (float)rp;
     k_prune<<<c->nsmax, 256, 0, s>>>(c->xq, c->perm, c->scio, c->cjo, c->cjw, c->nw, c->ref_prune, c->L[0], c->L[1],
-                                     c->L[2], rp2, c->counts, conditional ? 1 : 0);
+                                     c->L[2], rp2, (float)c->p.prune_buffer, c->counts, conditional ? 1 : 0);
     PD_LAUNCHED();
     return PD_OK;
 }
@@ -791,9 +817,9 @@ int pd_cluster_create(pd_cluster **out, const pd_cluster_params *p, const double
     pp.eshift = p->coul_eshift;
     pp.ne = p->coulomb ? p->coul_ne : 1;
     pp.nf = p->coulomb ? p->coul_nf : 1;
-    for (int k = 0; k < PD_MAX_POLY; ++k) {
-        pp.pe[k] = p->coul_pe[k];
-        pp.pf[k] = p->coul_pf[k];
+    for (int k = 0; k < PD_MAX_POLY; ++k) {   // coefficients past the fitted length are zero (exact padding)
+        pp.pe[k] = k < pp.ne ? p->coul_pe[k] : 0.f;
+        pp.pf[k] = k < pp.nf ? p->coul_pf[k] : 0.f;
     }
     if ((rc = pd_cluster_setup(c, box))) {
         pd_cluster_destroy(c);

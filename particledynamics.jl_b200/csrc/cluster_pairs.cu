@@ -45,13 +45,18 @@ __device__ __forceinline__ float reduce_i(float v) {
     return v;
 }
 
-__device__ __forceinline__ float horner(const float *c, int n, float x) {
-    float acc = c[n - 1];
-    for (int k = n - 2; k >= 0; --k) acc = fmaf(acc, x, c[k]);
+// Horner evaluation of a polynomial held in registers; the coefficient count is a
+// compile-time bucket and the coefficients above the fitted degree are zero, which
+// leaves the value unchanged (fma(0, x, 0) = 0 until the leading coefficient).
+template <int NP>
+__device__ __forceinline__ float horner(const float (&c)[NP], float x) {
+    float acc = c[NP - 1];
+#pragma unroll
+    for (int k = NP - 2; k >= 0; --k) acc = fmaf(acc, x, c[k]);
     return acc;
 }
 
-template <int LJK, bool COUL, bool ENERGY>
+template <int LJK, bool COUL, bool ENERGY, int NP>
 __global__ void __launch_bounds__(64) k_pairs(const float4 *__restrict__ xq, const int *__restrict__ ts,
                                               const uint2 *__restrict__ cjw, const int *__restrict__ scio,
                                               const int *__restrict__ nw, const int *__restrict__ counts,
@@ -74,6 +79,12 @@ __global__ void __launch_bounds__(64) k_pairs(const float4 *__restrict__ xq, con
     const float Lx = pp.Lx, Ly = pp.Ly, Lz = pp.Lz;
     const float hx = 0.5f * Lx, hy = 0.5f * Ly, hz = 0.5f * Lz;
     const float inf = __int_as_float(0x7f800000);
+    float cpf[NP], cpe[NP];
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+        cpf[k] = COUL ? pp.pf[k] : 0.f;
+        cpe[k] = (COUL && ENERGY) ? pp.pe[k] : 0.f;
+    }
     float fxi[8], fyi[8], fzi[8];
     float ei[8], w1i[8], w2i[8], w3i[8], w4i[8], w5i[8], w6i[8];
 #pragma unroll
@@ -99,6 +110,7 @@ __global__ void __launch_bounds__(64) k_pairs(const float4 *__restrict__ xq, con
         }
         const uint32_t imask = (cur.y >> (8 * w)) & 0xffu;
         if (imask == 0) continue;   // uniform per warp
+        const bool pbc = (cur.y >> 16) & 1u;   // tile may cross a box face before the next prune
         const int cj = (int)cur.x;
         const int js = cj * 8 + tj;
         float fjx = 0.f, fjy = 0.f, fjz = 0.f;
@@ -108,8 +120,8 @@ __global__ void __launch_bounds__(64) k_pairs(const float4 *__restrict__ xq, con
             if ((imask >> a) & 1u) {
                 const float4 pi = sxq[a * 8 + ti];
                 float dx = pi.x - cpj.x, dy = pi.y - cpj.y, dz = pi.z - cpj.z;
-                // compensated periodic difference only when a lane of this warp needs it
-                if (__any_sync(0xffffffffu, (fabsf(dx) > hx) | (fabsf(dy) > hy) | (fabsf(dz) > hz))) {
+                // compensated periodic difference (PeriodicDisplacement.jl:4-14) for marked tiles only
+                if (pbc) {
                     dx = periodic_delta(pi.x, cpj.x, hx, Lx);
                     dy = periodic_delta(pi.y, cpj.y, hy, Ly);
                     dz = periodic_delta(pi.z, cpj.z, hz, Lz);
@@ -141,12 +153,12 @@ __global__ void __launch_bounds__(64) k_pairs(const float4 *__restrict__ xq, con
                 if (COUL) {
                     const bool inr = r2 < pp.rc2;
                     const float x = fmaf(r2, pp.sx, -1.f);
-                    const float pf = horner(pp.pf, pp.nf, x);
+                    const float pf = horner(cpf, x);
                     const float rinv3 = rinv * rinv2;
                     const float cq = pp.C * (pi.w * cpj.w);
                     f += cq * (inr ? rinv3 - pf : 0.f);
                     if (ENERGY) {
-                        const float pe = horner(pp.pe, pp.ne, x);
+                        const float pe = horner(cpe, x);
                         en += cq * (inr ? rinv + pe - pp.eshift : 0.f);
                     }
                 }
@@ -272,36 +284,42 @@ __global__ void k_scatter(const int *__restrict__ perm, int nslot, const int *__
     }
 }
 
-int cluster_pairs_launch(pd_cluster *c, int energy, cudaStream_t s) {
-    const int grid = c->nsmax * c->nsplit;
+template <int LJK, bool COUL, bool EN, int NP>
+static void launch_pairs(pd_cluster *c, cudaStream_t s) {
+    k_pairs<LJK, COUL, EN, NP><<<c->nsmax * c->nsplit, 64, 0, s>>>(c->xq, c->ts, c->cjw, c->scio, c->nw, c->counts,
+                                                                   c->lj_table, c->fc, c->vc, c->nslot, c->nsplit,
+                                                                   c->pp);
+}
+
+template <int LJK, bool EN>
+static void launch_pairs_poly(pd_cluster *c, cudaStream_t s) {
     const PairParams &pp = c->pp;
-#define PD_PAIRS(LJK, COUL, EN)                                                                            \
-    k_pairs<LJK, COUL, EN><<<grid, 64, 0, s>>>(c->xq, c->ts, c->cjw, c->scio, c->nw, c->counts, c->lj_table, \
-                                               c->fc, c->vc, c->nslot, c->nsplit, pp)
-#define PD_PAIRS_E(LJK, COUL) \
-    do {                      \
-        if (energy)           \
-            PD_PAIRS(LJK, COUL, true); \
-        else                  \
-            PD_PAIRS(LJK, COUL, false); \
-    } while (0)
-    const bool coul = pp.coulomb != 0;
-    switch (pp.lj_kind) {
+    if (!pp.coulomb) {
+        launch_pairs<LJK, false, EN, 1>(c, s);
+        return;
+    }
+    const int n = EN ? (pp.nf > pp.ne ? pp.nf : pp.ne) : pp.nf;
+    if (n <= 8) launch_pairs<LJK, true, EN, 8>(c, s);
+    else if (n <= 10) launch_pairs<LJK, true, EN, 10>(c, s);
+    else if (n <= 12) launch_pairs<LJK, true, EN, 12>(c, s);
+    else if (n <= 14) launch_pairs<LJK, true, EN, 14>(c, s);
+    else if (n <= 16) launch_pairs<LJK, true, EN, 16>(c, s);
+    else if (n <= 20) launch_pairs<LJK, true, EN, 20>(c, s);
+    else launch_pairs<LJK, true, EN, 32>(c, s);
+}
+
+int cluster_pairs_launch(pd_cluster *c, int energy, cudaStream_t s) {
+    switch (c->pp.lj_kind) {
         case PD_LJ_NONE:
-            if (coul) PD_PAIRS_E(PD_LJ_NONE, true);
-            else PD_PAIRS_E(PD_LJ_NONE, false);
+            energy ? launch_pairs_poly<PD_LJ_NONE, true>(c, s) : launch_pairs_poly<PD_LJ_NONE, false>(c, s);
             break;
         case PD_LJ_UNIFORM:
-            if (coul) PD_PAIRS_E(PD_LJ_UNIFORM, true);
-            else PD_PAIRS_E(PD_LJ_UNIFORM, false);
+            energy ? launch_pairs_poly<PD_LJ_UNIFORM, true>(c, s) : launch_pairs_poly<PD_LJ_UNIFORM, false>(c, s);
             break;
         default:
-            if (coul) PD_PAIRS_E(PD_LJ_TABLE, true);
-            else PD_PAIRS_E(PD_LJ_TABLE, false);
+            energy ? launch_pairs_poly<PD_LJ_TABLE, true>(c, s) : launch_pairs_poly<PD_LJ_TABLE, false>(c, s);
             break;
     }
-#undef PD_PAIRS_E
-#undef PD_PAIRS
     PD_LAUNCHED();
     return PD_OK;
 }

@@ -29,6 +29,8 @@ struct pd_md {
     pd_md_state st;
     float L[3] = {0, 0, 0};
     cudaStream_t side = nullptr;
+    cudaStream_t body = nullptr;   // captures the bodies of the conditional nodes
+    bool cond_nodes = true;        // false after a failed conditional capture: gated kernels instead
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaGraphExec_t exec[2] = {nullptr, nullptr};   // [energy]
     float exec_dt[2] = {0.f, 0.f};
@@ -106,7 +108,13 @@ __global__ void __launch_bounds__(256) k_kick_drift(int n, float *__restrict__ x
     }
 }
 
-__global__ void k_decide_step(int *__restrict__ counts, int nstlist, int nstprune) {
+// Device build/prune decision (_decide_kernel!, Engine.jl:301-324).  In a captured
+// step it also sets the graph's two IF conditions, so the build and prune bodies
+// are not launched at all on steps that do not need them (the reference's
+// conditional graph nodes, DeviceConditionalGraph.jl:88-132).
+template <bool COND>
+__global__ void k_decide_step(int *__restrict__ counts, int nstlist, int nstprune, cudaGraphConditionalHandle hb,
+                              cudaGraphConditionalHandle hp) {
     float anyr = __int_as_float(counts[W_FLAG_ANY]);
     float br = __int_as_float(counts[W_FLAG_BUILD]);
     bool build, prune;
@@ -126,6 +134,10 @@ __global__ void k_decide_step(int *__restrict__ counts, int nstlist, int nstprun
     counts[W_NPRUNE] += prune ? 1 : 0;
     counts[W_FLAG_ANY] = 0;
     counts[W_FLAG_BUILD] = 0;
+    if (COND) {
+        cudaGraphSetConditional(hb, build ? 1u : 0u);
+        cudaGraphSetConditional(hp, prune ? 1u : 0u);
+    }
 }
 
 // Slot forces to storage order with the closing half kick (no mesh):
@@ -215,21 +227,70 @@ static int enqueue_forces(pd_md *md, int energy, float half_dt, cudaStream_t s) 
     return PD_OK;
 }
 
-// One full step, device-decided (capturable).
-static int enqueue_step(pd_md *md, float dt, int energy, cudaStream_t s) {
+// Append an IF node on `h` to the graph being captured on s and capture body(cs) into
+// its body graph on the helper stream cs; s then continues after the IF node.
+template <typename F>
+static int capture_if(cudaStream_t s, cudaStream_t cs, cudaGraphConditionalHandle h, F &&body) {
+    cudaStreamCaptureStatus status;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    unsigned long long id = 0;
+    PD_CUDA(cudaStreamGetCaptureInfo(s, &status, &id, &g, &deps, &ndeps));
+    PD_CHECK(status == cudaStreamCaptureStatusActive, PD_ESTATE, "conditional node outside a capture");
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeIf;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    PD_CUDA(cudaGraphAddNode(&node, g, deps, ndeps, &p));
+    cudaGraph_t bodyg = p.conditional.phGraph_out[0];
+    PD_CUDA(cudaStreamBeginCaptureToGraph(cs, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    const int rc = body(cs);
+    cudaGraph_t done = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(cs, &done);
+    if (rc) return rc;
+    PD_CHECK(e == cudaSuccess, PD_ECUDA, "conditional body capture failed: %s", cudaGetErrorString(e));
+    PD_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    return PD_OK;
+}
+
+// One full step, device-decided.  cond = 1 (inside a stream capture): the build and
+// prune bodies become IF nodes of the captured graph; otherwise their kernels are
+// launched and return at once when the device flags are clear.
+static int enqueue_step(pd_md *md, float dt, int energy, cudaStream_t s, int cond) {
     pd_cluster *c = md->c;
     pd_md_state &st = md->st;
     const float hb = (float)(0.5 * c->p.skin), hp = (float)(0.5 * c->p.prune_buffer);
+    const float *q = c->p.coulomb ? st.q : nullptr;
     k_kick_drift<<<(st.n + 255) / 256, 256, 0, s>>>(st.n, st.x, st.y, st.z, st.vx, st.vy, st.vz, st.fx, st.fy, st.fz,
                                                     st.inv_mass, st.inv_mass_uniform, dt, md->L[0], md->L[1], md->L[2],
-                                                    c->p.coulomb ? st.q : nullptr, c->slot_of, c->xq, c->ref_build,
-                                                    c->ref_prune, hb * hb, hp * hp, c->counts);
-    PD_LAUNCHED();
-    k_decide_step<<<1, 1, 0, s>>>(c->counts, c->p.nstlist, c->p.nstprune);
+                                                    q, c->slot_of, c->xq, c->ref_build, c->ref_prune, hb * hb,
+                                                    hp * hp, c->counts);
     PD_LAUNCHED();
     int rc;
-    if ((rc = cluster_build_launch(c, st.x, st.y, st.z, c->p.coulomb ? st.q : nullptr, st.type, 1, s))) return rc;
-    if ((rc = cluster_prune_launch(c, 1, s))) return rc;
+    if (cond) {
+        cudaStreamCaptureStatus status;
+        cudaGraph_t g = nullptr;
+        PD_CUDA(cudaStreamGetCaptureInfo(s, &status, nullptr, &g, nullptr, nullptr));
+        cudaGraphConditionalHandle hbuild, hprune;
+        PD_CUDA(cudaGraphConditionalHandleCreate(&hbuild, g, 0, cudaGraphCondAssignDefault));
+        PD_CUDA(cudaGraphConditionalHandleCreate(&hprune, g, 0, cudaGraphCondAssignDefault));
+        k_decide_step<true><<<1, 1, 0, s>>>(c->counts, c->p.nstlist, c->p.nstprune, hbuild, hprune);
+        PD_LAUNCHED();
+        if ((rc = capture_if(s, md->body, hbuild, [&](cudaStream_t cs) {
+                 return cluster_build_launch(c, st.x, st.y, st.z, q, st.type, 1, cs);
+             })))
+            return rc;
+        if ((rc = capture_if(s, md->body, hprune, [&](cudaStream_t cs) { return cluster_prune_launch(c, 1, cs); })))
+            return rc;
+    } else {
+        k_decide_step<false><<<1, 1, 0, s>>>(c->counts, c->p.nstlist, c->p.nstprune, 0, 0);
+        PD_LAUNCHED();
+        if ((rc = cluster_build_launch(c, st.x, st.y, st.z, q, st.type, 1, s))) return rc;
+        if ((rc = cluster_prune_launch(c, 1, s))) return rc;
+    }
     return enqueue_forces(md, energy, 0.5f * dt, s);
 }
 
@@ -252,6 +313,7 @@ int pd_md_create(pd_md **out, pd_cluster *c, pd_mesh *m, const pd_md_state *st, 
     for (int d = 0; d < 3; ++d) md->L[d] = (float)box[d];
     md->half_c_self = c->p.coulomb ? 0.5f * c->p.coul_C * c->p.selfc : 0.f;
     if (cudaStreamCreateWithFlags(&md->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&md->body, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&md->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&md->ev_join, cudaEventDisableTiming) != cudaSuccess ||
         dalloc(&md->esum, 1) != PD_OK) {
@@ -270,6 +332,7 @@ int pd_md_destroy(pd_md *md) {
     if (md->ev_fork) cudaEventDestroy(md->ev_fork);
     if (md->ev_join) cudaEventDestroy(md->ev_join);
     if (md->side) cudaStreamDestroy(md->side);
+    if (md->body) cudaStreamDestroy(md->body);
     dfree(md->esum);
     delete md;
     return PD_OK;
@@ -323,7 +386,7 @@ int pd_md_step(pd_md *md, int nsteps, float dt, int energy_last, int use_graph, 
     for (int k = 0; k < nsteps; ++k) {
         const int energy = (energy_last && k == nsteps - 1) ? 1 : 0;
         if (!use_graph) {
-            if ((rc = enqueue_step(md, dt, energy, s))) return rc;
+            if ((rc = enqueue_step(md, dt, energy, s, 0))) return rc;
             continue;
         }
         if (!md->exec[energy] || md->exec_dt[energy] != dt || md->exec_stream[energy] != s) {
@@ -332,18 +395,24 @@ int pd_md_step(pd_md *md, int nsteps, float dt, int energy_last, int use_graph, 
                 md->exec[energy] = nullptr;
             }
             PD_CHECK(s != nullptr, PD_EINVAL, "pd_md_step: graph replay needs a non-default stream");
-            cudaGraph_t g = nullptr;
-            PD_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-            rc = enqueue_step(md, dt, energy, s);
-            cudaError_t e = cudaStreamEndCapture(s, &g);
-            if (rc) {
+            // conditional IF nodes for build / prune; if this driver refuses them, capture the gated kernels
+            for (int attempt = 0; attempt < 2 && !md->exec[energy]; ++attempt) {
+                const int cond = md->cond_nodes ? 1 : 0;
+                cudaGraph_t g = nullptr;
+                PD_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+                rc = enqueue_step(md, dt, energy, s, cond);
+                cudaError_t e = cudaStreamEndCapture(s, &g);
+                if (rc == PD_OK && e == cudaSuccess) e = cudaGraphInstantiate(&md->exec[energy], g, 0);
                 if (g) cudaGraphDestroy(g);
-                return rc;
+                if (rc == PD_OK && e == cudaSuccess) break;
+                md->exec[energy] = nullptr;
+                cudaGetLastError();
+                if (!cond) {
+                    if (rc) return rc;
+                    PD_CHECK(false, PD_ECUDA, "step capture failed: %s", cudaGetErrorString(e));
+                }
+                md->cond_nodes = false;
             }
-            PD_CHECK(e == cudaSuccess, PD_ECUDA, "step capture failed: %s", cudaGetErrorString(e));
-            e = cudaGraphInstantiate(&md->exec[energy], g, 0);
-            cudaGraphDestroy(g);
-            PD_CHECK(e == cudaSuccess, PD_ECUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
             md->exec_dt[energy] = dt;
             md->exec_stream[energy] = s;
         }

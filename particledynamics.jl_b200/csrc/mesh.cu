@@ -113,15 +113,25 @@ __device__ __forceinline__ int signed_offset(int k, int r, int K) {
 // Brick of one chunk: first valid particle's stencil base is the reference;
 // every particle's base is expressed as an offset from it, and the brick is
 // the bounding box of the stencils.
+//
+// With vec (K1 a multiple of 4) the brick's x origin is aligned down to a
+// multiple of 4 nodes and its x extent rounded up to a multiple of 4, so every
+// brick row moves to and from the global grid as 16-byte vectors (a row of a
+// multiple-of-4 mesh never splits a vector across its periodic end).  The
+// wrapped global base of every brick row is tabulated once in shared memory.
 struct Brick {
     int o1, o2, o3;   // global origin node (not wrapped)
     int e1, e2, e3;   // extents
     int fits;
+    int vec;
 };
+
+constexpr int ROWS_MAX = TILE_MAX / 4;   // brick rows (the x extent is at least 4 when it fits)
 
 template <int P>
 __device__ __forceinline__ void chunk_brick(bool valid, int k1, int k2, int k3, int K1, int K2, int K3, int &d1,
-                                            int &d2, int &d3, Brick &b, int *sm /* >= 10 ints */) {
+                                            int &d2, int &d3, Brick &b, int *sm /* >= 10 ints */,
+                                            unsigned *rowbase) {
     // sm[0] first valid, sm[1..3] ref, sm[4..6] min, sm[7..9] max
     const int t = threadIdx.x;
     if (t == 0) {
@@ -151,16 +161,26 @@ __device__ __forceinline__ void chunk_brick(bool valid, int k1, int k2, int k3, 
         atomicMax(&sm[9], d3);
     }
     __syncthreads();
+    b.vec = (K1 & 3) == 0;
     if (any) {
-        b.o1 = sm[1] + sm[4];
+        int o1 = sm[1] + sm[4], e1 = sm[7] - sm[4] + P;
+        int shift = 0;
+        if (b.vec) {
+            shift = ((o1 % 4) + 4) % 4;
+            o1 -= shift;
+            e1 = (e1 + shift + 3) & ~3;
+        }
+        b.o1 = o1;
         b.o2 = sm[2] + sm[5];
         b.o3 = sm[3] + sm[6];
-        b.e1 = sm[7] - sm[4] + P;
+        b.e1 = e1;
         b.e2 = sm[8] - sm[5] + P;
         b.e3 = sm[9] - sm[6] + P;
-        b.fits = (long long)b.e1 * b.e2 * b.e3 <= TILE_MAX;
+        const long long nodes = (long long)b.e1 * b.e2 * b.e3;
+        b.fits = nodes <= TILE_MAX && b.e1 <= MESH_THREADS && (!b.vec || b.e1 <= K1) &&
+                 (long long)b.e2 * b.e3 <= ROWS_MAX;
         if (valid) {
-            d1 -= sm[4];
+            d1 += shift - sm[4];
             d2 -= sm[5];
             d3 -= sm[6];
         }
@@ -169,7 +189,32 @@ __device__ __forceinline__ void chunk_brick(bool valid, int k1, int k2, int k3, 
         b.e1 = b.e2 = b.e3 = 0;
         b.fits = 1;
     }
+    if (b.fits) {
+        const int nrows = b.e2 * b.e3;
+        for (int r = threadIdx.x; r < nrows; r += blockDim.x) {
+            const int l2 = r % b.e2, l3 = r / b.e2;
+            rowbase[r] = (unsigned)(((size_t)wrap_node(b.o3 + l3, K3) * K2 + wrap_node(b.o2 + l2, K2)) * K1);
+        }
+    }
     __syncthreads();
+}
+
+// Move a brick between shared memory and the global grid: lanes are laid out as
+// (row, x vector) with MESH_THREADS / nv rows in flight, nv = vectors (or nodes)
+// per row; visit(tile_element, global_node) gets the first node of each
+// 4-node vector (vec) or single node.
+template <typename F>
+__device__ __forceinline__ void for_brick(const Brick &b, const unsigned *rowbase, int K1, F &&visit) {
+    const int per = b.vec ? 4 : 1;
+    const int nv = b.e1 / per;
+    if (nv == 0) return;
+    const int rpi = MESH_THREADS / nv;
+    const int t = threadIdx.x;
+    const int r0 = t / nv, v = t - r0 * nv;
+    if (r0 >= rpi) return;
+    const int x0 = wrap_node(b.o1 + per * v, K1);
+    const int nrows = b.e2 * b.e3;
+    for (int r = r0; r < nrows; r += rpi) visit(r * nv + v, (size_t)rowbase[r] + x0);
 }
 
 // Spread of chunks of packed (x, y, z, q) particles (the charge assignment of
@@ -182,7 +227,8 @@ __global__ void __launch_bounds__(MESH_THREADS) k_spread(const float4 *__restric
     const int c = blockIdx.x;
     if (nchunk_dev && c >= *nchunk_dev) return;
     if (c >= nchunks) return;
-    __shared__ float tile[TILE_MAX];
+    __shared__ __align__(16) float tile[TILE_MAX];
+    __shared__ unsigned rowbase[ROWS_MAX];
     __shared__ int sm[10];
     const int t = threadIdx.x, p = t & (MESH_CHUNK - 1), h = t >> 6;
     const float4 v = xq[c * MESH_CHUNK + p];
@@ -197,15 +243,17 @@ __global__ void __launch_bounds__(MESH_THREADS) k_spread(const float4 *__restric
     int d1 = 0, d2 = 0, d3 = 0;
     Brick b;
     // both halves of a particle take part (their min/max contributions are identical)
-    chunk_brick<P>(valid, k1, k2, k3, K1, K2, K3, d1, d2, d3, b, sm);
+    chunk_brick<P>(valid, k1, k2, k3, K1, K2, K3, d1, d2, d3, b, sm, rowbase);
     constexpr int PH = (P + 1) / 2;
-    const int j3a = h == 0 ? 0 : PH, j3b = h == 0 ? PH : P;
+
     if (b.fits) {
-        const int nb = b.e1 * b.e2 * b.e3;
-        for (int k = t; k < nb; k += MESH_THREADS) tile[k] = 0.f;
+        const int nb4 = (b.e1 * b.e2 * b.e3 + 3) >> 2;
+        float4 *tile4 = reinterpret_cast<float4 *>(tile);
+        for (int k = t; k < nb4; k += MESH_THREADS) tile4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
         __syncthreads();
         if (valid) {
-            for (int j3 = j3a; j3 < j3b; ++j3) {
+            for (int j3 = 0; j3 < P; ++j3) {   // unrolled; this half's z nodes only (warp-uniform test)
+            if ((j3 < PH) != (h == 0)) continue;
                 const float q3 = v.w * w3[j3];
 #pragma unroll
                 for (int j2 = 0; j2 < P; ++j2) {
@@ -217,21 +265,28 @@ __global__ void __launch_bounds__(MESH_THREADS) k_spread(const float4 *__restric
             }
         }
         __syncthreads();
-        for (int k = t; k < nb; k += MESH_THREADS) {
-            const float val = tile[k];
-            if (val != 0.f) {
-                const int l1 = k % b.e1, r = k / b.e1, l2 = r % b.e2, l3 = r / b.e2;
-                const int n1 = wrap_node(b.o1 + l1, K1), n2 = wrap_node(b.o2 + l2, K2), n3 = wrap_node(b.o3 + l3, K3);
-                red_add(grid + ((size_t)n3 * K2 + n2) * K1 + n1, val);
-            }
+        if (b.vec) {
+            for_brick(b, rowbase, K1, [&](int kt, size_t kg) {
+                const float4 val = tile4[kt];
+                if (val.x != 0.f || val.y != 0.f || val.z != 0.f || val.w != 0.f)
+                    red_add_v4(grid + kg, val.x, val.y, val.z, val.w);
+            });
+        } else {
+            for_brick(b, rowbase, K1, [&](int kt, size_t kg) {
+                const float val = tile[kt];
+                if (val != 0.f) red_add(grid + kg, val);
+            });
         }
     } else if (valid) {
-        for (int j3 = j3a; j3 < j3b; ++j3) {
+        for (int j3 = 0; j3 < P; ++j3) {   // unrolled; this half's z nodes only (warp-uniform test)
+            if ((j3 < PH) != (h == 0)) continue;
             const int n3 = wrap_node(k3 + j3, K3);
             const float q3 = v.w * w3[j3];
+#pragma unroll
             for (int j2 = 0; j2 < P; ++j2) {
                 const int n2 = wrap_node(k2 + j2, K2);
                 const float q23 = q3 * w2[j2];
+#pragma unroll
                 for (int j1 = 0; j1 < P; ++j1)
                     red_add(grid + ((size_t)n3 * K2 + n2) * K1 + wrap_node(k1 + j1, K1), q23 * w1[j1]);
             }
@@ -333,7 +388,8 @@ __global__ void __launch_bounds__(MESH_THREADS) k_gather(const float4 *__restric
     const int c = blockIdx.x;
     if (nchunk_dev && c >= *nchunk_dev) return;
     if (c >= nchunks) return;
-    __shared__ float tile[TILE_MAX];
+    __shared__ __align__(16) float tile[TILE_MAX];
+    __shared__ unsigned rowbase[ROWS_MAX];
     __shared__ int sm[10];
     __shared__ float part[MESH_CHUNK][4];
     const int t = threadIdx.x, p = t & (MESH_CHUNK - 1), h = t >> 6;
@@ -341,6 +397,17 @@ __global__ void __launch_bounds__(MESH_THREADS) k_gather(const float4 *__restric
     const float4 v = xq[e];
     const int id = (MODE == 2) ? o.ids[e] : (e < o.n_entries ? (o.ids ? o.ids[e] : e) : -1);
     const bool charged = v.w != 0.f && isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && id >= 0;
+    // join: fetch the slot pair force and the particle's velocity now, so that their latency
+    // overlaps the brick set-up and the potential load below
+    float4 fpair = make_float4(0.f, 0.f, 0.f, 0.f);
+    float pvx = 0.f, pvy = 0.f, pvz = 0.f, pim = 0.f;
+    if (MODE == 2 && h == 0 && id >= 0) {
+        fpair = o.fc[e];
+        pvx = o.vx[id];
+        pvy = o.vy[id];
+        pvz = o.vz[id];
+        pim = o.inv_mass ? o.inv_mass[id] : o.inv_mass_uniform;
+    }
     float w1[P], w2[P], w3[P], g1[P], g2[P], g3[P];
     int k1 = 0, k2 = 0, k3 = 0;
     if (charged) {
@@ -350,20 +417,23 @@ __global__ void __launch_bounds__(MESH_THREADS) k_gather(const float4 *__restric
     }
     int d1 = 0, d2 = 0, d3 = 0;
     Brick b;
-    chunk_brick<P>(charged, k1, k2, k3, K1, K2, K3, d1, d2, d3, b, sm);
+    chunk_brick<P>(charged, k1, k2, k3, K1, K2, K3, d1, d2, d3, b, sm, rowbase);
     constexpr int PH = (P + 1) / 2;
-    const int j3a = h == 0 ? 0 : PH, j3b = h == 0 ? PH : P;
+
     float phi = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
     if (b.fits) {
-        const int nb = b.e1 * b.e2 * b.e3;
-        for (int k = t; k < nb; k += MESH_THREADS) {
-            const int l1 = k % b.e1, r = k / b.e1, l2 = r % b.e2, l3 = r / b.e2;
-            const int n1 = wrap_node(b.o1 + l1, K1), n2 = wrap_node(b.o2 + l2, K2), n3 = wrap_node(b.o3 + l3, K3);
-            tile[k] = grid[((size_t)n3 * K2 + n2) * K1 + n1];
+        if (b.vec) {
+            float4 *tile4 = reinterpret_cast<float4 *>(tile);
+            for_brick(b, rowbase, K1, [&](int kt, size_t kg) {
+                tile4[kt] = __ldg(reinterpret_cast<const float4 *>(grid + kg));
+            });
+        } else {
+            for_brick(b, rowbase, K1, [&](int kt, size_t kg) { tile[kt] = __ldg(grid + kg); });
         }
         __syncthreads();
         if (charged) {
-            for (int j3 = j3a; j3 < j3b; ++j3) {
+            for (int j3 = 0; j3 < P; ++j3) {   // unrolled; this half's z nodes only (warp-uniform test)
+            if ((j3 < PH) != (h == 0)) continue;
                 float s0 = 0.f, s1 = 0.f, s2 = 0.f;   // sum w1 w2 c, sum dw1 w2 c, sum w1 dw2 c over a z-plane
 #pragma unroll
                 for (int j2 = 0; j2 < P; ++j2) {
@@ -386,12 +456,15 @@ __global__ void __launch_bounds__(MESH_THREADS) k_gather(const float4 *__restric
             }
         }
     } else if (charged) {
-        for (int j3 = j3a; j3 < j3b; ++j3) {
+        for (int j3 = 0; j3 < P; ++j3) {   // unrolled; this half's z nodes only (warp-uniform test)
+            if ((j3 < PH) != (h == 0)) continue;
             const int n3 = wrap_node(k3 + j3, K3);
             float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+#pragma unroll
             for (int j2 = 0; j2 < P; ++j2) {
                 const int n2 = wrap_node(k2 + j2, K2);
                 float a0 = 0.f, a1 = 0.f;
+#pragma unroll
                 for (int j1 = 0; j1 < P; ++j1) {
                     const float cval = grid[((size_t)n3 * K2 + n2) * K1 + wrap_node(k1 + j1, K1)];
                     a0 = fmaf(w1[j1], cval, a0);
@@ -430,7 +503,7 @@ __global__ void __launch_bounds__(MESH_THREADS) k_gather(const float4 *__restric
     }
     if (MODE == 2) {
         if (id < 0) return;
-        const float4 f = o.fc[e];
+        const float4 f = fpair;
         o.fc[e] = make_float4(0.f, 0.f, 0.f, 0.f);
         Fx += f.x;
         Fy += f.y;
@@ -438,10 +511,10 @@ __global__ void __launch_bounds__(MESH_THREADS) k_gather(const float4 *__restric
         o.fx[id] = Fx;
         o.fy[id] = Fy;
         o.fz[id] = Fz;
-        const float cm = o.half_dt * (o.inv_mass ? o.inv_mass[id] : o.inv_mass_uniform);
-        o.vx[id] = fmaf(cm, Fx, o.vx[id]);
-        o.vy[id] = fmaf(cm, Fy, o.vy[id]);
-        o.vz[id] = fmaf(cm, Fz, o.vz[id]);
+        const float cm = o.half_dt * pim;
+        o.vx[id] = fmaf(cm, Fx, pvx);
+        o.vy[id] = fmaf(cm, Fy, pvy);
+        o.vz[id] = fmaf(cm, Fz, pvz);
         if (ENERGY) {
             o.epot[id] = Ei + f.w - o.half_c_self * qi * qi;
 #pragma unroll

@@ -24,10 +24,10 @@ def _ptr(t) -> int:
     return 0 if t is None else int(t.data_ptr())
 
 
-def _destroy(name: str, handle) -> None:
+def _destroy(name: str, handle, _native=N) -> None:
     """Release a native handle; a no-op during interpreter shutdown (module globals already cleared)."""
     try:
-        getattr(N.lib(), name)(handle)
+        getattr(_native.lib(), name)(handle)
     except Exception:
         pass
 
@@ -103,7 +103,7 @@ class ClusterPairEngine:
         self.handle = h
         self.box = tuple(float(b) for b in box)
 
-    def close(self):
+    def close(self, _destroy=_destroy):
         if getattr(self, "handle", None):
             _destroy("pd_cluster_destroy", self.handle)
             self.handle = None
@@ -305,7 +305,7 @@ class ElectrostaticsSolver:
         N.call("pd_mesh_create", C.byref(h), C.byref(p), N.dbl3(box))
         self.handle = h
 
-    def close(self):
+    def close(self, _destroy=_destroy):
         if getattr(self, "handle", None):
             _destroy("pd_mesh_destroy", self.handle)
             self.handle = None
@@ -396,7 +396,7 @@ class DeviceEngine:
         self.handle = h
         self._keep = s
 
-    def close(self):
+    def close(self, _destroy=_destroy):
         if getattr(self, "handle", None):
             _destroy("pd_md_destroy", self.handle)
             self.handle = None
@@ -410,8 +410,12 @@ class DeviceEngine:
         N.call("pd_md_step", self.handle, int(nsteps), float(dt), int(bool(energy_last)), int(bool(use_graph)),
                _stream(stream))
 
-    def step_host(self, host_xyz: np.ndarray, host_v: np.ndarray, nsteps: int, dt: float, stream=None) -> float:
+    def step_host(self, host_xyz: np.ndarray, host_v: np.ndarray, nsteps: int, dt: float, stream=None,
+                  energy: bool = True):
+        """Steps from and back to host buffers (3n floats each); the potential energy of the last step
+        when energy is set, else None."""
         e = C.c_double()
         N.call("pd_md_step_host", self.handle, host_xyz.ctypes.data_as(C.c_void_p),
-               host_v.ctypes.data_as(C.c_void_p), int(nsteps), float(dt), C.byref(e), _stream(stream))
-        return e.value
+               host_v.ctypes.data_as(C.c_void_p), int(nsteps), float(dt), C.byref(e) if energy else None,
+               _stream(stream))
+        return e.value if energy else None

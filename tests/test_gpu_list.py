@@ -42,7 +42,7 @@ def test_list_bit_exact(pd, ora, cuda, n, box, rc, skin, prune, seed):
     assert np.all(np.isnan(gpu["xq"][:64 * ref["ns"]][~occ, 0]))
     # pruned working list from the GPU's packed coordinates
     cjw, nw = ora.cluster_prune(ref["ns"], gpu["xq"][:64 * ref["ns"]].reshape(-1), ref["scio"], ref["cjo"], box,
-                                rc + prune)
+                                rc + prune, prune)
     assert np.array_equal(gpu["nw"], nw)
     for S in range(ref["ns"]):
         a, k = ref["scio"][S], nw[S]
