@@ -161,6 +161,27 @@ int pd_cluster_scatter(pd_cluster *c, float *fx, float *fy, float *fz, float *ep
 int pd_cluster_compute(pd_cluster *c, const float *x, const float *y, const float *z,
                        const float *q, const int *type, float *fx, float *fy, float *fz,
                        float *epot, float *vir6, int energy, pd_stream_t s);
+/* Allocation-free force evaluation.  This entry point has no counterpart in the reference.
+ *
+ * It serves callers that cannot call cudaMalloc: a host that has sized its device memory to the
+ * byte and forbids further allocation, code running while a CUDA graph region is being built,
+ * or a real-time loop that must stay out of the allocator.  It does the work of
+ * pd_cluster_compute (build, prune, pair pass, scatter) for one small system without a handle,
+ * taking every scratch buffer from one static device array of PD_STATIC_SCRATCH_BYTES that each
+ * GPU loading the library holds until the process exits.  The caller passes the inputs and the
+ * outputs as for pd_cluster_compute; it calls no allocating routine.
+ *
+ * Limits: 1 <= p->n <= PD_STATIC_MAX_N particles (larger counts return PD_EINVAL with a message);
+ * PD_ECAPACITY if the outer list outgrows the array.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current, so make that first
+ * call before any stream capture.  All calls share the array and it keeps the last call's
+ * contents (the call clears what must start at zero); calls that overlap on the GPU race.
+ * The call reads a device status word back at its end, so it synchronises s. */
+#define PD_STATIC_SCRATCH_BYTES (4u << 20)
+#define PD_STATIC_MAX_N 4096
+int pd_cluster_compute_static(const pd_cluster_params *p, const double box[3], const float *x, const float *y,
+                              const float *z, const float *q, const int *type, float *fx, float *fy, float *fz,
+                              float *epot, float *vir6, int energy, pd_stream_t s);
 /* statistics(eng) (Engine.jl:402-412): host read of the device counts (synchronises s). */
 int pd_cluster_status(pd_cluster *c, pd_cluster_stats *out, pd_stream_t s);
 /* mesh_order(eng) (Engine.jl:394): device pointer to the particles in slot order (n entries). */

@@ -89,6 +89,8 @@ _SIGS = {
     "pd_cluster_pairs": (C.c_int, [_p, C.c_int, _p]),
     "pd_cluster_scatter": (C.c_int, [_p, _fp, _fp, _fp, _fp, _fp, _fp, C.c_int, C.c_int, _p]),
     "pd_cluster_compute": (C.c_int, [_p, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, C.c_int, _p]),
+    "pd_cluster_compute_static": (C.c_int, [C.POINTER(ClusterParams), C.POINTER(C.c_double), _fp, _fp, _fp, _fp,
+                                            _fp, _fp, _fp, _fp, _fp, _fp, C.c_int, _p]),
     "pd_cluster_status": (C.c_int, [_p, C.POINTER(ClusterStats), _p]),
     "pd_cluster_order": (_fp, [_p]),
     "pd_cluster_buffers": (C.c_int, [_p, C.POINTER(_p), C.POINTER(_p), C.POINTER(_p), C.POINTER(_p),
