@@ -20,6 +20,10 @@
 #include <omp.h>
 #endif
 
+/* Packed coordinates above this value mark padding slots (the device fills them with
+ * far-away, pairwise distinct points near 1e7 and zero charge). */
+#define PAD_LIMIT 1.0e6f
+
 static double mi(double d, double L) { return d - L * nearbyint(d / L); }
 
 /* ------------------------------------------------------------------------
@@ -709,6 +713,9 @@ int ora_cluster_build(int n, const float *x, const float *y, const float *z, con
         if (cx > ncx - 1) cx = ncx - 1;
         if (cy > ncy - 1) cy = ncy - 1;
         if (cz > nzb - 1) cz = nzb - 1;
+        if (cx < 0) cx = 0;
+        if (cy < 0) cy = 0;
+        if (cz < 0) cz = 0;
         bin[i] = (cx + ncx * cy) * nzb + cz;
         bcnt[bin[i]]++;
     }
@@ -887,24 +894,39 @@ float ora_force_coordinate(float x, float L) {
 /* Distance-only prune of the outer list (_prune_only_kernel!, src/clusterpairs/Kernels.jl:349-394)
  * with the widened radius r_p^2 + eps (16 r_p L_max + 16 r_p^2), followed by the compaction of the
  * kept entries in list order (_compact_warp_kernel!, List.jl:719-759).  xq holds the packed force
- * coordinates and charges (4 floats per slot, NaN padding).  cjw receives (cj, mask_lo | mask_hi << 8)
- * pairs at the super-cluster's outer offset; nw the kept count per super-cluster. */
+ * coordinates and charges (4 floats per slot; padding slots above PAD_LIMIT take no part).  cjw
+ * receives (cj, mask_lo | mask_hi << 8 | mark << 16) pairs at the super-cluster's outer offset; nw the
+ * kept count per super-cluster.
+ *
+ * The periodic-path mark (bit 16) of an entry is set when its tile holds an atom within half the
+ * prune buffer of a face, or when an i-atom and a j-atom lie within m = 1.01 r_p + prune buffer of
+ * opposite faces of one dimension (face codes: bit 2d for +, 2d+1 for -). */
+static int ora_face_code(const float *p, const float sl[3], const float wl[3]) {
+    int c = 0;
+    for (int k = 0; k < 3; ++k) {
+        if (p[k] > sl[k]) c |= 1 << (2 * k);
+        if (p[k] < -sl[k]) c |= 2 << (2 * k);
+        if (fabsf(p[k]) > wl[k]) c |= 64;
+    }
+    return c;
+}
+
 void ora_cluster_prune(int NS, const float *xq, const int *scio, const uint32_t *cjo, const double box[3], double rp,
                        double pbuf, uint32_t *cjw, int *nw) {
     const float L[3] = {(float)box[0], (float)box[1], (float)box[2]};
-    /* periodic-path mark (bit 16): an atom within half the prune buffer of a face, or a separation
-     * component above L/2 - prune buffer, among the tile's atoms */
     const float pb = (float)pbuf;
-    float wl[3], dl[3];
+    const float rpf = (float)rp;
+    const float rp2 = rpf * rpf;
+    const float m1 = 1.01f * sqrtf(rp2);
+    const float mg = m1 + pb;
+    float wl[3], sl[3];
     for (int k = 0; k < 3; ++k) {
         const float hL = 0.5f * L[k], hp = 0.5f * pb;
         wl[k] = hL - hp;
-        dl[k] = hL - pb;
+        sl[k] = hL - mg;
     }
     const float iL[3] = {1.0f / L[0], 1.0f / L[1], 1.0f / L[2]};
     const float Lmax = fmaxf(L[0], fmaxf(L[1], L[2]));
-    const float rpf = (float)rp;
-    const float rp2 = rpf * rpf;
     const float epsf = 1.1920929e-7f;
     const float t16 = 16.0f * sqrtf(rp2);
     const float t16L = t16 * Lmax;
@@ -918,19 +940,24 @@ void ora_cluster_prune(int NS, const float *xq, const int *scio, const uint32_t 
             const int cj = (int)(cjo[e] >> 8);
             const uint32_t imask = cjo[e] & 0xffu;
             uint32_t m[2] = {0, 0};
-            int mark = 0;
+            int ic = 0, jc = 0;
             for (int a = 0; a < 8; ++a) {
                 if (!((imask >> a) & 1u)) continue;
-                for (int tj = 0; tj < 8; ++tj)
-                    for (int ti = 0; ti < 8; ++ti) {
-                        const float *pi = xq + 4 * (size_t)(64 * S + 8 * a + ti);
-                        const float *pj = xq + 4 * (size_t)(8 * cj + tj);
-                        for (int k = 0; k < 3; ++k) {
-                            const float r = pi[k] - pj[k];
-                            if (fabsf(pj[k]) > wl[k] || fabsf(pi[k]) > wl[k] || fabsf(r) > dl[k]) mark = 1;
-                        }
-                    }
+                for (int ti = 0; ti < 8; ++ti) {
+                    const float *pi = xq + 4 * (size_t)(64 * S + 8 * a + ti);
+                    if (!(pi[0] > PAD_LIMIT)) ic |= ora_face_code(pi, sl, wl);
+                }
             }
+            for (int tj = 0; tj < 8; ++tj) {
+                const float *pj = xq + 4 * (size_t)(8 * cj + tj);
+                if (!(pj[0] > PAD_LIMIT)) jc |= ora_face_code(pj, sl, wl);
+            }
+            int cross = 0;
+            for (int k = 0; k < 3; ++k)
+                if ((((ic >> (2 * k)) & 1) && ((jc >> (2 * k + 1)) & 1)) ||
+                    (((ic >> (2 * k + 1)) & 1) && ((jc >> (2 * k)) & 1)))
+                    cross = 1;
+            const int mark = cross || ((ic | jc) & 64);
             for (int h = 0; h < 2; ++h)
                 for (int a = 0; a < 8; ++a) {
                     if (!((imask >> a) & 1u)) continue;
@@ -945,7 +972,8 @@ void ora_cluster_prune(int NS, const float *xq, const int *scio, const uint32_t 
                                 d[k] = fmaf(-L[k], rintf(dd * iL[k]), dd);
                             }
                             const float r2 = fmaf(d[0], d[0], fmaf(d[1], d[1], d[2] * d[2]));
-                            const int ok = ((cj != 8 * S + a) || (tj > ti)) && (r2 < INFINITY);
+                            const int real = !(pi[0] > PAD_LIMIT) && !(pj[0] > PAD_LIMIT);
+                            const int ok = real && ((cj != 8 * S + a) || (tj > ti));
                             if (ok && r2 < rp2w) hit = 1;
                         }
                     if (hit) m[h] |= 1u << a;

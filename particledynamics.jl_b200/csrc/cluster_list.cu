@@ -53,9 +53,10 @@ __global__ void k_bin(const float *__restrict__ x, const float *__restrict__ y, 
         yw = 0.f;
         zw = 0.f;
     }
-    int cx = min((int)__fmul_rn(__fdiv_rn(xw, Lx), (float)ncx), ncx - 1);
-    int cy = min((int)__fmul_rn(__fdiv_rn(yw, Ly), (float)ncy), ncy - 1);
-    int cz = min((int)__fmul_rn(__fdiv_rn(zw, Lz), (float)nzb), nzb - 1);
+    // Far outside the box the wrap can round just below 0 or above L: clamp both ends.
+    const int cx = max(0, min((int)__fmul_rn(__fdiv_rn(xw, Lx), (float)ncx), ncx - 1));
+    const int cy = max(0, min((int)__fmul_rn(__fdiv_rn(yw, Ly), (float)ncy), ncy - 1));
+    const int cz = max(0, min((int)__fmul_rn(__fdiv_rn(zw, Lz), (float)nzb), nzb - 1));
     int key = (cx + ncx * cy) * nzb + cz;
     bin[i] = key;
     atomicAdd(&bcnt[key], 1);
@@ -204,7 +205,7 @@ __global__ void __launch_bounds__(64) k_assign(const int *__restrict__ sorted, c
     __shared__ float4 cc[8], ch[8];
     if (S >= NS) {  // unused super-cluster: padding everywhere
         perm[base + t] = -1;
-        xq[base + t] = make_float4(nanf_, nanf_, nanf_, 0.f);
+        xq[base + t] = pad_point(base + t);
         ts[base + t] = 1;
         if (t < 8) {
             cbc[S * 8 + t] = make_float4(nanf_, nanf_, nanf_, 0.f);
@@ -292,7 +293,7 @@ __global__ void __launch_bounds__(64) k_assign(const int *__restrict__ sorted, c
         ts[base + t] = type ? type[pi] : 1;
         ref_build[pi] = make_float4(v.x, v.y, v.z, 0.f);
     } else {
-        xq[base + t] = make_float4(nanf_, nanf_, nanf_, 0.f);
+        xq[base + t] = pad_point(base + t);
         ts[base + t] = 1;
     }
     // cluster boxes from the build coordinates (8 consecutive lanes = one cluster)
@@ -447,18 +448,40 @@ __global__ void __launch_bounds__(1024) k_entry_scan(const int *__restrict__ cnt
 
 // Distance-only prune of the outer list (_prune_only_kernel!, Kernels.jl:349-394)
 // fused with the compaction (_compact_warp_kernel!, List.jl:719-759): one CTA of
-// eight warps per super-cluster, four entries in flight (two warps per entry,
-// one per j half).  A tile is kept when any pair lies inside the prune radius,
-// widened by the rounding bound of a branch-free nearest image.  The kept
-// entries are written in order at the start of the super-cluster's own outer
-// segment, so no global scan is needed.  The prune reference coordinates of
-// the super-cluster's particles are refreshed here.
+// eight warps per super-cluster.  A tile is kept when any pair lies inside the
+// prune radius, widened by the rounding bound of a branch-free nearest image.
+// The kept entries are written in order at the start of the super-cluster's own
+// outer segment, so no global scan is needed.  The prune reference coordinates
+// of the super-cluster's particles are refreshed here.
 //
-// Bit 16 of a kept entry's mask word marks tiles that may need the periodic
-// (compensated) difference before the next prune: an atom within half the
-// prune buffer of a box face (it can wrap before the displacement trigger
-// forces a new prune) or a separation component above L/2 - prune_buffer.
-// Unmarked tiles take the plain difference in the pair kernel.
+// Layout: the segment's entries are staged in shared memory; a warp takes four
+// consecutive entries at a time, lane l loading atom l & 7 of entry l >> 3 (one
+// coalesced 512-byte load), and prefetches its next group while it evaluates the
+// current one.  For each entry, lane (ti, q) pairs i-atom ti of every i-cluster
+// in the mask with j-atoms q and q + 4 (the two j halves), taken from the loading
+// lanes by shuffles.
+//
+// Face codes: an atom's side bits mark coordinates within m = 1.01 r_p + prune
+// buffer of a face (bit 2d for +, 2d+1 for - in dimension d) and bit 6 marks
+// coordinates within half the prune buffer of a face (it may wrap before the
+// displacement trigger forces a new prune).  A pair can be nearer as a periodic
+// image than as a plain difference only if its atoms sit within r_p of opposite
+// faces, so an entry whose i- and j-side bits do not face each other takes the
+// plain difference, which then equals the nearest image bit for bit; the other
+// entries take the nearest image.  Bit 16 of a kept entry's mask word marks the
+// tiles with facing sides or a bit-6 atom: the pair kernel takes the compensated
+// periodic difference for those and the plain one for the rest.  Padding slots
+// (coordinates above PAD_LIMIT) carry no code and never pass the distance test.
+constexpr int PRUNE_CHUNK = 512;
+
+__device__ __forceinline__ int face_code(float x, float y, float z, float slx, float sly, float slz, float wlx,
+                                         float wly, float wlz) {
+    int c = (x > slx ? 1 : 0) | (x < -slx ? 2 : 0) | (y > sly ? 4 : 0) | (y < -sly ? 8 : 0) | (z > slz ? 16 : 0) |
+            (z < -slz ? 32 : 0);
+    if (fabsf(x) > wlx || fabsf(y) > wly || fabsf(z) > wlz) c |= 64;
+    return c;
+}
+
 __global__ void __launch_bounds__(256) k_prune(const float4 *__restrict__ xq, const int *__restrict__ perm,
                                                const int *__restrict__ scio, const uint32_t *__restrict__ cjo,
                                                uint2 *__restrict__ cjw, int *__restrict__ nw,
@@ -468,84 +491,150 @@ __global__ void __launch_bounds__(256) k_prune(const float4 *__restrict__ xq, co
     if (counts[W_ERR] != 0) return;
     const int S = blockIdx.x;
     if (S >= counts[W_NS]) return;
-    __shared__ float4 si[SUPER];
+    __shared__ float4 si[SUPER];   // i-atom coordinates; .w = 1 for padding
+    __shared__ int s_or[256];      // OR of the i-cluster face codes for every i-mask
+    __shared__ int s_cc[8];
+    __shared__ uint32_t s_ent[PRUNE_CHUNK];
+    __shared__ uint32_t s_res[PRUNE_CHUNK];
+    __shared__ int s_wtot[8];
     const int t = threadIdx.x;
+    const float wlx = __fsub_rn(__fmul_rn(0.5f, Lx), __fmul_rn(0.5f, pbuf));
+    const float wly = __fsub_rn(__fmul_rn(0.5f, Ly), __fmul_rn(0.5f, pbuf));
+    const float wlz = __fsub_rn(__fmul_rn(0.5f, Lz), __fmul_rn(0.5f, pbuf));
+    const float mg = __fadd_rn(__fmul_rn(1.01f, sqrtf(rp2)), pbuf);
+    const float slx = __fsub_rn(__fmul_rn(0.5f, Lx), mg);
+    const float sly = __fsub_rn(__fmul_rn(0.5f, Ly), mg);
+    const float slz = __fsub_rn(__fmul_rn(0.5f, Lz), mg);
     if (t < SUPER) {
-        float4 v = xq[S * SUPER + t];
-        si[t] = v;
-        int p = perm[S * SUPER + t];
+        const float4 v = xq[S * SUPER + t];
+        const bool pad = v.x > PAD_LIMIT;
+        int c = pad ? 0 : face_code(v.x, v.y, v.z, slx, sly, slz, wlx, wly, wlz);
+        c |= __shfl_xor_sync(0xffffffffu, c, 1);
+        c |= __shfl_xor_sync(0xffffffffu, c, 2);
+        c |= __shfl_xor_sync(0xffffffffu, c, 4);
+        if ((t & 7) == 0) s_cc[t >> 3] = c;
+        si[t] = make_float4(v.x, v.y, v.z, pad ? 1.f : 0.f);
+        const int p = perm[S * SUPER + t];
         if (p >= 0) ref_prune[p] = make_float4(v.x, v.y, v.z, 0.f);
     }
     __syncthreads();
+    {
+        int c = 0;
+#pragma unroll
+        for (int a = 0; a < 8; ++a) c |= ((t >> a) & 1) ? s_cc[a] : 0;
+        s_or[t] = c;
+    }
     const float iLx = 1.f / Lx, iLy = 1.f / Ly, iLz = 1.f / Lz;
     const float Lmax = fmaxf(Lx, fmaxf(Ly, Lz));
     const float epsf = 1.1920929e-7f;
     const float rp2w = __fadd_rn(rp2, __fmul_rn(epsf, __fadd_rn(__fmul_rn(__fmul_rn(16.f, sqrtf(rp2)), Lmax),
                                                                 __fmul_rn(16.f, rp2))));
     const int w = t >> 5, lane = t & 31;
-    const int g = w >> 1, h = w & 1;
-    const int ti = lane & 7, tj = h * 4 + (lane >> 3);
-    const float wlx = __fsub_rn(__fmul_rn(0.5f, Lx), __fmul_rn(0.5f, pbuf));
-    const float wly = __fsub_rn(__fmul_rn(0.5f, Ly), __fmul_rn(0.5f, pbuf));
-    const float wlz = __fsub_rn(__fmul_rn(0.5f, Lz), __fmul_rn(0.5f, pbuf));
-    const float dlx = __fsub_rn(__fmul_rn(0.5f, Lx), pbuf);
-    const float dly = __fsub_rn(__fmul_rn(0.5f, Ly), pbuf);
-    const float dlz = __fsub_rn(__fmul_rn(0.5f, Lz), pbuf);
+    const int ti = lane & 7, q = lane >> 3;
     const int e0 = scio[S], e1 = scio[S + 1];
-    // Chunks of PCH entries: each warp pair evaluates every fourth entry of the chunk and
-    // records its j-half mask; warp 0 then compacts the chunk in order with ballots.
-    constexpr int PCH = 256;
-    __shared__ uint32_t sm_ent[PCH];
-    __shared__ uint32_t sm_half[2][PCH];
-    int nkeep = 0;  // running kept count (warp 0)
-    for (int cb = e0; cb < e1; cb += PCH) {
-        const int ce = min(e1, cb + PCH);
-        for (int e = cb + g; e < ce; e += 4) {
-            uint32_t pm = 0;
-            bool pbc = false;
-            const uint32_t ent = cjo[e];
-            const int cj = (int)(ent >> 8);
-            const uint32_t imask = ent & 0xffu;
-            const float4 pj = xq[cj * 8 + tj];
-            const bool jnear = fabsf(pj.x) > wlx || fabsf(pj.y) > wly || fabsf(pj.z) > wlz;
+    int nkeep = 0;
+    for (int cb = e0; cb < e1; cb += PRUNE_CHUNK) {
+        const int nch = min(e1 - cb, PRUNE_CHUNK);
+        for (int k = t; k < nch; k += blockDim.x) s_ent[k] = cjo[cb + k];
+        __syncthreads();
+        const int ngroups = (nch + 3) >> 2;
+        // loader role: atom (lane & 7) of entry 4 g + (lane >> 3)
+        auto load = [&](int g) {
+            const int k = 4 * g + (lane >> 3);
+            return (g < ngroups && k < nch) ? xq[(int)(s_ent[k] >> 8) * 8 + (lane & 7)]
+                                            : make_float4(2.f * PAD_LIMIT, 2.f * PAD_LIMIT, 2.f * PAD_LIMIT, 0.f);
+        };
+        float4 nxt = load(w);
+        for (int g = w; g < ngroups; g += 8) {
+            const float4 cur = nxt;
+            nxt = load(g + 8);
+            const bool lpad = cur.x > PAD_LIMIT;
+            int jc = lpad ? 0 : face_code(cur.x, cur.y, cur.z, slx, sly, slz, wlx, wly, wlz);
+            jc |= __shfl_xor_sync(0xffffffffu, jc, 1);
+            jc |= __shfl_xor_sync(0xffffffffu, jc, 2);
+            jc |= __shfl_xor_sync(0xffffffffu, jc, 4);
+#pragma unroll 1
+            for (int kk = 0; kk < 4; ++kk) {
+                const int k = 4 * g + kk;
+                if (k >= nch) break;   // uniform per warp
+                const uint32_t ent = s_ent[k];
+                const int cj = (int)(ent >> 8);
+                const uint32_t imask = ent & 0xffu;
+                const int sa = kk * 8 + q, sb = sa + 4;
+                const float ax = __shfl_sync(0xffffffffu, cur.x, sa), ay = __shfl_sync(0xffffffffu, cur.y, sa),
+                            az = __shfl_sync(0xffffffffu, cur.z, sa);
+                const float bx = __shfl_sync(0xffffffffu, cur.x, sb), by = __shfl_sync(0xffffffffu, cur.y, sb),
+                            bz = __shfl_sync(0xffffffffu, cur.z, sb);
+                const int jcode = __shfl_sync(0xffffffffu, jc, kk * 8);
+                const int icode = s_or[imask];
+                const int jswap = ((jcode & 0x15) << 1) | ((jcode >> 1) & 0x15);
+                const bool cross = (icode & jswap & 0x3f) != 0;
+                const bool mark = cross || ((icode | jcode) & 64);
+                uint32_t lo = 0, hi = 0;
+                if (!cross) {
 #pragma unroll
-            for (int a = 0; a < 8; ++a) {
-                if ((imask >> a) & 1u) {
-                    const float4 p = si[a * 8 + ti];
-                    const float rx = p.x - pj.x, ry = p.y - pj.y, rz = p.z - pj.z;
-                    pbc = pbc || jnear || fabsf(p.x) > wlx || fabsf(p.y) > wly || fabsf(p.z) > wlz ||
-                          fabsf(rx) > dlx || fabsf(ry) > dly || fabsf(rz) > dlz;
-                    const float dx = fmaf(-Lx, rintf(rx * iLx), rx);
-                    const float dy = fmaf(-Ly, rintf(ry * iLy), ry);
-                    const float dz = fmaf(-Lz, rintf(rz * iLz), rz);
-                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                    const bool ok = ((cj != S * 8 + a) || (tj > ti)) && (r2 < __int_as_float(0x7f800000));
-                    const bool keep = __any_sync(0xffffffffu, ok && r2 < rp2w);
-                    pm |= keep ? (1u << a) : 0u;
+                    for (int a = 0; a < 8; ++a) {
+                        if ((imask >> a) & 1u) {
+                            const float4 p = si[a * 8 + ti];
+                            const float rax = p.x - ax, ray = p.y - ay, raz = p.z - az;
+                            const float rbx = p.x - bx, rby = p.y - by, rbz = p.z - bz;
+                            const float r2a = fmaf(rax, rax, fmaf(ray, ray, raz * raz));
+                            const float r2b = fmaf(rbx, rbx, fmaf(rby, rby, rbz * rbz));
+                            const bool self = cj == S * 8 + a;
+                            const bool okA = r2a < rp2w && (!self || q > ti);
+                            const bool okB = r2b < rp2w && (!self || q + 4 > ti);
+                            lo |= __any_sync(0xffffffffu, okA) ? (1u << a) : 0u;
+                            hi |= __any_sync(0xffffffffu, okB) ? (1u << a) : 0u;
+                        }
+                    }
+                } else {
+                    const bool apad = __shfl_sync(0xffffffffu, lpad, sa), bpad = __shfl_sync(0xffffffffu, lpad, sb);
+#pragma unroll
+                    for (int a = 0; a < 8; ++a) {
+                        if ((imask >> a) & 1u) {
+                            const float4 p = si[a * 8 + ti];
+                            const bool ipad = p.w != 0.f;
+                            const float rax = p.x - ax, ray = p.y - ay, raz = p.z - az;
+                            const float rbx = p.x - bx, rby = p.y - by, rbz = p.z - bz;
+                            const float dax = fmaf(-Lx, rintf(rax * iLx), rax);
+                            const float day = fmaf(-Ly, rintf(ray * iLy), ray);
+                            const float daz = fmaf(-Lz, rintf(raz * iLz), raz);
+                            const float dbx = fmaf(-Lx, rintf(rbx * iLx), rbx);
+                            const float dby = fmaf(-Ly, rintf(rby * iLy), rby);
+                            const float dbz = fmaf(-Lz, rintf(rbz * iLz), rbz);
+                            const float r2a = fmaf(dax, dax, fmaf(day, day, daz * daz));
+                            const float r2b = fmaf(dbx, dbx, fmaf(dby, dby, dbz * dbz));
+                            const bool self = cj == S * 8 + a;
+                            const bool okA = !ipad && !apad && r2a < rp2w && (!self || q > ti);
+                            const bool okB = !ipad && !bpad && r2b < rp2w && (!self || q + 4 > ti);
+                            lo |= __any_sync(0xffffffffu, okA) ? (1u << a) : 0u;
+                            hi |= __any_sync(0xffffffffu, okB) ? (1u << a) : 0u;
+                        }
+                    }
                 }
-            }
-            pbc = __any_sync(0xffffffffu, pbc);
-            if (lane == 0) {
-                sm_half[h][e - cb] = pm | (pbc ? 0x100u : 0u);
-                if (h == 0) sm_ent[e - cb] = (uint32_t)cj;
+                if (lane == 0) s_res[k] = lo | (hi << 8) | (mark ? 0x10000u : 0u);
             }
         }
         __syncthreads();
-        if (w == 0) {
-            for (int k = lane; k < ((ce - cb + 31) & ~31); k += 32) {
-                uint32_t m = 0, cj = 0;
-                if (k < ce - cb) {
-                    const uint32_t a0 = sm_half[0][k], a1 = sm_half[1][k];
-                    m = (a0 & 0xffu) | ((a1 & 0xffu) << 8) | (((a0 | a1) & 0x100u) << 8);
-                    cj = sm_ent[k];
-                }
-                const bool live = (m & 0xffffu) != 0;
-                const unsigned bal = __ballot_sync(0xffffffffu, live);
-                if (live) cjw[e0 + nkeep + __popc(bal & ((1u << lane) - 1u))] = make_uint2(cj, m);
-                nkeep += __popc(bal);
+        // in-order compaction of the chunk by the whole block
+        for (int base = 0; base < nch; base += blockDim.x) {
+            const int k = base + t;
+            const uint32_t m = k < nch ? s_res[k] : 0u;
+            const bool live = (m & 0xffffu) != 0;
+            const unsigned bal = __ballot_sync(0xffffffffu, live);
+            if (lane == 0) s_wtot[w] = __popc(bal);
+            __syncthreads();
+            int off = 0, tot = 0;
+#pragma unroll
+            for (int v = 0; v < 8; ++v) {
+                const int c = s_wtot[v];
+                off += v < w ? c : 0;
+                tot += c;
             }
+            if (live) cjw[e0 + nkeep + off + __popc(bal & ((1u << lane) - 1u))] = make_uint2(s_ent[k] >> 8, m);
+            nkeep += tot;
+            __syncthreads();
         }
-        __syncthreads();
     }
     if (t == 0) nw[S] = nkeep;
 }
@@ -635,7 +724,7 @@ __global__ void k_pack(const int *__restrict__ perm, int nslot, const float *__r
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= nslot) return;
     int i = perm[s];
-    if (i < 0) return;  // padding keeps its NaN coordinates and zero charge
+    if (i < 0) return;  // padding keeps its far-away coordinates and zero charge
     xq[s] = make_float4(force_coordinate(x[i], Lx), force_coordinate(y[i], Ly), force_coordinate(z[i], Lz),
                         q ? q[i] : 0.f);
     if (type) ts[s] = type[i];

@@ -6,11 +6,13 @@
 // library: one 64-thread CTA (two warps) per super-cluster part; thread
 // (ti, tj) = (tid & 7, tid >> 3) pairs i-atom ti of each of the 8 i-clusters
 // with j-atom tj of the current j-cluster.  The 64 i-atoms live in shared
-// memory as packed float4 (x, y, z, q); j-atoms are read as one float4 each,
+// memory as packed float4 (x, y, z, C q); j-atoms are read as one float4 each,
 // with the next entry's j-atom prefetched into registers while the current
 // entry is evaluated.  j-forces are reduced over the 8 ti lanes by shuffles and
 // added with three fence-free reductions; i-forces stay in registers and are
 // reduced once per CTA.
+#include <type_traits>
+
 #include "common.cuh"
 #include "internal.hpp"
 
@@ -69,7 +71,11 @@ __global__ void __launch_bounds__(64) k_pairs(const float4 *__restrict__ xq, con
     __shared__ float4 sxq[SUPER];
     __shared__ int sty[SUPER];
     __shared__ float4 stab[LJK == PD_LJ_TABLE ? PD_MAX_TYPES * PD_MAX_TYPES : 1];
-    sxq[tid] = xq[S * SUPER + tid];
+    {
+        float4 v = xq[S * SUPER + tid];
+        if (COUL) v.w *= pp.C;
+        sxq[tid] = v;
+    }
     if (LJK == PD_LJ_TABLE) {
         sty[tid] = (ts[S * SUPER + tid] - 1) * pp.ntypes;
         for (int k = tid; k < pp.ntypes * pp.ntypes; k += SUPER)
@@ -78,7 +84,6 @@ __global__ void __launch_bounds__(64) k_pairs(const float4 *__restrict__ xq, con
     __syncthreads();
     const float Lx = pp.Lx, Ly = pp.Ly, Lz = pp.Lz;
     const float hx = 0.5f * Lx, hy = 0.5f * Ly, hz = 0.5f * Lz;
-    const float inf = __int_as_float(0x7f800000);
     float cpf[NP], cpe[NP];
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
@@ -99,35 +104,30 @@ __global__ void __launch_bounds__(64) k_pairs(const float4 *__restrict__ xq, con
     uint2 ent = ea < eb ? cjw[ea] : make_uint2(0u, 0u);
     float4 pj = ea < eb ? xq[(int)ent.x * 8 + tj] : make_float4(0.f, 0.f, 0.f, 0.f);
     int tyj = (LJK == PD_LJ_TABLE && ea < eb) ? ts[(int)ent.x * 8 + tj] : 1;
-    for (int e = ea; e < eb; ++e) {
-        const uint2 cur = ent;
-        const float4 cpj = pj;
-        const int ctyj = tyj;
-        if (e + 1 < eb) {
-            ent = cjw[e + 1];
-            pj = xq[(int)ent.x * 8 + tj];
-            if (LJK == PD_LJ_TABLE) tyj = ts[(int)ent.x * 8 + tj];
-        }
-        const uint32_t imask = (cur.y >> (8 * w)) & 0xffu;
-        if (imask == 0) continue;   // uniform per warp
-        const bool pbc = (cur.y >> 16) & 1u;   // tile may cross a box face before the next prune
-        const int cj = (int)cur.x;
-        const int js = cj * 8 + tj;
+    // One tile: the 8 i-clusters of the mask against j-cluster cj.  DIAG tiles hold the
+    // i-cluster itself (cj == S * 8 + a for one a) and mask the self and double-counted
+    // pairs; marked (pbc) tiles take the compensated periodic difference
+    // (PeriodicDisplacement.jl:4-14).  Padding atoms sit far away with zero charge and
+    // contribute exact zeros without a mask.
+    auto tile = [&](auto diag_c, bool pbc, uint32_t imask, int cj, float4 cpj, int ctyj, int js) {
+        constexpr bool DIAG = decltype(diag_c)::value;
         float fjx = 0.f, fjy = 0.f, fjz = 0.f;
         float ej = 0.f, vj1 = 0.f, vj2 = 0.f, vj3 = 0.f, vj4 = 0.f, vj5 = 0.f, vj6 = 0.f;
 #pragma unroll
         for (int a = 0; a < 8; ++a) {
             if ((imask >> a) & 1u) {
                 const float4 pi = sxq[a * 8 + ti];
-                float dx = pi.x - cpj.x, dy = pi.y - cpj.y, dz = pi.z - cpj.z;
-                // compensated periodic difference (PeriodicDisplacement.jl:4-14) for marked tiles only
+                float dx, dy, dz;
                 if (pbc) {
                     dx = periodic_delta(pi.x, cpj.x, hx, Lx);
                     dy = periodic_delta(pi.y, cpj.y, hy, Ly);
                     dz = periodic_delta(pi.z, cpj.z, hz, Lz);
+                } else {
+                    dx = pi.x - cpj.x;
+                    dy = pi.y - cpj.y;
+                    dz = pi.z - cpj.z;
                 }
                 const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                const bool ok = ((cj != S * 8 + a) || (tj > ti)) && (r2 < inf);
                 const float rinv = rsqrtf(r2);
                 const float rinv2 = rinv * rinv;
                 float f = 0.f, en = 0.f;
@@ -151,32 +151,38 @@ __global__ void __launch_bounds__(64) k_pairs(const float4 *__restrict__ xq, con
                     if (ENERGY) en += use ? (c12 * ir6 - c6) * ir6 - esh : 0.f;
                 }
                 if (COUL) {
+                    // pi.w holds C q_i (premultiplied when the i-atoms were staged)
                     const bool inr = r2 < pp.rc2;
                     const float x = fmaf(r2, pp.sx, -1.f);
                     const float pf = horner(cpf, x);
                     const float rinv3 = rinv * rinv2;
-                    const float cq = pp.C * (pi.w * cpj.w);
-                    f += cq * (inr ? rinv3 - pf : 0.f);
+                    const float cq = pi.w * cpj.w;
+                    f = fmaf(cq, inr ? rinv3 - pf : 0.f, f);
                     if (ENERGY) {
                         const float pe = horner(cpe, x);
-                        en += cq * (inr ? rinv + pe - pp.eshift : 0.f);
+                        en = fmaf(cq, inr ? rinv + pe - pp.eshift : 0.f, en);
                     }
                 }
-                f = ok ? f : 0.f;
-                dx = ok ? dx : 0.f;
-                dy = ok ? dy : 0.f;
-                dz = ok ? dz : 0.f;
-                const float fxp = f * dx, fyp = f * dy, fzp = f * dz;
-                fxi[a] += fxp;
-                fyi[a] += fyp;
-                fzi[a] += fzp;
-                fjx -= fxp;
-                fjy -= fyp;
-                fjz -= fzp;
+                if (DIAG) {
+                    const bool ok = (cj != S * 8 + a) || (tj > ti);
+                    f = ok ? f : 0.f;
+                    en = ok ? en : 0.f;
+                    dx = ok ? dx : 0.f;
+                    dy = ok ? dy : 0.f;
+                    dz = ok ? dz : 0.f;
+                }
+                fxi[a] = fmaf(f, dx, fxi[a]);
+                fyi[a] = fmaf(f, dy, fyi[a]);
+                fzi[a] = fmaf(f, dz, fzi[a]);
+                fjx = fmaf(-f, dx, fjx);
+                fjy = fmaf(-f, dy, fjy);
+                fjz = fmaf(-f, dz, fjz);
                 if (ENERGY) {
-                    en = ok ? 0.5f * en : 0.f;
-                    const float w1 = 0.5f * fxp * dx, w2 = 0.5f * fyp * dy, w3 = 0.5f * fzp * dz;
-                    const float w4 = 0.5f * fxp * dy, w5 = 0.5f * fxp * dz, w6 = 0.5f * fyp * dz;
+                    en *= 0.5f;
+                    const float hf = 0.5f * f;
+                    const float hfx = hf * dx, hfy = hf * dy;
+                    const float w1 = hfx * dx, w2 = hfy * dy, w3 = hf * dz * dz;
+                    const float w4 = hfx * dy, w5 = hfx * dz, w6 = hfy * dz;
                     ei[a] += en;
                     w1i[a] += w1;
                     w2i[a] += w2;
@@ -206,6 +212,25 @@ __global__ void __launch_bounds__(64) k_pairs(const float4 *__restrict__ xq, con
             }
             if (ti == 0) red_add(reinterpret_cast<float *>(&fc[js]) + 3, ej);
         }
+    };
+    using T_ = std::true_type;
+    using F_ = std::false_type;
+    for (int e = ea; e < eb; ++e) {
+        const uint2 cur = ent;
+        const float4 cpj = pj;
+        const int ctyj = tyj;
+        if (e + 1 < eb) {
+            ent = cjw[e + 1];
+            pj = xq[(int)ent.x * 8 + tj];
+            if (LJK == PD_LJ_TABLE) tyj = ts[(int)ent.x * 8 + tj];
+        }
+        const uint32_t imask = (cur.y >> (8 * w)) & 0xffu;
+        if (imask == 0) continue;   // uniform per warp
+        const bool pbc = (cur.y >> 16) & 1u;   // tile may cross a box face before the next prune
+        const int cj = (int)cur.x;
+        const int js = cj * 8 + tj;
+        if ((unsigned)(cj - S * 8) < 8u) tile(T_{}, pbc, imask, cj, cpj, ctyj, js);
+        else tile(F_{}, pbc, imask, cj, cpj, ctyj, js);
     }
     const int lane = tid & 31;
 #pragma unroll

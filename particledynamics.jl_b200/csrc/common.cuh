@@ -68,6 +68,20 @@ __device__ __forceinline__ float mic(float d, float L) {
     return d;
 }
 
+// Padding slots of the packed coordinates hold far-away, pairwise distinct points and
+// zero charge: component k is 1e7 + 1000 * (k-th 10-bit digit of the slot index), so
+// two slots differ by at least 1000 in some component (all values below 1.3e7 are
+// exact in FP32).  Every pair with a padding atom then lies far beyond any cutoff on
+// the plain (non-wrapping) difference and its LJ and Coulomb terms are exact zeros
+// without masking.  Real coordinates stay far below PAD_LIMIT.
+constexpr float PAD_BASE = 1.0e7f;
+constexpr float PAD_STEP = 1000.0f;
+constexpr float PAD_LIMIT = 1.0e6f;
+__device__ __forceinline__ float4 pad_point(int slot) {
+    return make_float4(PAD_BASE + PAD_STEP * (float)(slot & 1023), PAD_BASE + PAD_STEP * (float)((slot >> 10) & 1023),
+                       PAD_BASE + PAD_STEP * (float)(slot >> 20), 0.f);
+}
+
 __device__ __forceinline__ float warp_max(float v) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, off));

@@ -192,18 +192,26 @@ __global__ void k_sum(const float *__restrict__ v, int n, double *__restrict__ o
 
 }  // namespace pdb
 
-// Closing part of a step: pair pass beside the mesh transform, then the join.
+// The mesh transform forks onto the side stream as soon as the packed coordinates
+// of the step exist (after the pack or build), so that it runs beside the prune and
+// the pair pass; it reads only the packed coordinates and the super-cluster count.
+static int fork_mesh(pd_md *md, int energy, cudaStream_t s) {
+    if (!md->m) return PD_OK;
+    pd_cluster *c = md->c;
+    int rc;
+    PD_CUDA(cudaEventRecord(md->ev_fork, s));
+    PD_CUDA(cudaStreamWaitEvent(md->side, md->ev_fork, 0));
+    if ((rc = mesh_transform_packed(md->m, c->xq, c->nsmax, c->counts + W_NS, energy, md->side))) return rc;
+    PD_CUDA(cudaEventRecord(md->ev_join, md->side));
+    return PD_OK;
+}
+
+// Closing part of a step: the pair pass (the mesh transform already forked), then the join.
 static int enqueue_forces(pd_md *md, int energy, float half_dt, cudaStream_t s) {
     pd_cluster *c = md->c;
     pd_mesh *m = md->m;
     pd_md_state &st = md->st;
     int rc;
-    if (m) {
-        PD_CUDA(cudaEventRecord(md->ev_fork, s));
-        PD_CUDA(cudaStreamWaitEvent(md->side, md->ev_fork, 0));
-        if ((rc = mesh_transform_packed(m, c->xq, c->nsmax, c->counts + W_NS, energy, md->side))) return rc;
-        PD_CUDA(cudaEventRecord(md->ev_join, md->side));
-    }
     if ((rc = cluster_pairs_launch(c, energy, s))) return rc;
     if (m) {
         PD_CUDA(cudaStreamWaitEvent(s, md->ev_join, 0));
@@ -283,12 +291,14 @@ static int enqueue_step(pd_md *md, float dt, int energy, cudaStream_t s, int con
                  return cluster_build_launch(c, st.x, st.y, st.z, q, st.type, 1, cs);
              })))
             return rc;
+        if ((rc = fork_mesh(md, energy, s))) return rc;
         if ((rc = capture_if(s, md->body, hprune, [&](cudaStream_t cs) { return cluster_prune_launch(c, 1, cs); })))
             return rc;
     } else {
         k_decide_step<false><<<1, 1, 0, s>>>(c->counts, c->p.nstlist, c->p.nstprune, 0, 0);
         PD_LAUNCHED();
         if ((rc = cluster_build_launch(c, st.x, st.y, st.z, q, st.type, 1, s))) return rc;
+        if ((rc = fork_mesh(md, energy, s))) return rc;
         if ((rc = cluster_prune_launch(c, 1, s))) return rc;
     }
     return enqueue_forces(md, energy, 0.5f * dt, s);
@@ -371,6 +381,7 @@ int pd_md_evaluate(pd_md *md, int energy, pd_stream_t sp) {
     } else {
         if ((rc = pd_cluster_pack(c, st.x, st.y, st.z, q, st.type, sp))) return rc;
     }
+    if ((rc = fork_mesh(md, energy, s))) return rc;
     if ((rc = cluster_prune_launch(c, 1, s))) return rc;
     return enqueue_forces(md, energy, 0.f, s);
 }

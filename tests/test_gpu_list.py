@@ -39,7 +39,9 @@ def test_list_bit_exact(pd, ora, cuda, n, box, rc, skin, prune, seed):
     for d in range(3):
         fc = ora.force_coordinate(pos[perm[occ], d], box[d])
         assert np.array_equal(gpu["xq"][:64 * ref["ns"]][occ, d], fc)
-    assert np.all(np.isnan(gpu["xq"][:64 * ref["ns"]][~occ, 0]))
+    pad = gpu["xq"][:64 * ref["ns"]][~occ]
+    assert np.all(pad[:, :3] > 1e6) and np.all(pad[:, 3] == 0)
+    assert len(np.unique(pad[:, :3], axis=0)) == len(pad)
     # pruned working list from the GPU's packed coordinates
     cjw, nw = ora.cluster_prune(ref["ns"], gpu["xq"][:64 * ref["ns"]].reshape(-1), ref["scio"], ref["cjo"], box,
                                 rc + prune, prune)
@@ -53,6 +55,29 @@ def test_list_bit_exact(pd, ora, cuda, n, box, rc, skin, prune, seed):
     rows = ora.neighbor_rows(pos.astype(np.float64), box, rc * (1 - 1e-6))
     need = {(min(i, j), max(i, j)) for i, r in enumerate(rows) for j in r}
     assert need <= set(pairs)
+    eng.close()
+
+
+def test_far_coordinates_stay_in_range(pd, ora, cuda):
+    # Finite coordinates billions of box lengths away wrap with a rounding error of up to half an
+    # ulp (here 128), so the wrapped value can fall below 0 or above L; the column and z-bin
+    # indices are clamped, and the list still equals the oracle's bit for bit.
+    rng = np.random.default_rng(5)
+    box = (12.0, 12.0, 12.0)
+    n = 2000
+    pos = (rng.random((n, 3)) * 12 - 6).astype(np.float32)
+    far = rng.choice(n, 200, replace=False)
+    pos[far] = (rng.uniform(-1, 1, (200, 3)) * 3e9).astype(np.float32)
+    wrapped = pos[far] - np.float32(12.0) * np.floor(pos[far] / np.float32(12.0))
+    assert (wrapped < 0).any() or (wrapped >= 12.0).any()
+    eng = _build(pd, pos.astype(np.float64), box, 1.5, 0.3, 0.1)
+    gpu = eng.list_host()
+    ref = ora.cluster_build(pos, box, 1.8)
+    assert gpu["ns"] == ref["ns"]
+    perm = gpu["perm"][:64 * ref["ns"]]
+    assert np.array_equal(perm, ref["perm"][:64 * ref["ns"]])
+    assert np.array_equal(np.sort(perm[perm >= 0]), np.arange(n))
+    assert np.array_equal(gpu["scio"], ref["scio"]) and np.array_equal(gpu["cjo"], ref["cjo"])
     eng.close()
 
 
