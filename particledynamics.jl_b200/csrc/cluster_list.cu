@@ -95,6 +95,8 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int *warp_tot, int *t
 // Exclusive scan of the bin histogram (resetting it to zero for the next build),
 // then the per-column super-cluster counts, offsets and metadata
 // (_exclusive_kernel!, _super_count/_super_offsets/_super_meta_kernel!, List.jl:253-298).
+constexpr int SCAN_CHUNK = 8192;   // bins per pass of k_bin_scan (32 KiB of shared memory)
+
 __global__ void __launch_bounds__(1024) k_bin_scan(int *__restrict__ bcnt, int *__restrict__ bstart,
                                                    int *__restrict__ cursor, int nbin, int nzb, int ncol,
                                                    int *__restrict__ col_sc_off, int *__restrict__ sc_first,
@@ -103,17 +105,41 @@ __global__ void __launch_bounds__(1024) k_bin_scan(int *__restrict__ bcnt, int *
     if (gated && counts[W_BUILD] == 0) return;
     __shared__ int warp_tot[32];
     __shared__ int total;
+    // chunks of SCAN_CHUNK bins: coalesced load into shared memory (skewed by one word per
+    // 32 against bank conflicts), a serial scan of 8 consecutive bins per thread, one block
+    // scan of the thread totals, coalesced store
+    __shared__ int sb[SCAN_CHUNK + SCAN_CHUNK / 32];
+    const int t = threadIdx.x;
     int carry = 0;
-    for (int base = 0; base < nbin; base += blockDim.x) {
-        int idx = base + threadIdx.x;
-        int v = idx < nbin ? bcnt[idx] : 0;
-        int ex = block_exclusive_scan(v, warp_tot, &total) + carry;
-        if (idx < nbin) {
-            bstart[idx] = ex;
-            cursor[idx] = ex;
-            bcnt[idx] = 0;
+    for (int c0 = 0; c0 < nbin; c0 += SCAN_CHUNK) {
+        const int nc = min(SCAN_CHUNK, nbin - c0);
+        for (int k = t; k < SCAN_CHUNK; k += blockDim.x) {
+            sb[k + (k >> 5)] = k < nc ? bcnt[c0 + k] : 0;
+            if (k < nc) bcnt[c0 + k] = 0;
+        }
+        __syncthreads();
+        constexpr int PER = SCAN_CHUNK / 1024;
+        int run = 0;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int i = t * PER + k;
+            run += sb[i + (i >> 5)];
+        }
+        int ex = block_exclusive_scan(run, warp_tot, &total) + carry;
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int i = t * PER + k;
+            const int v = sb[i + (i >> 5)];
+            sb[i + (i >> 5)] = ex;
+            ex += v;
         }
         carry += total;
+        __syncthreads();
+        for (int k = t; k < nc; k += blockDim.x) {
+            const int v = sb[k + (k >> 5)];
+            bstart[c0 + k] = v;
+            cursor[c0 + k] = v;
+        }
         __syncthreads();
     }
     if (threadIdx.x == 0) bstart[nbin] = carry;
@@ -158,27 +184,52 @@ __global__ void k_bin_scatter(const int *__restrict__ bin, int n, int *__restric
     sorted[p] = i;
 }
 
-// Order each bin by (wrapped z, particle id): insertion sort of the few entries of a bin.
-__global__ void k_bin_sort(const int *__restrict__ bstart, int nbin, int *__restrict__ sorted,
+// Order each bin by (wrapped z, particle id), one warp per bin: every lane takes
+// entries of the bin, ranks them against all entries of the bin (the keys are
+// distinct, so the ranks form a permutation; non-finite z sorts last, by id) and
+// the warp writes the bin back in rank order.
+__device__ __forceinline__ bool zid_less(float za, int ia, float zb, int ib) {
+    const bool fa = za == za, fb = zb == zb;
+    if (fa != fb) return fa;   // finite before non-finite
+    if (fa && za != zb) return za < zb;
+    return ia < ib;
+}
+
+__global__ void k_bin_sort(const int *__restrict__ bstart, int nbin, int *__restrict__ sorted, int *__restrict__ tmp,
                            const float *__restrict__ z, float Lz, const int *__restrict__ counts, int gated) {
     if (gated && counts[W_BUILD] == 0) return;
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= nbin) return;
-    int a = bstart[b], e = bstart[b + 1];
-    for (int k = a + 1; k < e; ++k) {
-        int id = sorted[k];
-        float zk = wrap_positive(z[id], Lz);
-        int m = k - 1;
-        while (m >= a) {
-            int jd = sorted[m];
-            float zm = wrap_positive(z[jd], Lz);
-            bool greater = (zm > zk) || (zm == zk && jd > id) || (zm != zm && zk == zk);
-            if (!greater) break;
-            sorted[m + 1] = jd;
-            --m;
+    const int b = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (b >= nbin) return;   // uniform per warp
+    const int a = bstart[b], n = bstart[b + 1] - a;
+    if (n <= 1) return;
+    if (n <= 32) {
+        const int id = lane < n ? sorted[a + lane] : 0x7fffffff;
+        const float zk = lane < n ? wrap_positive(z[id], Lz) : 0.f;
+        int r = 0;
+        for (int j = 0; j < n; ++j) {
+            const float zj = __shfl_sync(0xffffffffu, zk, j);
+            const int ij = __shfl_sync(0xffffffffu, id, j);
+            r += zid_less(zj, ij, zk, id) ? 1 : 0;
         }
-        sorted[m + 1] = id;
+        __syncwarp();
+        if (lane < n) sorted[a + r] = id;
+        return;
     }
+    // long bins: every entry is ranked against the whole bin and its id is written to its
+    // rank position in `tmp` (the bin-key array, free after the scatter); the bin is then
+    // copied back
+    for (int k = lane; k < n; k += 32) {
+        const int id = sorted[a + k];
+        const float zk = wrap_positive(z[id], Lz);
+        int r = 0;
+        for (int j = 0; j < n; ++j) {
+            const int ij = sorted[a + j];
+            r += zid_less(wrap_positive(z[ij], Lz), ij, zk, id) ? 1 : 0;
+        }
+        tmp[a + r] = id;
+    }
+    __syncwarp();
+    for (int k = lane; k < n; k += 32) sorted[a + k] = tmp[a + k];
 }
 
 // _cluster_assign_kernel! (List.jl:301-358) fused with the order, the pack of
@@ -229,10 +280,11 @@ __global__ void __launch_bounds__(64) k_assign(const int *__restrict__ sorted, c
     __syncthreads();
     int hx = 0, hy = 0, slot = -1;
     if (t < n) {
-        float xt = sx[t];
+        const float xt = sx[t];
         int r = 0;
+#pragma unroll 8
         for (int u = 0; u < n; ++u) {
-            float xu = sx[u];
+            const float xu = sx[u];
             r += ((xu < xt) || (xu == xt && u < t)) ? 1 : 0;
         }
         hx = r >= ((n + 1) >> 1) ? 1 : 0;
@@ -241,13 +293,13 @@ __global__ void __launch_bounds__(64) k_assign(const int *__restrict__ sorted, c
     __syncthreads();
     if (t < n) {
         int m = 0, r = 0;
-        float yt = sy[t];
+        const float yt = sy[t];
+#pragma unroll 8
         for (int u = 0; u < n; ++u) {
-            if (shx[u] == hx) {
-                ++m;
-                float yu = sy[u];
-                r += ((yu < yt) || (yu == yt && u < t)) ? 1 : 0;
-            }
+            const bool same = shx[u] == hx;
+            const float yu = sy[u];
+            m += same ? 1 : 0;
+            r += (same && ((yu < yt) || (yu == yt && u < t))) ? 1 : 0;
         }
         hy = r >= ((m + 1) >> 1) ? 1 : 0;
         shy[t] = hy;
@@ -255,13 +307,13 @@ __global__ void __launch_bounds__(64) k_assign(const int *__restrict__ sorted, c
     __syncthreads();
     if (t < n) {
         int m = 0, r = 0;
-        float zt = sz[t];
+        const float zt = sz[t];
+#pragma unroll 8
         for (int u = 0; u < n; ++u) {
-            if (shx[u] == hx && shy[u] == hy) {
-                ++m;
-                float zu = sz[u];
-                r += ((zu < zt) || (zu == zt && u < t)) ? 1 : 0;
-            }
+            const bool same = shx[u] == hx && shy[u] == hy;
+            const float zu = sz[u];
+            m += same ? 1 : 0;
+            r += (same && ((zu < zt) || (zu == zt && u < t))) ? 1 : 0;
         }
         int m0 = (m + 1) >> 1;
         int hz = r >= m0 ? 1 : 0;
@@ -352,43 +404,66 @@ __device__ __forceinline__ float bbgap2(float4 c1, float4 h1, float4 c2, float4 
     return __fadd_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy)), __fmul_rn(gz, gz));
 }
 
-// Outer-list search (_search_warp_kernel!, List.jl:478-557): one warp per
-// super-cluster walks its neighbouring columns in (dy, dx) order; lanes take
-// (candidate super-cluster, j-cluster) pairs and emit (cj << 8) | i-mask with
-// ballot-ordered positions, so the entry order equals a serial loop's.
+// Outer-list search (_search_warp_kernel!, List.jl:478-557): one CTA of four
+// warps per super-cluster.  The neighbouring columns are walked in (dy, dx)
+// order; warp w takes columns w, w + 4, ...; lanes take (candidate
+// super-cluster, j-cluster) pairs and emit (cj << 8) | i-mask with
+// ballot-ordered positions.  The count pass records every column's entry count,
+// so the fill pass writes each column at its own offset and the entry order
+// equals a serial loop's.
 template <bool FILL>
 __global__ void __launch_bounds__(128) k_search(const int *__restrict__ sc_col, const int *__restrict__ col_sc_off,
                                                 int ncx, int ncy, int mx, int my, const float4 *__restrict__ cbc,
                                                 const float4 *__restrict__ cbh, const float4 *__restrict__ sbc,
                                                 const float4 *__restrict__ sbh, float Lx, float Ly, float Lz,
-                                                float rl2, int *__restrict__ cnt_sc, const int *__restrict__ scio,
-                                                uint32_t *__restrict__ cjo, int *__restrict__ counts, int gated) {
+                                                float rl2, int *__restrict__ cnt_sc, int *__restrict__ colcnt, int ncs,
+                                                const int *__restrict__ scio, uint32_t *__restrict__ cjo,
+                                                int *__restrict__ counts, int gated) {
     if (gated && counts[W_BUILD] == 0) return;
     if (FILL && counts[W_ERR] != 0) return;
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int S = blockIdx.x * 4 + w;
-    __shared__ float4 ic[4][8], ih[4][8];
-    const int NS = counts[W_NS];
-    if (S >= NS) return;
-    if (lane < 8) {
-        ic[w][lane] = cbc[S * 8 + lane];
-        ih[w][lane] = cbh[S * 8 + lane];
+    const int S = blockIdx.x;
+    if (S >= counts[W_NS]) return;
+    const int t = threadIdx.x, w = t >> 5, lane = t & 31;
+    __shared__ float4 ic[8], ih[8];
+    __shared__ int s_off[SEARCH_MAX_COLS];
+    __shared__ int s_tot[4];
+    if (t < 8) {
+        ic[t] = cbc[S * 8 + t];
+        ih[t] = cbh[S * 8 + t];
     }
-    __syncwarp();
-    const float4 s1c = sbc[S], s1h = sbh[S];
     const int c = sc_col[S];
     const int cx = c % ncx, cy = c / ncx;
     const int nxr = min(2 * mx + 1, ncx), nyr = min(2 * my + 1, ncy);
+    const int ncand = nxr * nyr;   // == ncs
     const int x0 = nxr == ncx ? 0 : cx - mx;
     const int y0 = nyr == ncy ? 0 : cy - my;
-    const int out = FILL ? scio[S] : 0;
-    int n = 0;
-    for (int k = 0; k < nxr * nyr; ++k) {
+    if (FILL && w == 0) {
+        // exclusive prefix of the column counts of the count pass
+        int carry = 0;
+        for (int k0 = 0; k0 < ncand; k0 += 32) {
+            const int v = k0 + lane < ncand ? colcnt[(size_t)S * ncs + k0 + lane] : 0;
+            int inc = v;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, inc, off);
+                if (lane >= off) inc += y;
+            }
+            if (k0 + lane < ncand) s_off[k0 + lane] = carry + inc - v;
+            carry += __shfl_sync(0xffffffffu, inc, 31);
+        }
+    }
+    __syncthreads();
+    const float4 s1c = sbc[S], s1h = sbh[S];
+    const int e0 = FILL ? scio[S] : 0;
+    int total = 0;
+    for (int k = w; k < ncand; k += 4) {
         const int dy = k / nxr, dx = k % nxr;
         const int ccx = ((x0 + dx) % ncx + ncx) % ncx, ccy = ((y0 + dy) % ncy + ncy) % ncy;
         const int cc = ccx + ncx * ccy;
         int lo = col_sc_off[cc], hi = col_sc_off[cc + 1];
         lo = max(lo, S);
+        const int out = FILL ? e0 + s_off[k] : 0;
+        int n = 0;
         for (int base = lo * 8; base < hi * 8; base += 32) {
             const int idx = base + lane;
             uint32_t m = 0;
@@ -404,9 +479,9 @@ __global__ void __launch_bounds__(128) k_search(const int *__restrict__ sc_col, 
                         for (int a = 0; a < 8; ++a) {
                             const int ci = S * 8 + a;
                             if (cj < ci) continue;
-                            const float4 ac = ic[w][a];
+                            const float4 ac = ic[a];
                             if (ac.x != ac.x) continue;
-                            if (bbgap2(ac, ih[w][a], jc, jh, Lx, Ly, Lz) < rl2) m |= 1u << a;
+                            if (bbgap2(ac, ih[a], jc, jh, Lx, Ly, Lz) < rl2) m |= 1u << a;
                         }
                     }
                 }
@@ -415,8 +490,14 @@ __global__ void __launch_bounds__(128) k_search(const int *__restrict__ sc_col, 
             if (FILL && m) cjo[out + n + __popc(bal & ((1u << lane) - 1u))] = ((uint32_t)cj << 8) | m;
             n += __popc(bal);
         }
+        if (!FILL && lane == 0) colcnt[(size_t)S * ncs + k] = n;
+        total += n;
     }
-    if (!FILL && lane == 0) cnt_sc[S] = n;
+    if (!FILL) {
+        if (lane == 0) s_tot[w] = total;
+        __syncthreads();
+        if (t == 0) cnt_sc[S] = s_tot[0] + s_tot[1] + s_tot[2] + s_tot[3];
+    }
 }
 
 // scio = exclusive scan of the per-super-cluster entry counts; NE and the
@@ -494,6 +575,7 @@ __global__ void __launch_bounds__(256) k_prune(const float4 *__restrict__ xq, co
     __shared__ float4 si[SUPER];   // i-atom coordinates; .w = 1 for padding
     __shared__ int s_or[256];      // OR of the i-cluster face codes for every i-mask
     __shared__ int s_cc[8];
+    __shared__ float4 s_blo[8], s_bhi[8];   // current i-cluster boxes
     __shared__ uint32_t s_ent[PRUNE_CHUNK];
     __shared__ uint32_t s_res[PRUNE_CHUNK];
     __shared__ int s_wtot[8];
@@ -513,6 +595,23 @@ __global__ void __launch_bounds__(256) k_prune(const float4 *__restrict__ xq, co
         c |= __shfl_xor_sync(0xffffffffu, c, 2);
         c |= __shfl_xor_sync(0xffffffffu, c, 4);
         if ((t & 7) == 0) s_cc[t >> 3] = c;
+        // current box of each i-cluster over its real atoms (padding contributes nothing)
+        const float inf = __int_as_float(0x7f800000);
+        float lx = pad ? inf : v.x, ly = pad ? inf : v.y, lz = pad ? inf : v.z;
+        float ux = pad ? -inf : v.x, uy = pad ? -inf : v.y, uz = pad ? -inf : v.z;
+#pragma unroll
+        for (int off = 1; off < 8; off <<= 1) {
+            lx = fminf(lx, __shfl_xor_sync(0xffffffffu, lx, off));
+            ly = fminf(ly, __shfl_xor_sync(0xffffffffu, ly, off));
+            lz = fminf(lz, __shfl_xor_sync(0xffffffffu, lz, off));
+            ux = fmaxf(ux, __shfl_xor_sync(0xffffffffu, ux, off));
+            uy = fmaxf(uy, __shfl_xor_sync(0xffffffffu, uy, off));
+            uz = fmaxf(uz, __shfl_xor_sync(0xffffffffu, uz, off));
+        }
+        if ((t & 7) == 0) {
+            s_blo[t >> 3] = make_float4(lx, ly, lz, 0.f);
+            s_bhi[t >> 3] = make_float4(ux, uy, uz, 0.f);
+        }
         si[t] = make_float4(v.x, v.y, v.z, pad ? 1.f : 0.f);
         const int p = perm[S * SUPER + t];
         if (p >= 0) ref_prune[p] = make_float4(v.x, v.y, v.z, 0.f);
@@ -553,13 +652,27 @@ __global__ void __launch_bounds__(256) k_prune(const float4 *__restrict__ xq, co
             jc |= __shfl_xor_sync(0xffffffffu, jc, 1);
             jc |= __shfl_xor_sync(0xffffffffu, jc, 2);
             jc |= __shfl_xor_sync(0xffffffffu, jc, 4);
+            // current box of each loaded j-cluster (8 lanes each, real atoms only)
+            const float inf = __int_as_float(0x7f800000);
+            float jlx = lpad ? inf : cur.x, jly = lpad ? inf : cur.y, jlz = lpad ? inf : cur.z;
+            float jux = lpad ? -inf : cur.x, juy = lpad ? -inf : cur.y, juz = lpad ? -inf : cur.z;
+#pragma unroll
+            for (int off = 1; off < 8; off <<= 1) {
+                jlx = fminf(jlx, __shfl_xor_sync(0xffffffffu, jlx, off));
+                jly = fminf(jly, __shfl_xor_sync(0xffffffffu, jly, off));
+                jlz = fminf(jlz, __shfl_xor_sync(0xffffffffu, jlz, off));
+                jux = fmaxf(jux, __shfl_xor_sync(0xffffffffu, jux, off));
+                juy = fmaxf(juy, __shfl_xor_sync(0xffffffffu, juy, off));
+                juz = fmaxf(juz, __shfl_xor_sync(0xffffffffu, juz, off));
+            }
 #pragma unroll 1
             for (int kk = 0; kk < 4; ++kk) {
                 const int k = 4 * g + kk;
                 if (k >= nch) break;   // uniform per warp
-                const uint32_t ent = s_ent[k];
+                // the entry word is the same for every lane; the reduction makes that visible
+                const uint32_t ent = __reduce_or_sync(0xffffffffu, s_ent[k]);
                 const int cj = (int)(ent >> 8);
-                const uint32_t imask = ent & 0xffu;
+                uint32_t imask = ent & 0xffu;
                 const int sa = kk * 8 + q, sb = sa + 4;
                 const float ax = __shfl_sync(0xffffffffu, cur.x, sa), ay = __shfl_sync(0xffffffffu, cur.y, sa),
                             az = __shfl_sync(0xffffffffu, cur.z, sa);
@@ -568,10 +681,24 @@ __global__ void __launch_bounds__(256) k_prune(const float4 *__restrict__ xq, co
                 const int jcode = __shfl_sync(0xffffffffu, jc, kk * 8);
                 const int icode = s_or[imask];
                 const int jswap = ((jcode & 0x15) << 1) | ((jcode >> 1) & 0x15);
-                const bool cross = (icode & jswap & 0x3f) != 0;
+                const bool cross = __any_sync(0xffffffffu, (icode & jswap & 0x3f) != 0);
                 const bool mark = cross || ((icode | jcode) & 64);
-                uint32_t lo = 0, hi = 0;
+                uint32_t bits = 0;   // this lane's hits: bit a (j half 0), bit 8 + a (j half 1)
                 if (!cross) {
+                    // i-clusters whose box lies beyond the prune radius from the j-cluster's box hold no
+                    // pair inside it (the factor covers the rounding of the pair distances)
+                    {
+                        const int src = kk * 8;
+                        const float4 bl = s_blo[lane & 7], bh = s_bhi[lane & 7];
+                        const float gx = fmaxf(0.f, fmaxf(bl.x - __shfl_sync(0xffffffffu, jux, src),
+                                                          __shfl_sync(0xffffffffu, jlx, src) - bh.x));
+                        const float gy = fmaxf(0.f, fmaxf(bl.y - __shfl_sync(0xffffffffu, juy, src),
+                                                          __shfl_sync(0xffffffffu, jly, src) - bh.y));
+                        const float gz = fmaxf(0.f, fmaxf(bl.z - __shfl_sync(0xffffffffu, juz, src),
+                                                          __shfl_sync(0xffffffffu, jlz, src) - bh.z));
+                        const bool near = fmaf(gx, gx, fmaf(gy, gy, gz * gz)) <= 1.0001f * rp2w;
+                        imask &= __ballot_sync(0xffffffffu, near) & 0xffu;
+                    }
 #pragma unroll
                     for (int a = 0; a < 8; ++a) {
                         if ((imask >> a) & 1u) {
@@ -583,8 +710,7 @@ __global__ void __launch_bounds__(256) k_prune(const float4 *__restrict__ xq, co
                             const bool self = cj == S * 8 + a;
                             const bool okA = r2a < rp2w && (!self || q > ti);
                             const bool okB = r2b < rp2w && (!self || q + 4 > ti);
-                            lo |= __any_sync(0xffffffffu, okA) ? (1u << a) : 0u;
-                            hi |= __any_sync(0xffffffffu, okB) ? (1u << a) : 0u;
+                            bits |= (okA ? (1u << a) : 0u) | (okB ? (0x100u << a) : 0u);
                         }
                     }
                 } else {
@@ -607,12 +733,12 @@ __global__ void __launch_bounds__(256) k_prune(const float4 *__restrict__ xq, co
                             const bool self = cj == S * 8 + a;
                             const bool okA = !ipad && !apad && r2a < rp2w && (!self || q > ti);
                             const bool okB = !ipad && !bpad && r2b < rp2w && (!self || q + 4 > ti);
-                            lo |= __any_sync(0xffffffffu, okA) ? (1u << a) : 0u;
-                            hi |= __any_sync(0xffffffffu, okB) ? (1u << a) : 0u;
+                            bits |= (okA ? (1u << a) : 0u) | (okB ? (0x100u << a) : 0u);
                         }
                     }
                 }
-                if (lane == 0) s_res[k] = lo | (hi << 8) | (mark ? 0x10000u : 0u);
+                bits = __reduce_or_sync(0xffffffffu, bits);
+                if (lane == 0) s_res[k] = bits | (mark ? 0x10000u : 0u);
             }
         }
         __syncthreads();
@@ -778,6 +904,7 @@ static void free_geometry(pd_cluster *c) {
     dfree(c->sbc);
     dfree(c->sbh);
     dfree(c->cnt_sc);
+    dfree(c->colcnt);
     dfree(c->scio);
     dfree(c->nw);
     dfree(c->fc);
@@ -797,21 +924,23 @@ int cluster_build_launch(pd_cluster *c, const float *x, const float *y, const fl
     PD_LAUNCHED();
     k_bin_scatter<<<(N + 255) / 256, 256, 0, s>>>(c->bin, N, c->cursor, c->sorted, c->counts, g);
     PD_LAUNCHED();
-    k_bin_sort<<<(c->nbin + 255) / 256, 256, 0, s>>>(c->bstart, c->nbin, c->sorted, z, Lz, c->counts, g);
+    k_bin_sort<<<(int)(((long long)c->nbin * 32 + 255) / 256), 256, 0, s>>>(c->bstart, c->nbin, c->sorted, c->bin, z, Lz,
+                                                                          c->counts, g);
     PD_LAUNCHED();
     k_assign<<<c->nsmax, SUPER, 0, s>>>(c->sorted, c->sc_first, c->sc_n, x, y, z, q, type, Lx, Ly, Lz, c->perm,
                                         c->slot_of, c->order, c->xq, c->ts, c->cbc, c->cbh, c->sbc, c->sbh,
                                         c->ref_build, c->counts, g);
     PD_LAUNCHED();
     const float rl2 = (float)c->rlist * (float)c->rlist;
-    const int wblocks = (c->nsmax + 3) / 4;
-    k_search<false><<<wblocks, 128, 0, s>>>(c->sc_col, c->col_sc_off, c->ncx, c->ncy, c->mx, c->my, c->cbc, c->cbh,
-                                            c->sbc, c->sbh, Lx, Ly, Lz, rl2, c->cnt_sc, c->scio, c->cjo, c->counts, g);
+    k_search<false><<<c->nsmax, 128, 0, s>>>(c->sc_col, c->col_sc_off, c->ncx, c->ncy, c->mx, c->my, c->cbc, c->cbh,
+                                             c->sbc, c->sbh, Lx, Ly, Lz, rl2, c->cnt_sc, c->colcnt, c->ncs, c->scio,
+                                             c->cjo, c->counts, g);
     PD_LAUNCHED();
     k_entry_scan<<<1, 1024, 0, s>>>(c->cnt_sc, c->nsmax, c->scio, c->necap, c->counts, g);
     PD_LAUNCHED();
-    k_search<true><<<wblocks, 128, 0, s>>>(c->sc_col, c->col_sc_off, c->ncx, c->ncy, c->mx, c->my, c->cbc, c->cbh,
-                                           c->sbc, c->sbh, Lx, Ly, Lz, rl2, c->cnt_sc, c->scio, c->cjo, c->counts, g);
+    k_search<true><<<c->nsmax, 128, 0, s>>>(c->sc_col, c->col_sc_off, c->ncx, c->ncy, c->mx, c->my, c->cbc, c->cbh,
+                                            c->sbc, c->sbh, Lx, Ly, Lz, rl2, c->cnt_sc, c->colcnt, c->ncs, c->scio,
+                                            c->cjo, c->counts, g);
     PD_LAUNCHED();
     return PD_OK;
 }
@@ -953,7 +1082,11 @@ int pd_cluster_setup(pd_cluster *c, const double box[3]) {
     const double shrink = 0.98;
     int mx = (int)std::floor(rlist / (shrink * Lx / ncx)) + 1;
     int my = (int)std::floor(rlist / (shrink * Ly / ncy)) + 1;
-    bool same_geom = c->nslot > 0 && ncx == c->ncx && ncy == c->ncy && nzb == c->nzb && nsmax == c->nsmax;
+    const int ncs = std::min(2 * mx + 1, ncx) * std::min(2 * my + 1, ncy);
+    PD_CHECK(ncs <= SEARCH_MAX_COLS, PD_EINVAL, "cluster-pair search needs %d columns per super-cluster (limit %d).",
+             ncs, SEARCH_MAX_COLS);
+    bool same_geom = c->nslot > 0 && ncx == c->ncx && ncy == c->ncy && nzb == c->nzb && nsmax == c->nsmax &&
+                     ncs == c->ncs;
     for (int d = 0; d < 3; ++d) {
         c->box[d] = box[d];
         c->L[d] = (float)box[d];
@@ -966,13 +1099,13 @@ int pd_cluster_setup(pd_cluster *c, const double box[3]) {
     c->nbin = (int)nbin;
     c->mx = mx;
     c->my = my;
-    c->ncs = std::min(2 * mx + 1, ncx) * std::min(2 * my + 1, ncy);
     c->pp.Lx = c->L[0];
     c->pp.Ly = c->L[1];
     c->pp.Lz = c->L[2];
     c->nsplit = std::max(1, std::min(32, (32 * c->num_sms + nsmax - 1) / std::max(nsmax, 1)));
     if (!same_geom) {
         free_geometry(c);
+        c->ncs = ncs;
         c->nsmax = nsmax;
         c->nslot = nslot;
         int rc;
@@ -984,7 +1117,8 @@ int pd_cluster_setup(pd_cluster *c, const double box[3]) {
             (rc = dalloc(&c->xq, (size_t)nslot)) || (rc = dalloc(&c->ts, (size_t)nslot)) ||
             (rc = dalloc(&c->cbc, (size_t)8 * nsmax)) || (rc = dalloc(&c->cbh, (size_t)8 * nsmax)) ||
             (rc = dalloc(&c->sbc, (size_t)nsmax)) || (rc = dalloc(&c->sbh, (size_t)nsmax)) ||
-            (rc = dalloc(&c->cnt_sc, (size_t)nsmax)) || (rc = dalloc(&c->scio, (size_t)nsmax + 1)) ||
+            (rc = dalloc(&c->cnt_sc, (size_t)nsmax)) || (rc = dalloc(&c->colcnt, (size_t)nsmax * ncs)) ||
+            (rc = dalloc(&c->scio, (size_t)nsmax + 1)) ||
             (rc = dalloc(&c->nw, (size_t)nsmax)) || (rc = dalloc(&c->fc, (size_t)nslot)) ||
             (rc = dalloc(&c->vc, (size_t)6 * nslot)))
             return rc;

@@ -11,8 +11,6 @@
 // entry is evaluated.  j-forces are reduced over the 8 ti lanes by shuffles and
 // added with three fence-free reductions; i-forces stay in registers and are
 // reduced once per CTA.
-#include <type_traits>
-
 #include "common.cuh"
 #include "internal.hpp"
 
@@ -64,8 +62,8 @@ __global__ void __launch_bounds__(64) k_pairs(const float4 *__restrict__ xq, con
                                               const int *__restrict__ nw, const int *__restrict__ counts,
                                               const float *__restrict__ lj_table, float4 *__restrict__ fc,
                                               float *__restrict__ vc, int nslot, int nsplit, const PairParams pp) {
-    const int tid = threadIdx.x;
-    const int ti = tid & 7, tj = tid >> 3, w = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int ti = lane & 7, q = lane >> 3;
     const int S = blockIdx.x / nsplit, part = blockIdx.x % nsplit;
     if (S >= counts[W_NS] || counts[W_ERR] != 0) return;
     __shared__ float4 sxq[SUPER];
@@ -97,115 +95,96 @@ __global__ void __launch_bounds__(64) k_pairs(const float4 *__restrict__ xq, con
         fxi[a] = fyi[a] = fzi[a] = 0.f;
         if (ENERGY) ei[a] = w1i[a] = w2i[a] = w3i[a] = w4i[a] = w5i[a] = w6i[a] = 0.f;
     }
-    const int e0 = scio[S], ne = nw[S];
-    const int ea = e0 + (int)(((long long)ne * part) / nsplit);
-    const int eb = e0 + (int)(((long long)ne * (part + 1)) / nsplit);
-    // software pipeline: the entry and j-atom of the next iteration are loaded ahead
-    uint2 ent = ea < eb ? cjw[ea] : make_uint2(0u, 0u);
-    float4 pj = ea < eb ? xq[(int)ent.x * 8 + tj] : make_float4(0.f, 0.f, 0.f, 0.f);
-    int tyj = (LJK == PD_LJ_TABLE && ea < eb) ? ts[(int)ent.x * 8 + tj] : 1;
-    // One tile: the 8 i-clusters of the mask against j-cluster cj.  DIAG tiles hold the
-    // i-cluster itself (cj == S * 8 + a for one a) and mask the self and double-counted
-    // pairs; marked (pbc) tiles take the compensated periodic difference
-    // (PeriodicDisplacement.jl:4-14).  Padding atoms sit far away with zero charge and
-    // contribute exact zeros without a mask.
-    auto tile = [&](auto diag_c, bool pbc, uint32_t imask, int cj, float4 cpj, int ctyj, int js) {
-        constexpr bool DIAG = decltype(diag_c)::value;
-        float fjx = 0.f, fjy = 0.f, fjz = 0.f;
-        float ej = 0.f, vj1 = 0.f, vj2 = 0.f, vj3 = 0.f, vj4 = 0.f, vj5 = 0.f, vj6 = 0.f;
-#pragma unroll
-        for (int a = 0; a < 8; ++a) {
-            if ((imask >> a) & 1u) {
-                const float4 pi = sxq[a * 8 + ti];
-                float dx, dy, dz;
-                if (pbc) {
-                    dx = periodic_delta(pi.x, cpj.x, hx, Lx);
-                    dy = periodic_delta(pi.y, cpj.y, hy, Ly);
-                    dz = periodic_delta(pi.z, cpj.z, hz, Lz);
-                } else {
-                    dx = pi.x - cpj.x;
-                    dy = pi.y - cpj.y;
-                    dz = pi.z - cpj.z;
-                }
-                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                const float rinv = rsqrtf(r2);
-                const float rinv2 = rinv * rinv;
-                float f = 0.f, en = 0.f;
-                if (LJK != PD_LJ_NONE) {
-                    float c6, c12, lrc2, esh;
-                    if (LJK == PD_LJ_TABLE) {
-                        const float4 tb = stab[sty[a * 8 + ti] + (ctyj - 1)];
-                        c6 = tb.x;
-                        c12 = tb.y;
-                        lrc2 = tb.z;
-                        esh = tb.w;
-                    } else {
-                        c6 = pp.c6;
-                        c12 = pp.c12;
-                        lrc2 = pp.lrc2;
-                        esh = pp.esh;
-                    }
-                    const bool use = r2 < lrc2;
-                    const float ir6 = rinv2 * rinv2 * rinv2;
-                    f += use ? (12.f * c12 * ir6 - 6.f * c6) * ir6 * rinv2 : 0.f;
-                    if (ENERGY) en += use ? (c12 * ir6 - c6) * ir6 - esh : 0.f;
-                }
-                if (COUL) {
-                    // pi.w holds C q_i (premultiplied when the i-atoms were staged)
-                    const bool inr = r2 < pp.rc2;
-                    const float x = fmaf(r2, pp.sx, -1.f);
-                    const float pf = horner(cpf, x);
-                    const float rinv3 = rinv * rinv2;
-                    const float cq = pi.w * cpj.w;
-                    f = fmaf(cq, inr ? rinv3 - pf : 0.f, f);
-                    if (ENERGY) {
-                        const float pe = horner(cpe, x);
-                        en = fmaf(cq, inr ? rinv + pe - pp.eshift : 0.f, en);
-                    }
-                }
-                if (DIAG) {
-                    const bool ok = (cj != S * 8 + a) || (tj > ti);
-                    f = ok ? f : 0.f;
-                    en = ok ? en : 0.f;
-                    dx = ok ? dx : 0.f;
-                    dy = ok ? dy : 0.f;
-                    dz = ok ? dz : 0.f;
-                }
-                fxi[a] = fmaf(f, dx, fxi[a]);
-                fyi[a] = fmaf(f, dy, fyi[a]);
-                fzi[a] = fmaf(f, dz, fzi[a]);
-                fjx = fmaf(-f, dx, fjx);
-                fjy = fmaf(-f, dy, fjy);
-                fjz = fmaf(-f, dz, fjz);
-                if (ENERGY) {
-                    en *= 0.5f;
-                    const float hf = 0.5f * f;
-                    const float hfx = hf * dx, hfy = hf * dy;
-                    const float w1 = hfx * dx, w2 = hfy * dy, w3 = hf * dz * dz;
-                    const float w4 = hfx * dy, w5 = hfx * dz, w6 = hfy * dz;
-                    ei[a] += en;
-                    w1i[a] += w1;
-                    w2i[a] += w2;
-                    w3i[a] += w3;
-                    w4i[a] += w4;
-                    w5i[a] += w5;
-                    w6i[a] += w6;
-                    ej += en;
-                    vj1 += w1;
-                    vj2 += w2;
-                    vj3 += w3;
-                    vj4 += w4;
-                    vj5 += w5;
-                    vj6 += w6;
-                }
+    // One pair: i-atom pi of i-cluster a against j-atom pj; J accumulates the j-atom's
+    // force (and with ENERGY its half energy and half virial).  `masked` drops the self
+    // and double-counted pairs of the tile that holds the i-cluster itself; marked
+    // (pbc) tiles take the compensated periodic difference (PeriodicDisplacement.jl:4-14).
+    // Padding atoms sit far away with zero charge and contribute exact zeros.
+    auto pair = [&](const int a, const float4 &pi, const float4 &pj, int tyi, int tyj, bool masked, bool pbc,
+                    float (&J)[10]) {
+        float dx, dy, dz;
+        if (pbc) {
+            dx = periodic_delta(pi.x, pj.x, hx, Lx);
+            dy = periodic_delta(pi.y, pj.y, hy, Ly);
+            dz = periodic_delta(pi.z, pj.z, hz, Lz);
+        } else {
+            dx = pi.x - pj.x;
+            dy = pi.y - pj.y;
+            dz = pi.z - pj.z;
+        }
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const float rinv = rsqrtf(r2);
+        const float rinv2 = rinv * rinv;
+        float f = 0.f, en = 0.f;
+        if (LJK != PD_LJ_NONE) {
+            float c6, c12, lrc2, esh;
+            if (LJK == PD_LJ_TABLE) {
+                const float4 tb = stab[tyi + (tyj - 1)];
+                c6 = tb.x;
+                c12 = tb.y;
+                lrc2 = tb.z;
+                esh = tb.w;
+            } else {
+                c6 = pp.c6;
+                c12 = pp.c12;
+                lrc2 = pp.lrc2;
+                esh = pp.esh;
+            }
+            const bool use = r2 < lrc2;
+            const float ir6 = rinv2 * rinv2 * rinv2;
+            f += use ? (12.f * c12 * ir6 - 6.f * c6) * ir6 * rinv2 : 0.f;
+            if (ENERGY) en += use ? (c12 * ir6 - c6) * ir6 - esh : 0.f;
+        }
+        if (COUL) {
+            // pi.w holds C q_i (premultiplied when the i-atoms were staged)
+            const bool inr = r2 < pp.rc2;
+            const float x = fmaf(r2, pp.sx, -1.f);
+            const float pf = horner(cpf, x);
+            const float rinv3 = rinv * rinv2;
+            const float cq = pi.w * pj.w;
+            f = fmaf(cq, inr ? rinv3 - pf : 0.f, f);
+            if (ENERGY) {
+                const float pe = horner(cpe, x);
+                en = fmaf(cq, inr ? rinv + pe - pp.eshift : 0.f, en);
             }
         }
-        const float r = reduce3(fjx, fjy, fjz, ti);
+        f = masked ? 0.f : f;
+        fxi[a] = fmaf(f, dx, fxi[a]);
+        fyi[a] = fmaf(f, dy, fyi[a]);
+        fzi[a] = fmaf(f, dz, fzi[a]);
+        J[0] = fmaf(-f, dx, J[0]);
+        J[1] = fmaf(-f, dy, J[1]);
+        J[2] = fmaf(-f, dz, J[2]);
+        if (ENERGY) {
+            en = masked ? 0.f : 0.5f * en;
+            const float hf = 0.5f * f;
+            const float hfx = hf * dx, hfy = hf * dy;
+            const float w1 = hfx * dx, w2 = hfy * dy, w3 = hf * dz * dz;
+            const float w4 = hfx * dy, w5 = hfx * dz, w6 = hfy * dz;
+            ei[a] += en;
+            w1i[a] += w1;
+            w2i[a] += w2;
+            w3i[a] += w3;
+            w4i[a] += w4;
+            w5i[a] += w5;
+            w6i[a] += w6;
+            J[3] += en;
+            J[4] += w1;
+            J[5] += w2;
+            J[6] += w3;
+            J[7] += w4;
+            J[8] += w5;
+            J[9] += w6;
+        }
+    };
+    // j-atom results of one entry: reduced over the 8 ti lanes and added to the slot
+    auto flush = [&](const float (&J)[10], int js) {
+        const float r = reduce3(J[0], J[1], J[2], ti);
         if (ti < 3) red_add(reinterpret_cast<float *>(&fc[js]) + ti, r);
         if (ENERGY) {
-            const float rv1 = reduce3(vj1, vj2, vj3, ti);
-            const float rv2 = reduce3(vj4, vj5, vj6, ti);
-            ej = sum8(ej);
+            const float rv1 = reduce3(J[4], J[5], J[6], ti);
+            const float rv2 = reduce3(J[7], J[8], J[9], ti);
+            const float ej = sum8(J[3]);
             if (ti < 3) {
                 red_add(&vc[(size_t)ti * nslot + js], rv1);
                 red_add(&vc[(size_t)(ti + 3) * nslot + js], rv2);
@@ -213,26 +192,58 @@ __global__ void __launch_bounds__(64) k_pairs(const float4 *__restrict__ xq, con
             if (ti == 0) red_add(reinterpret_cast<float *>(&fc[js]) + 3, ej);
         }
     };
-    using T_ = std::true_type;
-    using F_ = std::false_type;
-    for (int e = ea; e < eb; ++e) {
-        const uint2 cur = ent;
-        const float4 cpj = pj;
-        const int ctyj = tyj;
-        if (e + 1 < eb) {
-            ent = cjw[e + 1];
-            pj = xq[(int)ent.x * 8 + tj];
-            if (LJK == PD_LJ_TABLE) tyj = ts[(int)ent.x * 8 + tj];
-        }
-        const uint32_t imask = (cur.y >> (8 * w)) & 0xffu;
-        if (imask == 0) continue;   // uniform per warp
-        const bool pbc = (cur.y >> 16) & 1u;   // tile may cross a box face before the next prune
-        const int cj = (int)cur.x;
-        const int js = cj * 8 + tj;
-        if ((unsigned)(cj - S * 8) < 8u) tile(T_{}, pbc, imask, cj, cpj, ctyj, js);
-        else tile(F_{}, pbc, imask, cj, cpj, ctyj, js);
+    const int e0 = scio[S], ne = nw[S];
+    const int ea = e0 + (int)(((long long)ne * part) / nsplit);
+    const int eb = e0 + (int)(((long long)ne * (part + 1)) / nsplit);
+    // The two warps take alternate entries.  Lane (ti, q) pairs i-atom ti of every
+    // i-cluster in the mask with j-atoms q (j half 0) and q + 4 (j half 1); the next
+    // entry's word and j-atoms are loaded while the current one is evaluated.
+    const bool gtA = q > ti, gtB = q + 4 > ti;
+    int e = ea + w;
+    uint2 ent = e < eb ? cjw[e] : make_uint2(0u, 0u);
+    float4 pa = e < eb ? xq[(int)ent.x * 8 + q] : make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 pb = e < eb ? xq[(int)ent.x * 8 + q + 4] : make_float4(0.f, 0.f, 0.f, 0.f);
+    int ta = 1, tb = 1;
+    if (LJK == PD_LJ_TABLE && e < eb) {
+        ta = ts[(int)ent.x * 8 + q];
+        tb = ts[(int)ent.x * 8 + q + 4];
     }
-    const int lane = tid & 31;
+    for (; e < eb; e += 2) {
+        const uint2 cur = ent;
+        const float4 ja = pa, jb = pb;
+        const int cta = ta, ctb = tb;
+        if (e + 2 < eb) {
+            ent = cjw[e + 2];
+            pa = xq[(int)ent.x * 8 + q];
+            pb = xq[(int)ent.x * 8 + q + 4];
+            if (LJK == PD_LJ_TABLE) {
+                ta = ts[(int)ent.x * 8 + q];
+                tb = ts[(int)ent.x * 8 + q + 4];
+            }
+        }
+        // the entry is the same for every lane; the warp reduction makes that visible to the
+        // compiler, so the branches on its bits below are uniform
+        const uint32_t word = __reduce_or_sync(0xffffffffu, cur.y);
+        const uint32_t lo = word & 0xffu, hi = (word >> 8) & 0xffu;
+        const bool pbc = (word >> 16) & 1u;   // tile may cross a box face before the next prune
+        const int cj = (int)__reduce_or_sync(0xffffffffu, cur.x);
+        const int da = cj - S * 8;   // index of the i-cluster that is the j-cluster itself, if in [0, 8)
+        float A[10], B[10];
+#pragma unroll
+        for (int k = 0; k < 10; ++k) A[k] = B[k] = 0.f;
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            if (((lo | hi) >> a) & 1u) {
+                const float4 pi = sxq[a * 8 + ti];
+                const int tyi = LJK == PD_LJ_TABLE ? sty[a * 8 + ti] : 0;
+                const bool self = da == a;
+                if ((lo >> a) & 1u) pair(a, pi, ja, tyi, cta, self && !gtA, pbc, A);
+                if ((hi >> a) & 1u) pair(a, pi, jb, tyi, ctb, self && !gtB, pbc, B);
+            }
+        }
+        flush(A, cj * 8 + q);
+        flush(B, cj * 8 + q + 4);
+    }
 #pragma unroll
     for (int a = 0; a < 8; ++a) {
         fxi[a] = reduce_i(fxi[a]);

@@ -11,6 +11,7 @@ namespace pdb {
 
 constexpr int CLUSTER = 8;   // particles per cluster (List.jl:29)
 constexpr int SUPER = 64;    // particles per super-cluster (List.jl:30)
+constexpr int SEARCH_MAX_COLS = 1024;   // neighbouring columns one super-cluster may search
 
 // Device count words of one cluster list (indices into pd_cluster::counts).
 enum CountWord {
@@ -27,6 +28,7 @@ enum CountWord {
     W_FLAG_ANY = 10, // max displacement ratio (build or prune) as float bits
     W_FLAG_BUILD = 11, // max displacement ratio since the build as float bits
     W_NWORK = 12,    // working entries (sum over super-clusters, diagnostics)
+    W_TICKET = 13,   // blocks of the step's kick kernel that have reported (last one decides)
     W_LEN = 16
 };
 
@@ -50,14 +52,14 @@ __device__ __forceinline__ float force_coordinate(float x, float L) {
 // periodic_delta (PeriodicDisplacement.jl:4-14): error-free TwoDiff followed by
 // the exact subtraction of L.  Compiled without fast-math; the operations below
 // must not be reassociated.
+// Branch-free: both results are formed and one is selected, so lanes of a warp
+// never diverge on it.
 __device__ __forceinline__ float periodic_delta(float xi, float xj, float halfL, float L) {
-    float d = __fsub_rn(xi, xj);
-    if (fabsf(d) > halfL) {
-        float bv = __fsub_rn(xi, d);
-        float res = __fadd_rn(__fsub_rn(xi, __fadd_rn(d, bv)), __fsub_rn(bv, xj));
-        return __fadd_rn(__fsub_rn(d, copysignf(L, d)), res);
-    }
-    return d;
+    const float d = __fsub_rn(xi, xj);
+    const float bv = __fsub_rn(xi, d);
+    const float res = __fadd_rn(__fsub_rn(xi, __fadd_rn(d, bv)), __fsub_rn(bv, xj));
+    const float w = __fadd_rn(__fsub_rn(d, copysignf(L, d)), res);
+    return fabsf(d) > halfL ? w : d;
 }
 
 // _mic (List.jl:192-197)
@@ -102,6 +104,11 @@ __device__ __forceinline__ void red_add(float *p, float v) {
 __device__ __forceinline__ void red_add_v4(float *p, float a, float b, float c, float d) {
     asm volatile("red.relaxed.gpu.global.add.v4.f32 [%0], {%1,%2,%3,%4};" ::"l"(p), "f"(a), "f"(b), "f"(c), "f"(d)
                  : "memory");
+}
+// Shared-memory float add without a returned value (no register waits on the result).
+__device__ __forceinline__ void red_add_shared(float *p, float v) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    asm volatile("red.shared.add.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
 }
 __device__ __forceinline__ void red_add_d(double *p, double v) {
     asm volatile("red.relaxed.gpu.global.add.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");

@@ -106,6 +106,7 @@ struct pd_cluster {
     float4 *cbc = nullptr, *cbh = nullptr;   // 8 nsmax cluster boxes (centre, half width)
     float4 *sbc = nullptr, *sbh = nullptr;   // nsmax super-cluster boxes
     int *cnt_sc = nullptr;     // nsmax
+    int *colcnt = nullptr;     // nsmax * ncs: outer entries per (super-cluster, search column)
     int *scio = nullptr;       // nsmax + 1
     uint32_t *cjo = nullptr;   // necap
     uint2 *cjw = nullptr;      // necap

@@ -41,9 +41,41 @@ struct pd_md {
 
 namespace pdb {
 
+// Device build/prune decision (_decide_kernel!, Engine.jl:301-324), taken by the
+// last block of k_kick_drift once every block's displacement maxima are in.  In a
+// captured step it also sets the graph's IF condition for the build body, so the
+// build kernels are not launched at all on steps that keep the list (the
+// reference's conditional graph nodes, DeviceConditionalGraph.jl:88-132); the
+// prune kernel reads the prune flag and returns at once when it is clear.
+template <bool COND>
+__device__ void decide_step(int *counts, int nstlist, int nstprune, cudaGraphConditionalHandle hb) {
+    const float anyr = __int_as_float(atomicAdd(&counts[W_FLAG_ANY], 0));
+    const float br = __int_as_float(atomicAdd(&counts[W_FLAG_BUILD], 0));
+    bool build, prune;
+    if (nstlist > 0) {
+        const int k = counts[W_DSTEP];
+        counts[W_DSTEP] = k + 1;
+        build = (k % nstlist == 0) || (counts[W_REQUEST] != 0) || !isfinite(br);
+        prune = build || (nstprune > 0 && k % nstprune == 0);
+    } else {
+        build = (br > 1.0f) || (counts[W_REQUEST] != 0);
+        prune = build || (anyr > 1.0f);
+    }
+    counts[W_BUILD] = build ? 1 : 0;
+    counts[W_PRUNE] = prune ? 1 : 0;
+    counts[W_REQUEST] = 0;
+    counts[W_NBUILD] += build ? 1 : 0;
+    counts[W_NPRUNE] += prune ? 1 : 0;
+    counts[W_FLAG_ANY] = 0;
+    counts[W_FLAG_BUILD] = 0;
+    if (COND) cudaGraphSetConditional(hb, build ? 1u : 0u);
+}
+
 // _nve_kick_drift3_kernel! (NVEFusion.jl:3-27) fused with the pack of the force
-// coordinates (_pack_kernel!, List.jl:377-413) and the displacement maxima of
-// _displacement_kernel! (List.jl:787-819).
+// coordinates (_pack_kernel!, List.jl:377-413), the displacement maxima of
+// _displacement_kernel! (List.jl:787-819) and, in the last block to finish, the
+// list decision.
+template <bool COND>
 __global__ void __launch_bounds__(256) k_kick_drift(int n, float *__restrict__ x, float *__restrict__ y,
                                                     float *__restrict__ z, float *__restrict__ vx,
                                                     float *__restrict__ vy, float *__restrict__ vz,
@@ -53,7 +85,8 @@ __global__ void __launch_bounds__(256) k_kick_drift(int n, float *__restrict__ x
                                                     const float *__restrict__ q, const int *__restrict__ slot_of,
                                                     float4 *__restrict__ xq, const float4 *__restrict__ rb,
                                                     const float4 *__restrict__ rp, float tb2, float tp2,
-                                                    int *__restrict__ counts) {
+                                                    int *__restrict__ counts, int nstlist, int nstprune,
+                                                    cudaGraphConditionalHandle hb) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     float ra = 0.f, rbv = 0.f;
     if (i < n) {
@@ -104,39 +137,14 @@ __global__ void __launch_bounds__(256) k_kick_drift(int n, float *__restrict__ x
         if (lane == 0) {
             atomicMax(&counts[W_FLAG_ANY], __float_as_int(a));
             atomicMax(&counts[W_FLAG_BUILD], __float_as_int(c));
+            __threadfence();
+            // the last block to arrive takes the decision (threadfence-reduction pattern)
+            if (atomicAdd(&counts[W_TICKET], 1) == (int)gridDim.x - 1) {
+                __threadfence();
+                counts[W_TICKET] = 0;
+                decide_step<COND>(counts, nstlist, nstprune, hb);
+            }
         }
-    }
-}
-
-// Device build/prune decision (_decide_kernel!, Engine.jl:301-324).  In a captured
-// step it also sets the graph's two IF conditions, so the build and prune bodies
-// are not launched at all on steps that do not need them (the reference's
-// conditional graph nodes, DeviceConditionalGraph.jl:88-132).
-template <bool COND>
-__global__ void k_decide_step(int *__restrict__ counts, int nstlist, int nstprune, cudaGraphConditionalHandle hb,
-                              cudaGraphConditionalHandle hp) {
-    float anyr = __int_as_float(counts[W_FLAG_ANY]);
-    float br = __int_as_float(counts[W_FLAG_BUILD]);
-    bool build, prune;
-    if (nstlist > 0) {
-        int k = counts[W_DSTEP];
-        counts[W_DSTEP] = k + 1;
-        build = (k % nstlist == 0) || (counts[W_REQUEST] != 0) || !isfinite(br);
-        prune = build || (nstprune > 0 && k % nstprune == 0);
-    } else {
-        build = (br > 1.0f) || (counts[W_REQUEST] != 0);
-        prune = build || (anyr > 1.0f);
-    }
-    counts[W_BUILD] = build ? 1 : 0;
-    counts[W_PRUNE] = prune ? 1 : 0;
-    counts[W_REQUEST] = 0;
-    counts[W_NBUILD] += build ? 1 : 0;
-    counts[W_NPRUNE] += prune ? 1 : 0;
-    counts[W_FLAG_ANY] = 0;
-    counts[W_FLAG_BUILD] = 0;
-    if (COND) {
-        cudaGraphSetConditional(hb, build ? 1u : 0u);
-        cudaGraphSetConditional(hp, prune ? 1u : 0u);
     }
 }
 
@@ -272,35 +280,34 @@ static int enqueue_step(pd_md *md, float dt, int energy, cudaStream_t s, int con
     pd_md_state &st = md->st;
     const float hb = (float)(0.5 * c->p.skin), hp = (float)(0.5 * c->p.prune_buffer);
     const float *q = c->p.coulomb ? st.q : nullptr;
-    k_kick_drift<<<(st.n + 255) / 256, 256, 0, s>>>(st.n, st.x, st.y, st.z, st.vx, st.vy, st.vz, st.fx, st.fy, st.fz,
-                                                    st.inv_mass, st.inv_mass_uniform, dt, md->L[0], md->L[1], md->L[2],
-                                                    q, c->slot_of, c->xq, c->ref_build, c->ref_prune, hb * hb,
-                                                    hp * hp, c->counts);
-    PD_LAUNCHED();
     int rc;
+    const int kb = (st.n + 255) / 256;
     if (cond) {
         cudaStreamCaptureStatus status;
         cudaGraph_t g = nullptr;
         PD_CUDA(cudaStreamGetCaptureInfo(s, &status, nullptr, &g, nullptr, nullptr));
-        cudaGraphConditionalHandle hbuild, hprune;
+        cudaGraphConditionalHandle hbuild;
         PD_CUDA(cudaGraphConditionalHandleCreate(&hbuild, g, 0, cudaGraphCondAssignDefault));
-        PD_CUDA(cudaGraphConditionalHandleCreate(&hprune, g, 0, cudaGraphCondAssignDefault));
-        k_decide_step<true><<<1, 1, 0, s>>>(c->counts, c->p.nstlist, c->p.nstprune, hbuild, hprune);
+        k_kick_drift<true><<<kb, 256, 0, s>>>(st.n, st.x, st.y, st.z, st.vx, st.vy, st.vz, st.fx, st.fy, st.fz,
+                                              st.inv_mass, st.inv_mass_uniform, dt, md->L[0], md->L[1], md->L[2], q,
+                                              c->slot_of, c->xq, c->ref_build, c->ref_prune, hb * hb, hp * hp,
+                                              c->counts, c->p.nstlist, c->p.nstprune, hbuild);
         PD_LAUNCHED();
         if ((rc = capture_if(s, md->body, hbuild, [&](cudaStream_t cs) {
                  return cluster_build_launch(c, st.x, st.y, st.z, q, st.type, 1, cs);
              })))
             return rc;
-        if ((rc = fork_mesh(md, energy, s))) return rc;
-        if ((rc = capture_if(s, md->body, hprune, [&](cudaStream_t cs) { return cluster_prune_launch(c, 1, cs); })))
-            return rc;
     } else {
-        k_decide_step<false><<<1, 1, 0, s>>>(c->counts, c->p.nstlist, c->p.nstprune, 0, 0);
+        k_kick_drift<false><<<kb, 256, 0, s>>>(st.n, st.x, st.y, st.z, st.vx, st.vy, st.vz, st.fx, st.fy, st.fz,
+                                               st.inv_mass, st.inv_mass_uniform, dt, md->L[0], md->L[1], md->L[2], q,
+                                               c->slot_of, c->xq, c->ref_build, c->ref_prune, hb * hb, hp * hp,
+                                               c->counts, c->p.nstlist, c->p.nstprune, 0);
         PD_LAUNCHED();
         if ((rc = cluster_build_launch(c, st.x, st.y, st.z, q, st.type, 1, s))) return rc;
-        if ((rc = fork_mesh(md, energy, s))) return rc;
-        if ((rc = cluster_prune_launch(c, 1, s))) return rc;
     }
+    // the mesh transform forks before the prune, which runs as a flag-gated kernel
+    if ((rc = fork_mesh(md, energy, s))) return rc;
+    if ((rc = cluster_prune_launch(c, 1, s))) return rc;
     return enqueue_forces(md, energy, 0.5f * dt, s);
 }
 
@@ -322,7 +329,11 @@ int pd_md_create(pd_md **out, pd_cluster *c, pd_mesh *m, const pd_md_state *st, 
     md->st = *st;
     for (int d = 0; d < 3; ++d) md->L[d] = (float)box[d];
     md->half_c_self = c->p.coulomb ? 0.5f * c->p.coul_C * c->p.selfc : 0.f;
-    if (cudaStreamCreateWithFlags(&md->side, cudaStreamNonBlocking) != cudaSuccess ||
+    // the mesh chain (spread, transforms, solve) is latency-bound and on the step's
+    // critical path: its stream takes the highest priority, the pair pass fills in
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    if (cudaStreamCreateWithPriority(&md->side, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
         cudaStreamCreateWithFlags(&md->body, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&md->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&md->ev_join, cudaEventDisableTiming) != cudaSuccess ||

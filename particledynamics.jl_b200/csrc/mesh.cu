@@ -43,7 +43,8 @@ namespace pdb {
 
 constexpr int MESH_CHUNK = 64;        // particles per CTA
 constexpr int MESH_THREADS = 128;     // two threads per particle (halves of the z stencil)
-constexpr int TILE_MAX = 7168;        // floats of the shared brick (28 KiB)
+constexpr int TILE_MAX = 6144;        // floats of the shared brick (24 KiB)
+constexpr int MESH_CTAS_PER_SM = 8;   // resident spread / gather CTAs per SM (one wave at ~1200 chunks)
 
 // _grid_coordinate (MeshKernels.jl:9-15)
 __device__ __forceinline__ float grid_coordinate(float x, float L, int K) {
@@ -126,7 +127,7 @@ struct Brick {
     int vec;
 };
 
-constexpr int ROWS_MAX = TILE_MAX / 4;   // brick rows (the x extent is at least 4 when it fits)
+constexpr int ROWS_MAX = 512;   // brick rows tabulated in shared memory
 
 template <int P>
 __device__ __forceinline__ void chunk_brick(bool valid, int k1, int k2, int k3, int K1, int K2, int K3, int &d1,
@@ -221,7 +222,7 @@ __device__ __forceinline__ void for_brick(const Brick &b, const unsigned *rowbas
 // _spread_lines_kernel!, MeshKernels.jl:247-276).  nchunk_dev (optional) holds
 // the number of active chunks (the cluster list's super-cluster count).
 template <int P>
-__global__ void __launch_bounds__(MESH_THREADS) k_spread(const float4 *__restrict__ xq, int nchunks,
+__global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_spread(const float4 *__restrict__ xq, int nchunks,
                                                          const int *__restrict__ nchunk_dev, float *__restrict__ grid,
                                                          int K1, int K2, int K3, float Lx, float Ly, float Lz) {
     const int c = blockIdx.x;
@@ -252,7 +253,8 @@ __global__ void __launch_bounds__(MESH_THREADS) k_spread(const float4 *__restric
         for (int k = t; k < nb4; k += MESH_THREADS) tile4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
         __syncthreads();
         if (valid) {
-            for (int j3 = 0; j3 < P; ++j3) {   // unrolled; this half's z nodes only (warp-uniform test)
+#pragma unroll
+            for (int j3 = 0; j3 < P; ++j3) {   // this half's z nodes only (warp-uniform test)
             if ((j3 < PH) != (h == 0)) continue;
                 const float q3 = v.w * w3[j3];
 #pragma unroll
@@ -260,7 +262,7 @@ __global__ void __launch_bounds__(MESH_THREADS) k_spread(const float4 *__restric
                     const float q23 = q3 * w2[j2];
                     float *row = tile + ((d3 + j3) * b.e2 + (d2 + j2)) * b.e1 + d1;
 #pragma unroll
-                    for (int j1 = 0; j1 < P; ++j1) atomicAdd(row + j1, q23 * w1[j1]);
+                    for (int j1 = 0; j1 < P; ++j1) red_add_shared(row + j1, q23 * w1[j1]);
                 }
             }
         }
@@ -278,7 +280,8 @@ __global__ void __launch_bounds__(MESH_THREADS) k_spread(const float4 *__restric
             });
         }
     } else if (valid) {
-        for (int j3 = 0; j3 < P; ++j3) {   // unrolled; this half's z nodes only (warp-uniform test)
+#pragma unroll
+        for (int j3 = 0; j3 < P; ++j3) {   // this half's z nodes only (warp-uniform test)
             if ((j3 < PH) != (h == 0)) continue;
             const int n3 = wrap_node(k3 + j3, K3);
             const float q3 = v.w * w3[j3];
@@ -381,7 +384,7 @@ struct GatherOut {
 };
 
 template <int P, int MODE, bool ENERGY>   // MODE 0: add, 1: set, 2: join (+ kick)
-__global__ void __launch_bounds__(MESH_THREADS) k_gather(const float4 *__restrict__ xq, int nchunks,
+__global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_gather(const float4 *__restrict__ xq, int nchunks,
                                                          const int *__restrict__ nchunk_dev,
                                                          const float *__restrict__ grid, int K1, int K2, int K3,
                                                          float Lx, float Ly, float Lz, GatherOut o) {
@@ -432,7 +435,8 @@ __global__ void __launch_bounds__(MESH_THREADS) k_gather(const float4 *__restric
         }
         __syncthreads();
         if (charged) {
-            for (int j3 = 0; j3 < P; ++j3) {   // unrolled; this half's z nodes only (warp-uniform test)
+#pragma unroll
+            for (int j3 = 0; j3 < P; ++j3) {   // this half's z nodes only (warp-uniform test)
             if ((j3 < PH) != (h == 0)) continue;
                 float s0 = 0.f, s1 = 0.f, s2 = 0.f;   // sum w1 w2 c, sum dw1 w2 c, sum w1 dw2 c over a z-plane
 #pragma unroll
@@ -456,7 +460,8 @@ __global__ void __launch_bounds__(MESH_THREADS) k_gather(const float4 *__restric
             }
         }
     } else if (charged) {
-        for (int j3 = 0; j3 < P; ++j3) {   // unrolled; this half's z nodes only (warp-uniform test)
+#pragma unroll
+        for (int j3 = 0; j3 < P; ++j3) {   // this half's z nodes only (warp-uniform test)
             if ((j3 < PH) != (h == 0)) continue;
             const int n3 = wrap_node(k3 + j3, K3);
             float s0 = 0.f, s1 = 0.f, s2 = 0.f;

@@ -114,6 +114,8 @@ extern "C" int pd_cluster_compute_static(const pd_cluster_params *p, const doubl
     c.mx = (int)std::floor(rlist / (0.98 * Lx / c.ncx)) + 1;
     c.my = (int)std::floor(rlist / (0.98 * Ly / c.ncy)) + 1;
     c.ncs = std::min(2 * c.mx + 1, c.ncx) * std::min(2 * c.my + 1, c.ncy);
+    PD_CHECK(c.ncs <= SEARCH_MAX_COLS, PD_EINVAL, "pd_cluster_compute_static: %d search columns exceed %d", c.ncs,
+             SEARCH_MAX_COLS);
     for (int d = 0; d < 3; ++d) {
         c.box[d] = box[d];
         c.L[d] = (float)box[d];
@@ -171,6 +173,7 @@ extern "C" int pd_cluster_compute_static(const pd_cluster_params *p, const doubl
     c.sbc = cv.take<float4>(c.nsmax);
     c.sbh = cv.take<float4>(c.nsmax);
     c.cnt_sc = cv.take<int>(c.nsmax);
+    c.colcnt = cv.take<int>((size_t)c.nsmax * c.ncs);
     c.scio = cv.take<int>(c.nsmax + 1);
     c.nw = cv.take<int>(c.nsmax);
     c.fc = cv.take<float4>(c.nslot);
