@@ -275,6 +275,77 @@ int pd_md_step(pd_md *md, int nsteps, float dt, int energy_last, int use_graph, 
 int pd_md_step_host(pd_md *md, float *host_xyz, float *host_v, int nsteps, float dt,
                     double *epot_sum, pd_stream_t s);
 
+/* ======================================================================
+ * ELL route: cell list + fixed-capacity neighbour rows (the reference's default `CellList`
+ * route for LJ / WCA, src/neighbors/DeviceNeighborCUDA.jl, src/neighbors/DenseNeighborCUDA.jl)
+ * and the row pair kernels (src/engine/PairTraversal.jl:66-125, src/engine/PairModels.jl:13-49,
+ * src/nonbonded/LJELLEngineKernels.jl).  2D and 3D; rows are slot-major (slot t of particle i
+ * at t * n + i, _ell_index, src/neighbors/NeighborTypes.jl:31), 0-based ids.
+ * ====================================================================== */
+typedef struct pd_ell pd_ell;
+
+enum { PD_PAIR_LJ = 1, PD_PAIR_WCA = 2 };
+
+typedef struct {
+    int dim;            /* 2 or 3 */
+    int n;
+    double cutoff;      /* interaction cutoff; the list radius is cutoff + skin */
+    double skin;        /* CellList buffer (src/workflow/Forces.jl:33-42) */
+    int cap;            /* row capacity (CellList capacity) */
+    int interval;       /* initial rebuild interval 1..100 (CellList rebuild_interval) */
+    int model;          /* PD_PAIR_LJ or PD_PAIR_WCA (UniformLJ / UniformWCA) */
+    float eps, sigma;
+    float rc2;          /* pair cutoff squared (WCA: 1.2599211 sigma^2, PairModels.jl:25) */
+    float eshift;       /* LJ potential-shift modifier u(r_c), or 0 */
+    int lanes;          /* lanes per row in the pair kernel: 1, 2, 4, 8, or 0 to choose from the density */
+} pd_ell_params;
+
+typedef struct {
+    int valid, error, requested;   /* error: 0, 1 capacity (rows longer than cap), 2 coordinates */
+    long long step, last_build, interval, checks, builds;
+    long long required;            /* longest row of the last build attempt */
+    int cap, lanes, allpairs;      /* allpairs: box below three cells per dimension, rows from all pairs */
+} pd_ell_stats;
+
+/* DeviceNeighborWorkspace(T, N, box; cutoff, skin, cap, interval) (DeviceNeighborCUDA.jl:64-88) */
+int pd_ell_create(pd_ell **out, const pd_ell_params *p, const double box[3]);
+int pd_ell_destroy(pd_ell *e);
+/* update_device_neighbors! (DeviceNeighborCUDA.jl:420-427): displacement check and decision, then
+ * the rebuild kernels, which return at once unless the device decided to rebuild.  Coordinates
+ * must be centred (|x| <= L/2). */
+int pd_ell_update(pd_ell *e, const float *x, const float *y, const float *z, pd_stream_t s);
+/* request_device_rebuild!: invalidate the list so that the next update rebuilds it. */
+int pd_ell_request(pd_ell *e, pd_stream_t s);
+/* The row pair kernel: f (stored), with energy = 1 the per-particle energy (half of each pair) and
+ * the per-particle half virial (3D: n x 6 xx yy zz xy xz yz; 2D: n x 3 xx yy xy).  z / fz may be
+ * NULL in 2D.  No forces are written while the list is invalid. */
+int pd_ell_forces(pd_ell *e, const float *x, const float *y, const float *z, float *fx, float *fy, float *fz,
+                  float *epot, float *vir, int energy, pd_stream_t s);
+/* device_neighbor_status (DeviceNeighborCUDA.jl:624-637): boundary readback. */
+int pd_ell_status(pd_ell *e, pd_ell_stats *out);
+/* Device pointers of the rows (cap * n ints) and the row lengths (n ints). */
+int pd_ell_rows(pd_ell *e, int **rows, int **counts);
+/* resize_capacity! + rearm_capacity_rebuild! (DeviceNeighborCUDA.jl:606-620): new row storage of
+ * capacity cap, a latched capacity error cleared and a rebuild requested.  Captured graphs that
+ * hold the old storage must be re-captured (the step engine does so when its key changes). */
+int pd_ell_resize(pd_ell *e, int cap);
+
+/* Step engine on the ELL route (src/engine/Run.jl:162-294, src/engine/Langevin.jl): drift with the
+ * list decision fused, the flag-gated rebuild (a conditional graph node when captured), the pair
+ * kernel with the closing half kick.  The state's z, vz, fz may be NULL in 2D; q, type and
+ * vglobal6 are not used; vir6 holds n x 6 (3D) or n x 3 (2D) values. */
+typedef struct pd_ell_md pd_ell_md;
+int pd_ell_md_create(pd_ell_md **out, pd_ell *e, const pd_md_state *st);
+int pd_ell_md_destroy(pd_ell_md *md);
+/* evaluate_forces_into_f! on this route: decision + rebuild at the current positions, forces. */
+int pd_ell_md_evaluate(pd_ell_md *md, int energy, pd_stream_t s);
+/* nsteps velocity-Verlet NVE steps of size dt. */
+int pd_ell_md_step(pd_ell_md *md, int nsteps, float dt, int energy_last, int use_graph, pd_stream_t s);
+/* nsteps Langevin BAOAB steps (_baoa_kernel!, Langevin.jl:58-88): friction gamma, temperature kT,
+ * noise from Philox4x32-10 keyed on (particle id, device step) and seed (src/engine/Philox.jl). */
+int pd_ell_md_langevin(pd_ell_md *md, int nsteps, float dt, float gamma, float kT, unsigned long long seed,
+                       int energy_last, int use_graph, pd_stream_t s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,6 +59,9 @@ def _load():
         L.ora_cluster_prune.argtypes = [C.c_int, _f, _i, _u, _d, C.c_double, C.c_double, _u, _i]
         L.ora_force_coordinate.argtypes = [C.c_float, C.c_float]
         L.ora_force_coordinate.restype = C.c_float
+        L.ora_philox_normals4.argtypes = [C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32, _f, _u]
+        L.ora_baoab_drift.argtypes = [C.c_int, C.c_int, _f, _f, _f, _f, _f, _f, _f, _f, _f, _f, C.c_float,
+                                      C.c_float, C.c_float, C.c_uint64, C.c_uint64, _d]
         _lib = L
     return _lib
 
@@ -383,3 +386,37 @@ class CpuMelt:
         self.pos -= L * np.floor(self.pos / L + 0.5)
         self.F = self.forces()
         self.vel += 0.5 * dt * self.im[:, None] * self.F
+
+
+# ------------------------------------------------------------------ Langevin
+
+def philox_normals4(seed: int, step: int, pid: int, stream: int = 0):
+    """Four Float32 normals and the four Philox4x32-10 words for (pid, stream, step) under seed
+    (src/engine/Philox.jl:20-67)."""
+    L = _load()
+    out = np.zeros(4, np.float32)
+    words = np.zeros(4, np.uint32)
+    L.ora_philox_normals4(int(seed) & 0xFFFFFFFFFFFFFFFF, int(step), int(pid), int(stream), _p(out, _f),
+                          _p(words, _u))
+    return out, words
+
+
+def baoab_drift(pos, vel, force, inv_mass, box, *, dt, gamma, kT, seed, step):
+    """One BAOAB drift (B1 A1 O A2) of Float32 state arrays (N x D) with FP64 intermediates
+    (_baoa_kernel!, src/engine/Langevin.jl:58-88); returns new (pos, vel)."""
+    L = _load()
+    pos = np.asarray(pos, np.float32)
+    n, dim = pos.shape
+    comp = lambda a, d: np.ascontiguousarray(np.asarray(a, np.float32)[:, d])  # noqa: E731
+    p = [comp(pos, d) for d in range(dim)]
+    v = [comp(vel, d) for d in range(dim)]
+    f = [comp(force, d) for d in range(dim)]
+    if dim == 2:
+        p.append(np.zeros(n, np.float32)); v.append(np.zeros(n, np.float32)); f.append(np.zeros(n, np.float32))
+    im = np.ascontiguousarray(np.broadcast_to(np.asarray(inv_mass, np.float32), (n,)))
+    noise = np.float32(np.sqrt(2.0 * float(gamma) * float(kT) * float(np.float32(dt))))
+    b = np.array(list(box) + [1.0] * (3 - len(box)), np.float64)
+    L.ora_baoab_drift(n, dim, *[_p(a, _f) for a in p], *[_p(a, _f) for a in v], *[_p(a, _f) for a in f],
+                      _p(im, _f), float(dt), float(gamma), float(noise), int(seed) & 0xFFFFFFFFFFFFFFFF, int(step),
+                      _p(b))
+    return np.stack(p[:dim], 1), np.stack(v[:dim], 1)

@@ -987,3 +987,74 @@ void ora_cluster_prune(int NS, const float *xq, const int *scio, const uint32_t 
         nw[S] = keep;
     }
 }
+
+/* ------------------------------------------------------------------------
+ * Langevin noise and BAOAB drift.
+ *   Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): counter (id, stream, step low, step
+ *   high), key (seed low, seed high), ten rounds with the published multipliers and Weyl key
+ *   increments; four standard normals by Box-Muller of open-interval uniforms from the top 24
+ *   bits (src/engine/Philox.jl:20-67).
+ *   BAOAB drift B1 A1 O A2 with FP64 intermediates (_baoa_kernel!, src/engine/Langevin.jl:58-88):
+ *   v1 = v + dt/(2m) f, x1 = x + dt/2 v1, c = exp(-g dt/m), r = sqrt((1-c^2)/(2 g dt m)) with the
+ *   per-mass form, beta = noise * xi (Float32), v2 = c v1 + r beta, x2 = x1 + dt/2 v2, positions
+ *   wrapped once into [-L/2, L/2).
+ * ---------------------------------------------------------------------- */
+static void ora_philox(uint32_t c[4], uint32_t k0, uint32_t k1) {
+    for (int r = 0; r < 10; ++r) {
+        if (r > 0) {
+            k0 += 0x9E3779B9u;
+            k1 += 0xBB67AE85u;
+        }
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c[0], p1 = (uint64_t)0xCD9E8D57u * c[2];
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0, n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+        c[1] = (uint32_t)p1;
+        c[3] = (uint32_t)p0;
+        c[0] = n0;
+        c[2] = n2;
+    }
+}
+
+static float ora_open01(uint32_t u) { return ((float)(u >> 8) + 0.5f) * 5.9604644775390625e-8f; }
+
+void ora_philox_normals4(uint64_t seed, uint64_t step, uint32_t id, uint32_t stream, float *out, uint32_t *words) {
+    uint32_t c[4] = {id, stream, (uint32_t)step, (uint32_t)(step >> 32)};
+    ora_philox(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    if (words)
+        for (int k = 0; k < 4; ++k) words[k] = c[k];
+    for (int h = 0; h < 2; ++h) {
+        const float u1 = ora_open01(c[2 * h]), u2 = ora_open01(c[2 * h + 1]);
+        const float r = sqrtf(-2.0f * logf(u1));
+        const double a = M_PI * (double)(2.0f * u2);
+        out[2 * h] = r * (float)cos(a);
+        out[2 * h + 1] = r * (float)sin(a);
+    }
+}
+
+static float ora_wrap_half(float x, float L) {
+    if (x >= 0.5f * L) x -= L;
+    if (x < -0.5f * L) x += L;
+    return x;
+}
+
+void ora_baoab_drift(int n, int dim, float *x, float *y, float *z, float *vx, float *vy, float *vz, const float *fx,
+                     const float *fy, const float *fz, const float *inv_mass, float dt, float gamma, float noise,
+                     uint64_t seed, uint64_t step, const double box[3]) {
+    for (int i = 0; i < n; ++i) {
+        float *p[3] = {x + i, y + i, dim == 3 ? z + i : NULL};
+        float *v[3] = {vx + i, vy + i, dim == 3 ? vz + i : NULL};
+        const float f[3] = {fx[i], fy[i], dim == 3 ? fz[i] : 0.0f};
+        const double dtA = dt, imA = inv_mass[i], g = gamma;
+        const double hk = dtA * imA / 2.0;
+        const double c = exp(-g * dtA * imA), rr = sqrt((1.0 - c * c) * imA / (2.0 * g * dtA));
+        float xi[4];
+        ora_philox_normals4(seed, step, (uint32_t)(i + 1), 0u, xi, NULL);
+        for (int d = 0; d < dim; ++d) {
+            const double v1 = (double)*v[d] + hk * (double)f[d];
+            const double x1 = (double)*p[d] + 0.5 * dtA * v1;
+            const double beta = (double)(noise * xi[d]);
+            const double v2 = c * v1 + rr * beta;
+            *v[d] = (float)v2;
+            *p[d] = ora_wrap_half((float)(x1 + 0.5 * dtA * v2), (float)box[d]);
+        }
+    }
+}

@@ -6,10 +6,12 @@ math, the engine objects and the workflow API.  Importing the package does
 not require a GPU; creating an engine does, and there is no CPU fallback.
 """
 from . import _native, splits, synthetic  # noqa: F401
-from .engine import ClusterPairEngine, DeviceEngine, ElectrostaticsSolver, ElectrostaticsSpec  # noqa: F401
+from .engine import (ClusterPairEngine, DeviceEngine, ELLDeviceEngine, ELLEngine, ElectrostaticsSolver,  # noqa: F401
+                     ElectrostaticsSpec)
 from .workflow import (  # noqa: F401
-    PME, PPPM, WCA, CellList, ClusterPairList, ConstantVolume, Integrator, LennardJones, ParticleSystem, Simulation,
-    SimulationState, Stage, electrostatics_spec, evaluate_forces_into_f, run, state, step,
+    BAOAB, PME, PPPM, WCA, CellList, ClusterPairList, ConstantVolume, Integrator, Langevin, LennardJones,
+    ParticleSystem, Simulation, SimulationState, Stage, VelocityVerlet, electrostatics_spec, evaluate_forces_into_f,
+    run, state, step,
 )
 
 __version__ = "0.1.0"

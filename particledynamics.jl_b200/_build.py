@@ -17,7 +17,7 @@ CSRC = HERE / "csrc"
 LIB = HERE / "libpdb200.so"
 ROOT = HERE.parent
 
-SOURCES = ["cluster_list.cu", "cluster_pairs.cu", "mesh.cu", "md.cu", "noalloc.cu"]
+SOURCES = ["cluster_list.cu", "cluster_pairs.cu", "mesh.cu", "md.cu", "noalloc.cu", "ell.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

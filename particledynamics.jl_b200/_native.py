@@ -16,6 +16,7 @@ PD_LJ_NONE, PD_LJ_UNIFORM, PD_LJ_TABLE = 0, 1, 2
 PD_MESH_SPME, PD_MESH_P3M_AD, PD_MESH_P3M_IK = 1, 2, 3
 PD_MAX_POLY = 32
 PD_MAX_TYPES = 16
+PD_PAIR_LJ, PD_PAIR_WCA = 1, 2
 
 _p = C.c_void_p
 _fp = C.c_void_p   # device pointers are passed as integers
@@ -71,6 +72,25 @@ class MDState(C.Structure):
     ]
 
 
+class EllParams(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int), ("n", C.c_int),
+        ("cutoff", C.c_double), ("skin", C.c_double),
+        ("cap", C.c_int), ("interval", C.c_int), ("model", C.c_int),
+        ("eps", C.c_float), ("sigma", C.c_float), ("rc2", C.c_float), ("eshift", C.c_float),
+        ("lanes", C.c_int),
+    ]
+
+
+class EllStats(C.Structure):
+    _fields_ = [
+        ("valid", C.c_int), ("error", C.c_int), ("requested", C.c_int),
+        ("step", C.c_longlong), ("last_build", C.c_longlong), ("interval", C.c_longlong),
+        ("checks", C.c_longlong), ("builds", C.c_longlong), ("required", C.c_longlong),
+        ("cap", C.c_int), ("lanes", C.c_int), ("allpairs", C.c_int),
+    ]
+
+
 # name: (restype, argtypes)
 _SIGS = {
     "pd_version": (C.c_int, []),
@@ -109,6 +129,20 @@ _SIGS = {
     "pd_md_evaluate": (C.c_int, [_p, C.c_int, _p]),
     "pd_md_step": (C.c_int, [_p, C.c_int, C.c_float, C.c_int, C.c_int, _p]),
     "pd_md_step_host": (C.c_int, [_p, _p, _p, C.c_int, C.c_float, C.POINTER(C.c_double), _p]),
+    "pd_ell_create": (C.c_int, [C.POINTER(_p), C.POINTER(EllParams), C.POINTER(C.c_double)]),
+    "pd_ell_destroy": (C.c_int, [_p]),
+    "pd_ell_update": (C.c_int, [_p, _fp, _fp, _fp, _p]),
+    "pd_ell_request": (C.c_int, [_p, _p]),
+    "pd_ell_forces": (C.c_int, [_p, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, C.c_int, _p]),
+    "pd_ell_status": (C.c_int, [_p, C.POINTER(EllStats)]),
+    "pd_ell_rows": (C.c_int, [_p, C.POINTER(_p), C.POINTER(_p)]),
+    "pd_ell_resize": (C.c_int, [_p, C.c_int]),
+    "pd_ell_md_create": (C.c_int, [C.POINTER(_p), _p, C.POINTER(MDState)]),
+    "pd_ell_md_destroy": (C.c_int, [_p]),
+    "pd_ell_md_evaluate": (C.c_int, [_p, C.c_int, _p]),
+    "pd_ell_md_step": (C.c_int, [_p, C.c_int, C.c_float, C.c_int, C.c_int, _p]),
+    "pd_ell_md_langevin": (C.c_int, [_p, C.c_int, C.c_float, C.c_float, C.c_float, C.c_ulonglong, C.c_int,
+                                     C.c_int, _p]),
 }
 
 EXPORTED = tuple(_SIGS)

@@ -419,3 +419,131 @@ class DeviceEngine:
                host_v.ctypes.data_as(C.c_void_p), int(nsteps), float(dt), C.byref(e) if energy else None,
                _stream(stream))
         return e.value if energy else None
+
+
+# ----------------------------------------------------------------------------- ELL route
+
+WCA_RC2_FACTOR = 1.2599211   # rc^2 / sigma^2 of the WCA model (src/engine/PairModels.jl:25)
+
+
+class ELLEngine:
+    """Cell-list neighbour rows with a fixed capacity and the row pair kernels (the reference's default
+    `CellList` route for Lennard-Jones and WCA: DeviceNeighborWorkspace, DeviceNeighborCUDA.jl:64-88;
+    UniformLJ / UniformWCA, src/engine/PairModels.jl:13-49).
+
+    ``dim`` is 2 or 3; coordinates are centred (|x| <= L/2).  ``capacity`` and ``interval`` are the
+    CellList ``capacity`` and ``rebuild_interval``; ``skin`` is its ``buffer``.
+    """
+
+    def __init__(self, n: int, box, *, dim: int = 3, model: str = "lj", epsilon: float = 1.0, sigma: float = 1.0,
+                 cutoff: float | None = None, skin: float = 0.4, capacity: int = 96, interval: int = 20,
+                 shift: bool = False, lanes: int = 0):
+        if model not in ("lj", "wca"):
+            raise ValueError(f"unknown pair model {model!r}")
+        eps, sig = float(epsilon), float(sigma)
+        if model == "wca":
+            rc2 = np.float32(WCA_RC2_FACTOR) * np.float32(sig * sig)
+            rc = float(np.sqrt(rc2)) if cutoff is None else float(cutoff)
+            eshift = 0.0
+        else:
+            if cutoff is None:
+                raise ValueError("LennardJones requires an explicit cutoff.")
+            rc = float(cutoff)
+            rc2 = np.float32(rc) * np.float32(rc)
+            eshift = splits.lj_cutoff_energy(sig, eps, rc) if shift else 0.0
+        p = N.EllParams()
+        p.dim, p.n = int(dim), int(n)
+        p.cutoff, p.skin = rc, float(skin)
+        p.cap, p.interval = int(capacity), int(interval)
+        p.model = N.PD_PAIR_LJ if model == "lj" else N.PD_PAIR_WCA
+        p.eps, p.sigma, p.rc2, p.eshift = eps, sig, float(rc2), float(eshift)
+        p.lanes = int(lanes)
+        self.params = p
+        self.n, self.dim, self.model = int(n), int(dim), model
+        self.box = tuple(float(b) for b in box) + (1.0,) * (3 - len(box))
+        h = C.c_void_p()
+        N.call("pd_ell_create", C.byref(h), C.byref(p), N.dbl3(self.box))
+        self.handle = h
+
+    def close(self, _destroy=_destroy):
+        if getattr(self, "handle", None):
+            _destroy("pd_ell_destroy", self.handle)
+            self.handle = None
+
+    __del__ = close
+
+    def update(self, x, y, z=None, stream=None):
+        N.call("pd_ell_update", self.handle, _ptr(x), _ptr(y), _ptr(z), _stream(stream))
+
+    def request(self, stream=None):
+        N.call("pd_ell_request", self.handle, _stream(stream))
+
+    def forces(self, x, y, z, fx, fy, fz, epot=None, vir=None, energy=False, stream=None):
+        N.call("pd_ell_forces", self.handle, _ptr(x), _ptr(y), _ptr(z), _ptr(fx), _ptr(fy), _ptr(fz), _ptr(epot),
+               _ptr(vir), int(bool(energy)), _stream(stream))
+
+    def status(self) -> dict:
+        st = N.EllStats()
+        N.call("pd_ell_status", self.handle, C.byref(st))
+        return {k: getattr(st, k) for k, _ in N.EllStats._fields_}
+
+    def resize(self, capacity: int):
+        N.call("pd_ell_resize", self.handle, int(capacity))
+
+    def rows_host(self):
+        """Host copies of the rows (as a list of neighbour-id arrays, truncated at the capacity)."""
+        r, c = C.c_void_p(), C.c_void_p()
+        N.call("pd_ell_rows", self.handle, C.byref(r), C.byref(c))
+        st = self.status()
+        cap, n = st["cap"], self.n
+        rows = torch.empty(cap * n, dtype=torch.int32, device="cuda")
+        counts = torch.empty(n, dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        _memcpy_d2d(rows.data_ptr(), r.value, 4 * cap * n)
+        _memcpy_d2d(counts.data_ptr(), c.value, 4 * n)
+        R = rows.cpu().numpy().reshape(cap, n)
+        cnt = counts.cpu().numpy()
+        return [R[:min(cnt[i], cap), i].copy() for i in range(n)], cnt
+
+
+class ELLDeviceEngine:
+    """Captured NVE / Langevin (BAOAB) steps on the ELL route (src/engine/Run.jl:162-294,
+    src/engine/Langevin.jl:58-88).  ``state``: dict of CUDA tensors x, y, (z), vx, vy, (vz), fx, fy,
+    (fz), inv_mass (or a float), epot, vir (N x 6 in 3D, N x 3 in 2D)."""
+
+    def __init__(self, ell: ELLEngine, state: dict):
+        s = N.MDState()
+        s.n = int(state["x"].numel())
+        for k in ("x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz"):
+            setattr(s, k, _ptr(state.get(k)))
+        im = state.get("inv_mass", 1.0)
+        if isinstance(im, torch.Tensor):
+            s.inv_mass, s.inv_mass_uniform = _ptr(im), 0.0
+        else:
+            s.inv_mass, s.inv_mass_uniform = 0, float(im)
+        s.epot = _ptr(state.get("epot"))
+        s.vir6 = _ptr(state.get("vir"))
+        self.state, self.ell = state, ell
+        h = C.c_void_p()
+        N.call("pd_ell_md_create", C.byref(h), ell.handle, C.byref(s))
+        self.handle = h
+        self._keep = s
+
+    def close(self, _destroy=_destroy):
+        if getattr(self, "handle", None):
+            _destroy("pd_ell_md_destroy", self.handle)
+            self.handle = None
+
+    __del__ = close
+
+    def evaluate(self, energy=False, stream=None):
+        N.call("pd_ell_md_evaluate", self.handle, int(bool(energy)), _stream(stream))
+
+    def step(self, nsteps: int, dt: float, energy_last=False, use_graph=True, stream=None):
+        N.call("pd_ell_md_step", self.handle, int(nsteps), float(dt), int(bool(energy_last)), int(bool(use_graph)),
+               _stream(stream))
+
+    def langevin(self, nsteps: int, dt: float, gamma: float, kT: float, seed: int, energy_last=False,
+                 use_graph=True, stream=None):
+        N.call("pd_ell_md_langevin", self.handle, int(nsteps), float(dt), float(gamma), float(kT),
+               int(seed) & 0xFFFFFFFFFFFFFFFF, int(bool(energy_last)), int(bool(use_graph)), _stream(stream))

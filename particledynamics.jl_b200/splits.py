@@ -214,3 +214,13 @@ def lj_type_table(sigma, epsilon, rcut, shift: bool = False, wca: bool = False) 
 
 
 WCA_RC_FACTOR = 1.2599211 ** 0.5   # r_c = 2^(1/6) sigma, written as the reference's sqrt(1.2599211)
+
+
+def lj_cutoff_energy(sigma: float, epsilon: float, rc: float) -> float:
+    """4 eps ((sigma/rc)^12 - (sigma/rc)^6), the potential-shift constant (lj_cutoff_energy,
+    src/engine/PairModels.jl:27-32)."""
+    if rc <= 0:
+        return 0.0
+    s2 = sigma * sigma / (rc * rc)
+    s6 = s2 * s2 * s2
+    return 4.0 * epsilon * (s6 * s6 - s6)

@@ -32,14 +32,32 @@ def fcc_lattice(ncell: int, rho: float, jitter: float = 0.05, seed: int = 0xC0FF
     return pos, (L, L, L)
 
 
-def maxwell_boltzmann(masses, T: float, seed: int = 0, kB: float = 1.0, remove_com: bool = True):
+def hex_random_2d(n_side: int, phi: float, sigma: float = 1.0, displacement: float = 0.25, seed: int = 0):
+    """n_side^2 disks of diameter sigma on a hexagonal lattice (rows shifted by half a spacing)
+    in a square box at packing fraction phi, each displaced uniformly by up to `displacement`
+    sigma per component; centred coordinates."""
+    rng = np.random.default_rng(seed)
+    n = n_side * n_side
+    L = math.sqrt(n * math.pi * sigma * sigma / (4.0 * phi))
+    a = L / n_side
+    i, j = np.meshgrid(np.arange(n_side), np.arange(n_side), indexing="ij")
+    x = (i + 0.5 * (j % 2) + 0.25) * a
+    y = (j + 0.5) * a
+    pos = np.stack([x.ravel(), y.ravel()], 1)
+    pos += rng.uniform(-displacement, displacement, size=pos.shape) * sigma
+    pos -= L / 2
+    pos -= L * np.floor(pos / L + 0.5)
+    return pos, (L, L)
+
+
+def maxwell_boltzmann(masses, T: float, seed: int = 0, kB: float = 1.0, remove_com: bool = True, dim: int = 3):
     """Velocities at temperature T (COM momentum removed, rescaled to exactly T)."""
     rng = np.random.default_rng(seed)
     m = np.asarray(masses, float)
-    v = rng.normal(size=(m.size, 3)) * np.sqrt(kB * T / m)[:, None]
+    v = rng.normal(size=(m.size, dim)) * np.sqrt(kB * T / m)[:, None]
     if remove_com:
         v -= (m[:, None] * v).sum(0) / m.sum()
-    dof = 3 * m.size - (3 if remove_com else 0)
+    dof = dim * m.size - (dim if remove_com else 0)
     ke = 0.5 * (m[:, None] * v * v).sum()
     if ke > 0:
         v *= math.sqrt(0.5 * dof * kB * T / ke)

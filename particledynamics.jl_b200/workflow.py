@@ -9,9 +9,12 @@ src/workflow/RunLoop.jl:403-457): force descriptors ``LennardJones``, ``WCA``,
 ``evaluate_forces_into_f!`` in Julia).  Every force evaluation and step runs on
 the GPU through libpdb200; there is no CPU path.
 
-Charged systems run on the cluster-pair backend (as the reference's user rule,
-src/simulation/ElectrostaticsCoupling.jl:76-86).  Uncharged 3D LJ/WCA systems
-also run on the cluster-pair list here.
+Routes follow the reference's user rules: charged systems run on the
+cluster-pair backend (src/simulation/ElectrostaticsCoupling.jl:76-86), as do
+LJ/WCA forces that ask for a ``ClusterPairList``; LJ/WCA forces with a
+``CellList`` (the default) run on the ELL route (cell list + neighbour rows,
+2D or 3D).  ``ConstantVolume`` integrates NVE; ``Langevin`` integrates BAOAB
+(ELL route).
 """
 from __future__ import annotations
 
@@ -22,7 +25,8 @@ import numpy as np
 import torch
 
 from . import splits
-from .engine import ClusterPairEngine, DeviceEngine, ElectrostaticsSolver, ElectrostaticsSpec
+from .engine import (ClusterPairEngine, DeviceEngine, ELLDeviceEngine, ELLEngine, ElectrostaticsSolver,
+                     ElectrostaticsSpec)
 
 
 # ----------------------------------------------------------------------------- descriptors
@@ -140,8 +144,26 @@ def electrostatics_spec(f) -> ElectrostaticsSpec:
 
 @dataclass
 class ConstantVolume:
-    """NVE velocity Verlet on a group (the whole system)."""
+    """NVE velocity Verlet on a group (the whole system) (src/workflow/Integrator.jl:45-55)."""
     group: object = None
+    thermostat: object = None
+
+
+@dataclass
+class Langevin:
+    """Langevin method on a group (the whole system) with friction gamma and bath temperature kT
+    (src/workflow/Integrator.jl:57-66), integrated by BAOAB."""
+    group: object = None
+    gamma: float = 1.0
+    kT: float = 1.0
+
+
+class VelocityVerlet:
+    """Velocity-Verlet stepping scheme (Integrator.jl:6-7)."""
+
+
+class BAOAB:
+    """BAOAB Langevin splitting (Integrator.jl:8-9)."""
 
 
 @dataclass
@@ -149,6 +171,7 @@ class Integrator:
     dt: float
     forces: list = field(default_factory=list)
     methods: list = field(default_factory=lambda: [ConstantVolume()])
+    scheme: object = None
 
 
 @dataclass
@@ -161,14 +184,15 @@ class Stage:
 
 
 class ParticleSystem:
-    """Positions (N x 3), box, types, per-type masses and charges (host data)."""
+    """Positions (N x D, D = 2 or 3 from the box), box, types, per-type masses and charges (host data)."""
 
     def __init__(self, positions, box, types=("A",), typeids=None, masses=None, charges=None, velocities=None):
-        self.positions = np.asarray(positions, float).reshape(-1, 3)
-        n = len(self.positions)
         self.box = tuple(float(b) for b in box)
-        if len(self.box) != 3:
-            raise ValueError("this build supports 3D periodic boxes")
+        if len(self.box) not in (2, 3):
+            raise ValueError("periodic boxes are 2D or 3D")
+        self.dim = len(self.box)
+        self.positions = np.asarray(positions, float).reshape(-1, self.dim)
+        n = len(self.positions)
         self.types = [str(t) for t in types]
         self.typeids = np.ones(n, np.int32) if typeids is None else np.asarray(typeids, np.int32)
 
@@ -182,7 +206,7 @@ class ParticleSystem:
 
         self.masses = per_particle(masses, 1.0)
         self.charges = None if charges is None else per_particle(charges, 0.0)
-        self.velocities = None if velocities is None else np.asarray(velocities, float).reshape(n, 3)
+        self.velocities = None if velocities is None else np.asarray(velocities, float).reshape(n, self.dim)
 
     @property
     def n(self) -> int:
@@ -194,22 +218,36 @@ class ParticleSystem:
 class SimulationState:
     """Device state of one system and its engines (the SimulationState of the reference)."""
 
-    def __init__(self, system: ParticleSystem, forces, dt: float, device="cuda"):
+    def __init__(self, system: ParticleSystem, forces, dt: float, device="cuda", methods=None, seed: int = 0):
         if not torch.cuda.is_available():
             raise RuntimeError("libpdb200 needs a CUDA device; there is no CPU force path")
         self.dev = torch.device(device)
         n = system.n
         self.n = n
+        self.dim = system.dim
         self.box = system.box
         f32 = dict(dtype=torch.float32, device=self.dev)
         L = np.array(self.box)
+        D = self.dim
         pos = system.positions - L * np.floor(system.positions / L + 0.5)   # centred image
-        self.x, self.y, self.z = (torch.tensor(pos[:, d], **f32) for d in range(3))
-        v = system.velocities if system.velocities is not None else np.zeros((n, 3))
-        self.vx, self.vy, self.vz = (torch.tensor(v[:, d], **f32) for d in range(3))
-        self.fx, self.fy, self.fz = (torch.zeros(n, **f32) for _ in range(3))
+        comp = [torch.tensor(pos[:, d], **f32) for d in range(D)] + [None] * (3 - D)
+        self.x, self.y, self.z = comp
+        v = system.velocities if system.velocities is not None else np.zeros((n, D))
+        comp = [torch.tensor(v[:, d], **f32) for d in range(D)] + [None] * (3 - D)
+        self.vx, self.vy, self.vz = comp
+        comp = [torch.zeros(n, **f32) for _ in range(D)] + [None] * (3 - D)
+        self.fx, self.fy, self.fz = comp
         self.epot = torch.zeros(n, **f32)
-        self.vir6 = torch.zeros((n, 6), **f32)
+        self.vir6 = torch.zeros((n, 6 if D == 3 else 3), **f32)
+        self.langevin = None
+        for m in methods or []:
+            if isinstance(m, Langevin):
+                if float(m.gamma) <= 0:
+                    raise ValueError("Langevin gamma must be positive")
+                self.langevin = (float(m.gamma), float(m.kT))
+            elif not isinstance(m, ConstantVolume):
+                raise NotImplementedError(f"integration method {type(m).__name__} is not part of this build")
+        self.seed = int(seed)
         self.vglobal = torch.zeros(6, **f32)
         self.q = torch.tensor(system.charges, **f32) if system.charges is not None else None
         self.typ = torch.tensor(system.typeids, dtype=torch.int32, device=self.dev)
@@ -225,6 +263,14 @@ class SimulationState:
         elec = [f for f in forces if isinstance(f, (PME, PPPM))]
         if len(vdw) > 1 or len(elec) > 1:
             raise ValueError("at most one short-range vdW force and one electrostatics force")
+        self.ell = None
+        if vdw and not elec and not isinstance(vdw[0].neighborlist, ClusterPairList):
+            self._compile_ell(vdw[0])
+            return
+        if self.dim != 3:
+            raise ValueError("the cluster-pair backend needs a 3D box")
+        if self.langevin is not None:
+            raise NotImplementedError("Langevin runs on the CellList (ELL) route in this build")
         lj = None
         rlj = 0.0
         nl = None
@@ -280,6 +326,49 @@ class SimulationState:
         self.engine = DeviceEngine(self.cluster, self.solver, state, self.box)
         self.forces_valid = False
 
+    def _compile_ell(self, f):
+        """The ELL route: cell list + rows with the CellList policy (Forces.jl:255-283)."""
+        if f.mode != "standard":
+            raise ValueError(f"Only mode=standard is supported for {type(f).__name__}.")
+        if f.pair_table is not None:
+            raise NotImplementedError("type-dependent pair tables run on the cluster-pair route in this build")
+        if f.epsilon is None or f.sigma is None:
+            raise ValueError(f"{type(f).__name__} requires epsilon and sigma.")
+        nl = f.neighborlist if isinstance(f.neighborlist, CellList) else CellList()
+        if f.neighborlist is not None and not isinstance(f.neighborlist, CellList):
+            raise ValueError(f"Neighbor specification must be CellList or ClusterPairList; got {type(f.neighborlist).__name__}.")
+        if nl.capacity <= 0:
+            raise ValueError("CellList capacity must be positive.")
+        if nl.buffer < 0:
+            raise ValueError("CellList buffer must be nonnegative.")
+        if nl.rebuild_interval <= 0:
+            raise ValueError("CellList rebuild_interval must be positive.")
+        if isinstance(f, WCA):
+            model, cutoff, shift = "wca", (None if f.cutoff is None else float(f.cutoff)), False
+        else:
+            if f.cutoff is None:
+                raise ValueError("LennardJones requires an explicit cutoff.")
+            model, cutoff, shift = "lj", float(f.cutoff), f.vdw_modifier == "potential_shift"
+        self.solver = None
+        self.cluster = None
+        self.ell = ELLEngine(self.n, self.box, dim=self.dim, model=model, epsilon=f.epsilon, sigma=f.sigma,
+                             cutoff=cutoff, skin=nl.buffer, capacity=nl.capacity,
+                             interval=min(max(int(nl.rebuild_interval), 1), 100), shift=shift)
+        state = dict(x=self.x, y=self.y, z=self.z, vx=self.vx, vy=self.vy, vz=self.vz, fx=self.fx, fy=self.fy,
+                     fz=self.fz, inv_mass=self.inv_mass, epot=self.epot, vir=self.vir6)
+        self.engine = ELLDeviceEngine(self.ell, state)
+        self.forces_valid = False
+
+    def _ell_check(self):
+        st = self.ell.status()
+        if st["error"] == 1:
+            raise RuntimeError(f"Neighbor capacity {st['cap']} exceeded: a row needs {st['required']} entries; "
+                               "raise CellList capacity")
+        if st["error"] == 2:
+            raise ValueError("Device ELL requires finite, centered coordinates; execution stopped before "
+                             "rebuilding/forces")
+        return st
+
     # -- force evaluation
     def evaluate_forces_into_f(self, energy: bool = False):
         """evaluate_forces_into_f!(st, energy) (ForceEvaluation.jl:40-44)."""
@@ -287,13 +376,26 @@ class SimulationState:
             if self.solver is None:
                 self.vglobal.zero_()
             self.engine.evaluate(energy=energy, stream=self.stream)
+            if self.ell is not None:
+                self.stream.synchronize()
+                st = self.ell.status()
+                if st["error"] == 1:
+                    # capacity recovery at a host boundary: larger rows, rebuild, evaluate again
+                    self.ell.resize(max(int(st["required"] * 1.25) + 8, st["cap"] + 8))
+                    self.engine.evaluate(energy=energy, stream=self.stream)
         self.stream.synchronize()
+        if self.ell is not None:
+            self._ell_check()
         self.forces_valid = True
 
     def step(self, nsteps: int = 1, energy_last: bool = False, use_graph: bool = True):
         if not self.forces_valid:
             self.evaluate_forces_into_f(False)
-        self.engine.step(nsteps, self.dt, energy_last=energy_last, use_graph=use_graph, stream=self.stream)
+        if self.langevin is not None:
+            self.engine.langevin(nsteps, self.dt, self.langevin[0], self.langevin[1], self.seed,
+                                 energy_last=energy_last, use_graph=use_graph, stream=self.stream)
+        else:
+            self.engine.step(nsteps, self.dt, energy_last=energy_last, use_graph=use_graph, stream=self.stream)
         self.step_count += nsteps
 
     def synchronize(self):
@@ -304,24 +406,33 @@ class SimulationState:
         self.synchronize()
         return float(self.epot.double().sum())
 
+    def _comps(self, a, b, c):
+        return [a, b] + ([c] if self.dim == 3 else [])
+
     def kinetic_energy(self) -> float:
         self.synchronize()
-        v2 = (self.vx.double() ** 2 + self.vy.double() ** 2 + self.vz.double() ** 2).cpu().numpy()
+        v2 = sum(t.double() ** 2 for t in self._comps(self.vx, self.vy, self.vz)).cpu().numpy()
         return 0.5 * float((self.masses * v2).sum())
 
     def virial_tensor(self) -> dict:
-        """Pair virial rows plus the mesh virial (xx, yy, zz, xy, xz, yz)."""
+        """Pair virial rows plus the mesh virial (xx, yy, zz, xy, xz, yz; 2D: xx, yy, xy)."""
         self.synchronize()
+        if self.dim == 2:
+            return dict(zip(("xx", "yy", "xy"), self.vir6.double().sum(0).cpu().numpy()))
         w = self.vir6.double().sum(0).cpu().numpy() + self.vglobal.double().cpu().numpy()
         return dict(zip(("xx", "yy", "zz", "xy", "xz", "yz"), w))
 
     def forces(self) -> np.ndarray:
         self.synchronize()
-        return torch.stack([self.fx, self.fy, self.fz], 1).double().cpu().numpy()
+        return torch.stack(self._comps(self.fx, self.fy, self.fz), 1).double().cpu().numpy()
+
+    def velocities(self) -> np.ndarray:
+        self.synchronize()
+        return torch.stack(self._comps(self.vx, self.vy, self.vz), 1).double().cpu().numpy()
 
     def positions(self) -> np.ndarray:
         self.synchronize()
-        return torch.stack([self.x, self.y, self.z], 1).double().cpu().numpy()
+        return torch.stack(self._comps(self.x, self.y, self.z), 1).double().cpu().numpy()
 
 
 class Simulation:
@@ -330,13 +441,18 @@ class Simulation:
     def __init__(self, system: ParticleSystem, integrator: Integrator, precision="f32", seed: int = 0):
         if precision not in ("f32", np.float32, "Float32"):
             raise ValueError("this build runs the Float32 force path")
-        for m in integrator.methods:
-            if not isinstance(m, ConstantVolume):
-                raise NotImplementedError(f"integration method {type(m).__name__} is not part of this build")
+        if len(integrator.methods) != 1:
+            raise NotImplementedError("one integration method covering the whole system")
+        m = integrator.methods[0]
+        if isinstance(m, ConstantVolume) and m.thermostat is not None:
+            raise NotImplementedError("thermostats other than Langevin are not part of this build")
+        if isinstance(m, Langevin) and integrator.scheme not in (None, BAOAB) and not isinstance(integrator.scheme,
+                                                                                                  BAOAB):
+            raise NotImplementedError("Langevin integrates with the BAOAB scheme in this build")
         self.system = system
         self.integrator = integrator
         self.seed = seed
-        self.state = SimulationState(system, integrator.forces, integrator.dt)
+        self.state = SimulationState(system, integrator.forces, integrator.dt, methods=integrator.methods, seed=seed)
 
 
 def state(sim: Simulation) -> SimulationState:
