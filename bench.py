@@ -220,6 +220,17 @@ def cpu_baseline_run(pd, ora, steps_budget_s=15.0, max_steps=None):
     return ms, nsteps, os.cpu_count()
 
 
+def profiled_traffic(name: str):
+    """DRAM bytes per launch (read + write) of one ncu capture, from its committed summary."""
+    import re
+    try:
+        txt = (ROOT / "profiles" / name).read_text()
+    except OSError:
+        return None
+    m = re.search(r"dram bytes per launch \(read \+ write\) \| (\d+)", txt)
+    return int(m.group(1)) if m else None
+
+
 def run_reference(args, world, rank):
     """--impl reference: the CPU restatement on the host cores (rank 0 only)."""
     if rank != 0:
@@ -266,6 +277,9 @@ def main():
     ap.add_argument("--no-flush", action="store_true", help="(diagnostic) do not flush L2 between steps")
     ap.add_argument("--buffer", type=float, default=BUFFER, help="cluster list buffer (Angstrom)")
     ap.add_argument("--prune", type=float, default=PRUNE, help="prune buffer (Angstrom)")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling run for ncu: the same workload, --warmup then --steps directly launched steps "
+                         "(no graph, no timing, no baseline), so a launch list sees every kernel")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -290,6 +304,15 @@ def main():
     st = sim.state
     s = st.stream
     pd.evaluate_forces_into_f(sim, energy=False)
+    if args.profile:
+        st.step(args.warmup, use_graph=False)
+        st.synchronize()
+        st.step(args.steps, use_graph=False)
+        st.synchronize()
+        if rank == 0:
+            print(json.dumps({"profile": "melt64k eager steps", "steps": args.steps, "warmup": args.warmup,
+                              "list": st.cluster.statistics()}))
+        return
     # kernels of one eager step: the always-run part (the prune kernel included: it is launched every
     # step and returns at once unless the device decision asks for a prune) plus the build kernels, which
     # the captured graph launches only inside its conditional node on steps that rebuild the list
@@ -364,7 +387,8 @@ def main():
     achieved = flops / (pair_ms * 1e-3) / 1e12
     roofline = {"kernel": "k_pairs<LJ uniform, Coulomb polynomial, force only>", "bound": "fp32",
                 "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                "traffic": None, "per_launch_ms": pair_ms, "pairs_within_rc": npairs, "flop_per_pair": flop_pair,
+                "traffic": profiled_traffic("k_pairs_melt64k.md"), "per_launch_ms": pair_ms,
+                "pairs_within_rc": npairs, "flop_per_pair": flop_pair,
                 "peak_source": "nominal FP32 FMA rate at sm_max_mhz (MEASURED_PEAKS.json has no FP32 figure)"}
 
     cpu = None
