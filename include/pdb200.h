@@ -346,6 +346,78 @@ int pd_ell_md_step(pd_ell_md *md, int nsteps, float dt, int energy_last, int use
 int pd_ell_md_langevin(pd_ell_md *md, int nsteps, float dt, float gamma, float kT, unsigned long long seed,
                        int energy_last, int use_graph, pd_stream_t s);
 
+/* ------------------------------------------------------------------------------------------
+ * Learned coarse-mesh correction (no reference counterpart: an added form judged against the
+ * plain fine-mesh PME above).  PME runs on a 2x coarser mesh; a 32-128-128-1 SiLU network
+ * (BF16 tensor cores, FP32 accumulation) maps each particle's local charge descriptors to a
+ * scalar s_i, and the force residual is F_i = s_i V_i with
+ * V_i = sum_{r_ij < rcut} q_i q_j b(r_ij) (r_i - r_j).
+ * ------------------------------------------------------------------------------------------ */
+#define PD_LEARNED_MAX_RADIAL 8
+typedef struct pd_mlp pd_mlp;
+typedef struct pd_learned pd_learned;
+
+/* Network parameters, FP32, concatenated: w1 [128][32], b1 [128], w2 [128][128], b2 [128],
+ * w3 [128], b3 [1] (pd_mlp_param_count() floats).  The tensor cores read BF16 copies of w1, w2. */
+int pd_mlp_param_count(void);
+int pd_mlp_create(pd_mlp **out);
+int pd_mlp_destroy(pd_mlp *net);
+int pd_mlp_set_params(pd_mlp *net, const float *host);   /* also clears gradients and Adam state */
+int pd_mlp_get_params(pd_mlp *net, float *host);
+int pd_mlp_get_grads(pd_mlp *net, float *host);
+/* Inference over n rows of X (n x 32 BF16, device): s (n floats, may be NULL) and, with V4
+ * (n x float4) given, corr4 (n x float4) = (s V.x, s V.y, s V.z, s). */
+int pd_mlp_forward(pd_mlp *net, const void *X, int n, float *s, const float *V4, float *corr4, pd_stream_t st);
+/* Fused forward + backward over n rows for the loss sum_r (s_r^2 a_r - 2 s_r b_r) scale / 2, i.e.
+ * dL/ds_r = scale (s_r a_r - b_r), with ab = n x (a, b) floats; gradients are added to the
+ * network's gradient buffers and the loss to its FP64 loss word. */
+int pd_mlp_train(pd_mlp *net, const void *X, const float *ab, int n, float scale, pd_stream_t st);
+/* Adam on the FP32 parameters with the gradients times grad_scale; clears the gradients and
+ * refreshes the BF16 weight copies. */
+int pd_mlp_adam(pd_mlp *net, float lr, float beta1, float beta2, float eps, float grad_scale, pd_stream_t st);
+int pd_mlp_loss(pd_mlp *net, double *out, int reset);
+int pd_mlp_zero_grads(pd_mlp *net, pd_stream_t st);
+/* 1 after a tensor-core wait that timed out (latched). */
+int pd_mlp_error(pd_mlp *net, int *out);
+
+typedef struct {
+    float rcut;                 /* descriptor / residual cutoff (6 A) */
+    float skin;                 /* neighbour-row skin */
+    int cap;                    /* row capacity */
+    float mu0, dmu, sigma;      /* feature Gaussians: centres mu0 + k dmu (k < 16), width sigma */
+    int nb;                     /* radial terms of b(r), 1..PD_LEARNED_MAX_RADIAL */
+    float nu0, dnu, tau;        /* their centres nu0 + m dnu and width tau */
+    float coef[PD_LEARNED_MAX_RADIAL];   /* b(r) = fc(r) sum_m coef[m] exp(-(r - nu_m)^2 / (2 tau^2)) */
+} pd_learned_params;
+
+int pd_learned_create(pd_learned **out, const pd_learned_params *p, int n, const double box[3]);
+int pd_learned_destroy(pd_learned *h);
+int pd_learned_set_radial(pd_learned *h, const float *coef, int nb);
+/* Row update (own displacement decision) and descriptors at centred coordinates: X (n x 32 BF16),
+ * species 0 = type id 1, species 1 = every other id (1-based type ids; type may be NULL),
+ * V4 (n x float4); NULL selects the handle's buffers.  With Vb4 (nb x n x float4) the radial-term
+ * vectors V_i^(m) are written instead of V. */
+int pd_learned_descriptors(pd_learned *h, const float *x, const float *y, const float *z, const float *q,
+                           const int *type, void *X, float *V4, float *Vb4, pd_stream_t st);
+/* Descriptors + network: corr4 (n x float4, NULL: the handle's buffer) = (s V, s). */
+int pd_learned_correction(pd_learned *h, pd_mlp *net, const float *x, const float *y, const float *z, const float *q,
+                          const int *type, float *corr4, pd_stream_t st);
+int pd_learned_buffers(pd_learned *h, void **X, float **V4, float **corr4);
+int pd_learned_status(pd_learned *h, pd_ell_stats *out);
+int pd_learned_resize(pd_learned *h, int cap);
+/* Attach (or with NULL detach) the correction to a step engine: every force pass then adds
+ * corr = s V to the forces before the closing kick (the descriptors and the network run on a
+ * third stream beside the pair pass and the mesh). */
+int pd_md_set_learned(pd_md *md, pd_learned *h, pd_mlp *net);
+
+/* FP64 Ewald sum on the GPU (ewald_reference, test/ewald_reference.jl:50-127, restated): rq4 =
+ * n x (x, y, z, q) doubles on the device; real space over minimum images within x / alpha
+ * (must be below half the smallest box length), reciprocal space within |k| < 2 alpha x,
+ * x = sqrt(digits ln 10); parts: 1 real space, 2 reciprocal space, 4 self energy.  F (n x 3
+ * doubles, device) is overwritten; E (host, may be NULL) receives the energy. */
+int pd_ewald_oracle(int n, const double *rq4, const double box[3], double C, double alpha, double digits, int parts,
+                    double *F, double *E);
+
 #ifdef __cplusplus
 }
 #endif

@@ -17,7 +17,8 @@ CSRC = HERE / "csrc"
 LIB = HERE / "libpdb200.so"
 ROOT = HERE.parent
 
-SOURCES = ["cluster_list.cu", "cluster_pairs.cu", "mesh.cu", "md.cu", "noalloc.cu", "ell.cu"]
+SOURCES = ["cluster_list.cu", "cluster_pairs.cu", "mesh.cu", "md.cu", "noalloc.cu", "ell.cu", "mlp.cu", "learned.cu",
+           "ewald.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -37,26 +38,47 @@ def _stale() -> bool:
     return any(p.stat().st_mtime > t for p in deps if p.exists())
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    """Compile the library if a source is newer than the shared object."""
-    if not force and not _stale():
-        return LIB
-    cuda_lib = Path(nvcc()).resolve().parent.parent / "lib64"
-    cmd = [
-        nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-        "-Xcompiler", "-O2", "-o", str(LIB), *[str(CSRC / s) for s in SOURCES],
-        f"-L{cuda_lib}", "-lcufft", "-Xlinker", f"-rpath,{cuda_lib}",
-    ]
+def _compile(src: Path, obj: Path, verbose: bool) -> str:
+    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+           "-c", str(src), "-o", str(obj)]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
-        print(" ".join(cmd), file=sys.stderr)
-    tmp = LIB.with_suffix(".so.tmp")
-    cmd[cmd.index(str(LIB))] = str(tmp)
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
-    if verbose:
-        print(res.stdout + res.stderr, file=sys.stderr)
+        raise RuntimeError(f"nvcc failed on {src.name}:\n" + res.stdout + res.stderr)
+    return res.stdout + res.stderr
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compile the library if a source is newer than the shared object.
+
+    Each translation unit is compiled to an object under ``_build/`` in parallel (a unit is
+    recompiled when it, a shared header or this script is newer than its object), then the
+    objects are linked into the shared library."""
+    if not force and not _stale():
+        return LIB
+    from concurrent.futures import ThreadPoolExecutor
+
+    objdir = HERE / "_build"
+    objdir.mkdir(exist_ok=True)
+    headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.hpp")) + [ROOT / "include" / "pdb200.h", Path(__file__)]
+    newest_header = max(p.stat().st_mtime for p in headers if p.exists())
+    jobs = []
+    for s in SOURCES:
+        src, obj = CSRC / s, objdir / (Path(s).stem + ".o")
+        if force or not obj.exists() or obj.stat().st_mtime < max(src.stat().st_mtime, newest_header):
+            jobs.append((src, obj))
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for out in ex.map(lambda j: _compile(j[0], j[1], verbose), jobs):
+            if verbose and out:
+                print(out, file=sys.stderr)
+    cuda_lib = Path(nvcc()).resolve().parent.parent / "lib64"
+    tmp = LIB.with_suffix(".so.tmp")
+    cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *[str(objdir / (Path(s).stem + ".o")) for s in SOURCES],
+           f"-L{cuda_lib}", "-lcufft", "-Xlinker", f"-rpath,{cuda_lib}"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("nvcc link failed:\n" + res.stdout + res.stderr)
     os.replace(tmp, LIB)
     return LIB
 

@@ -17,6 +17,7 @@ PD_MESH_SPME, PD_MESH_P3M_AD, PD_MESH_P3M_IK = 1, 2, 3
 PD_MAX_POLY = 32
 PD_MAX_TYPES = 16
 PD_PAIR_LJ, PD_PAIR_WCA = 1, 2
+PD_LEARNED_MAX_RADIAL = 8
 
 _p = C.c_void_p
 _fp = C.c_void_p   # device pointers are passed as integers
@@ -91,6 +92,15 @@ class EllStats(C.Structure):
     ]
 
 
+class LearnedParams(C.Structure):
+    _fields_ = [
+        ("rcut", C.c_float), ("skin", C.c_float), ("cap", C.c_int),
+        ("mu0", C.c_float), ("dmu", C.c_float), ("sigma", C.c_float),
+        ("nb", C.c_int), ("nu0", C.c_float), ("dnu", C.c_float), ("tau", C.c_float),
+        ("coef", C.c_float * PD_LEARNED_MAX_RADIAL),
+    ]
+
+
 # name: (restype, argtypes)
 _SIGS = {
     "pd_version": (C.c_int, []),
@@ -143,6 +153,29 @@ _SIGS = {
     "pd_ell_md_step": (C.c_int, [_p, C.c_int, C.c_float, C.c_int, C.c_int, _p]),
     "pd_ell_md_langevin": (C.c_int, [_p, C.c_int, C.c_float, C.c_float, C.c_float, C.c_ulonglong, C.c_int,
                                      C.c_int, _p]),
+    "pd_mlp_param_count": (C.c_int, []),
+    "pd_mlp_create": (C.c_int, [C.POINTER(_p)]),
+    "pd_mlp_destroy": (C.c_int, [_p]),
+    "pd_mlp_set_params": (C.c_int, [_p, _p]),
+    "pd_mlp_get_params": (C.c_int, [_p, _p]),
+    "pd_mlp_get_grads": (C.c_int, [_p, _p]),
+    "pd_mlp_forward": (C.c_int, [_p, _fp, C.c_int, _fp, _fp, _fp, _p]),
+    "pd_mlp_train": (C.c_int, [_p, _fp, _fp, C.c_int, C.c_float, _p]),
+    "pd_mlp_adam": (C.c_int, [_p, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, _p]),
+    "pd_mlp_loss": (C.c_int, [_p, C.POINTER(C.c_double), C.c_int]),
+    "pd_mlp_zero_grads": (C.c_int, [_p, _p]),
+    "pd_mlp_error": (C.c_int, [_p, C.POINTER(C.c_int)]),
+    "pd_learned_create": (C.c_int, [C.POINTER(_p), C.POINTER(LearnedParams), C.c_int, C.POINTER(C.c_double)]),
+    "pd_learned_destroy": (C.c_int, [_p]),
+    "pd_learned_set_radial": (C.c_int, [_p, _p, C.c_int]),
+    "pd_learned_descriptors": (C.c_int, [_p, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _fp, _p]),
+    "pd_learned_correction": (C.c_int, [_p, _p, _fp, _fp, _fp, _fp, _fp, _fp, _p]),
+    "pd_learned_buffers": (C.c_int, [_p, C.POINTER(_p), C.POINTER(_p), C.POINTER(_p)]),
+    "pd_learned_status": (C.c_int, [_p, C.POINTER(EllStats)]),
+    "pd_learned_resize": (C.c_int, [_p, C.c_int]),
+    "pd_md_set_learned": (C.c_int, [_p, _p, _p]),
+    "pd_ewald_oracle": (C.c_int, [C.c_int, _fp, C.POINTER(C.c_double), C.c_double, C.c_double, C.c_double, C.c_int,
+                                  _fp, C.POINTER(C.c_double)]),
 }
 
 EXPORTED = tuple(_SIGS)

@@ -668,6 +668,7 @@ float4 *ell_packed(pd_ell *e) { return e->xq; }
 float4 *ell_ref(pd_ell *e) { return e->ref; }
 float ell_threshold(const pd_ell *e) { return e->threshold; }
 int ell_dim(const pd_ell *e) { return e->dim; }
+int ell_capacity(const pd_ell *e) { return e->cap; }
 
 static int ell_alloc_rows(pd_ell *e, int cap) {
     PD_CHECK(cap > 0, PD_EINVAL, "Invalid ELL capacity");

@@ -148,7 +148,7 @@ int mesh_transform_packed(pd_mesh *m, const float4 *xq, int nchunks, const int *
 int mesh_gather_join(pd_mesh *m, pd_cluster *c, const float4 *xq, const int *perm, const int *ns_dev, int nchunks,
                      float *fx, float *fy, float *fz, float *vx, float *vy, float *vz, const float *inv_mass,
                      float inv_mass_uniform, float half_dt, float *epot, float *vir6, float *vglobal6, const float *q,
-                     float half_c_self, int energy, cudaStream_t s);
+                     float half_c_self, const float4 *extra, int energy, cudaStream_t s);
 int mesh_store_virial(pd_mesh *m, float *vglobal6, cudaStream_t s);
 // Cluster internals used by the step engine.
 int cluster_decide_launch(pd_cluster *c, const float *x, const float *y, const float *z, int fixed, cudaStream_t s);
@@ -158,4 +158,11 @@ int cluster_build_launch(pd_cluster *c, const float *x, const float *y, const fl
 int cluster_prune_launch(pd_cluster *c, int conditional, cudaStream_t s);
 int cluster_read_counts(pd_cluster *c, int *host, cudaStream_t s);
 int cluster_set_word(pd_cluster *c, int word, int value, cudaStream_t s);
+// ELL, network and learned-correction internals used by the learned form and the step engine.
+int ell_capacity(const pd_ell *e);
+int mlp_forward_launch(const pd_mlp *q, const void *X, int n, float *s, const float4 *V, float4 *corr,
+                       cudaStream_t st);
+int learned_correction_launch(pd_learned *h, const pd_mlp *net, const float *x, const float *y, const float *z,
+                              const float *q, const int *type, float4 *corr, cudaStream_t s);
+const float4 *learned_corr(const pd_learned *h);
 }  // namespace pdb

@@ -37,6 +37,11 @@ struct pd_md {
     cudaStream_t exec_stream[2] = {nullptr, nullptr};
     double *esum = nullptr;   // device FP64 energy sum
     float half_c_self = 0.f;
+    // learned coarse-mesh correction: descriptors + network on a third stream
+    pd_learned *learned = nullptr;
+    const pd_mlp *net = nullptr;
+    cudaStream_t side2 = nullptr;
+    cudaEvent_t ev_fork2 = nullptr, ev_join2 = nullptr;
 };
 
 namespace pdb {
@@ -214,6 +219,20 @@ static int fork_mesh(pd_md *md, int energy, cudaStream_t s) {
     return PD_OK;
 }
 
+// The learned correction forks onto the third stream once the step's coordinates are final
+// (after the drift); the join waits for it before the closing gather.
+static int fork_learned(pd_md *md, cudaStream_t s) {
+    if (!md->learned) return PD_OK;
+    pd_md_state &st = md->st;
+    int rc;
+    PD_CUDA(cudaEventRecord(md->ev_fork2, s));
+    PD_CUDA(cudaStreamWaitEvent(md->side2, md->ev_fork2, 0));
+    if ((rc = learned_correction_launch(md->learned, md->net, st.x, st.y, st.z, st.q, st.type, nullptr, md->side2)))
+        return rc;
+    PD_CUDA(cudaEventRecord(md->ev_join2, md->side2));
+    return PD_OK;
+}
+
 // Closing part of a step: the pair pass (the mesh transform already forked), then the join.
 static int enqueue_forces(pd_md *md, int energy, float half_dt, cudaStream_t s) {
     pd_cluster *c = md->c;
@@ -223,9 +242,10 @@ static int enqueue_forces(pd_md *md, int energy, float half_dt, cudaStream_t s) 
     if ((rc = cluster_pairs_launch(c, energy, s))) return rc;
     if (m) {
         PD_CUDA(cudaStreamWaitEvent(s, md->ev_join, 0));
+        if (md->learned) PD_CUDA(cudaStreamWaitEvent(s, md->ev_join2, 0));
         rc = mesh_gather_join(m, c, c->xq, c->perm, c->counts + W_NS, c->nsmax, st.fx, st.fy, st.fz, st.vx, st.vy,
                               st.vz, st.inv_mass, st.inv_mass_uniform, half_dt, st.epot, st.vir6, st.vglobal6, st.q,
-                              md->half_c_self, energy, s);
+                              md->half_c_self, md->learned ? learned_corr(md->learned) : nullptr, energy, s);
         if (rc) return rc;
     } else {
         const int blocks = (c->nslot + 255) / 256;
@@ -306,6 +326,7 @@ static int enqueue_step(pd_md *md, float dt, int energy, cudaStream_t s, int con
         if ((rc = cluster_build_launch(c, st.x, st.y, st.z, q, st.type, 1, s))) return rc;
     }
     // the mesh transform forks before the prune, which runs as a flag-gated kernel
+    if ((rc = fork_learned(md, s))) return rc;
     if ((rc = fork_mesh(md, energy, s))) return rc;
     if ((rc = cluster_prune_launch(c, 1, s))) return rc;
     return enqueue_forces(md, energy, 0.5f * dt, s);
@@ -354,6 +375,9 @@ int pd_md_destroy(pd_md *md) {
     if (md->ev_join) cudaEventDestroy(md->ev_join);
     if (md->side) cudaStreamDestroy(md->side);
     if (md->body) cudaStreamDestroy(md->body);
+    if (md->side2) cudaStreamDestroy(md->side2);
+    if (md->ev_fork2) cudaEventDestroy(md->ev_fork2);
+    if (md->ev_join2) cudaEventDestroy(md->ev_join2);
     dfree(md->esum);
     delete md;
     return PD_OK;
@@ -392,9 +416,32 @@ int pd_md_evaluate(pd_md *md, int energy, pd_stream_t sp) {
     } else {
         if ((rc = pd_cluster_pack(c, st.x, st.y, st.z, q, st.type, sp))) return rc;
     }
+    if ((rc = fork_learned(md, s))) return rc;
     if ((rc = fork_mesh(md, energy, s))) return rc;
     if ((rc = cluster_prune_launch(c, 1, s))) return rc;
     return enqueue_forces(md, energy, 0.f, s);
+}
+
+int pd_md_set_learned(pd_md *md, pd_learned *h, pd_mlp *net) {
+    PD_CHECK(md, PD_EINVAL, "pd_md_set_learned: null handle");
+    PD_CHECK(!h == !net, PD_EINVAL, "pd_md_set_learned: the correction needs both the handle and the network");
+    PD_CHECK(!h || md->m, PD_EINVAL, "pd_md_set_learned: the correction needs a mesh");
+    if (h && !md->side2) {
+        int prio_lo = 0, prio_hi = 0;
+        cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+        PD_CUDA(cudaStreamCreateWithPriority(&md->side2, cudaStreamNonBlocking, prio_hi));
+        PD_CUDA(cudaEventCreateWithFlags(&md->ev_fork2, cudaEventDisableTiming));
+        PD_CUDA(cudaEventCreateWithFlags(&md->ev_join2, cudaEventDisableTiming));
+    }
+    md->learned = h;
+    md->net = net;
+    // captured steps hold the old sequence
+    for (int k = 0; k < 2; ++k)
+        if (md->exec[k]) {
+            cudaGraphExecDestroy(md->exec[k]);
+            md->exec[k] = nullptr;
+        }
+    return PD_OK;
 }
 
 int pd_md_step(pd_md *md, int nsteps, float dt, int energy_last, int use_graph, pd_stream_t sp) {

@@ -381,6 +381,7 @@ struct GatherOut {
     int nslot;
     float half_c_self;       // JOIN energy: 0.5 C selfc
     float bg;                // background potential per unit charge
+    const float4 *extra;     // JOIN: per-particle force added before the kick (learned correction), or null
 };
 
 template <int P, int MODE, bool ENERGY>   // MODE 0: add, 1: set, 2: join (+ kick)
@@ -404,8 +405,10 @@ __global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_gather(const
     // overlaps the brick set-up and the potential load below
     float4 fpair = make_float4(0.f, 0.f, 0.f, 0.f);
     float pvx = 0.f, pvy = 0.f, pvz = 0.f, pim = 0.f;
+    float4 fextra = make_float4(0.f, 0.f, 0.f, 0.f);
     if (MODE == 2 && h == 0 && id >= 0) {
         fpair = o.fc[e];
+        if (o.extra) fextra = o.extra[id];
         pvx = o.vx[id];
         pvy = o.vy[id];
         pvz = o.vz[id];
@@ -510,9 +513,9 @@ __global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_gather(const
         if (id < 0) return;
         const float4 f = fpair;
         o.fc[e] = make_float4(0.f, 0.f, 0.f, 0.f);
-        Fx += f.x;
-        Fy += f.y;
-        Fz += f.z;
+        Fx += f.x + fextra.x;
+        Fy += f.y + fextra.y;
+        Fz += f.z + fextra.z;
         o.fx[id] = Fx;
         o.fy[id] = Fy;
         o.fz[id] = Fz;
@@ -948,7 +951,7 @@ static void launch_gather(pd_mesh *m, const float4 *xq, int nchunks, const int *
 int mesh_gather_join(pd_mesh *m, pd_cluster *c, const float4 *xq, const int *perm, const int *ns_dev, int nchunks,
                      float *fx, float *fy, float *fz, float *vx, float *vy, float *vz, const float *inv_mass,
                      float inv_mass_uniform, float half_dt, float *epot, float *vir6, float *vglobal6, const float *q,
-                     float half_c_self, int energy, cudaStream_t s) {
+                     float half_c_self, const float4 *extra, int energy, cudaStream_t s) {
     (void)q;
     PD_CHECK(m->p.kind != PD_MESH_P3M_IK, PD_ENOTSUP, "the fused gather step supports analytic differentiation only");
     GatherOut o;
@@ -971,6 +974,7 @@ int mesh_gather_join(pd_mesh *m, pd_cluster *c, const float4 *xq, const int *per
     o.nslot = c->nslot;
     o.half_c_self = half_c_self;
     o.bg = m->bg;
+    o.extra = extra;
     if (energy)
         launch_gather<2, true>(m, xq, nchunks, ns_dev, o, s);
     else

@@ -406,6 +406,13 @@ class DeviceEngine:
     def evaluate(self, energy=False, stream=None):
         N.call("pd_md_evaluate", self.handle, int(bool(energy)), _stream(stream))
 
+    def set_learned(self, correction=None, net=None):
+        """Attach the learned coarse-mesh correction (``learned.LearnedCorrection`` + ``learned.MLPNetwork``):
+        every force pass then adds s_i V_i before the closing kick.  None detaches it."""
+        N.call("pd_md_set_learned", self.handle, correction.handle if correction is not None else None,
+               net.handle if net is not None else None)
+        self._learned = (correction, net)
+
     def step(self, nsteps: int, dt: float, energy_last=False, use_graph=True, stream=None):
         N.call("pd_md_step", self.handle, int(nsteps), float(dt), int(bool(energy_last)), int(bool(use_graph)),
                _stream(stream))

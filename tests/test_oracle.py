@@ -1,5 +1,6 @@
 """The CPU oracle pinned on the reference's known answers (no GPU needed)."""
 import math
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -178,3 +179,49 @@ def test_setup_math(pd):
     assert s.resolve_mesh(None, 2.0, (119.5,) * 3, 4) == (60, 60, 60)
     t = s.lj_type_table(1.0, 1.0, 2 ** (1 / 6), wca=True)
     assert t[0, 3] == -1.0
+
+
+def _learned_oracle():
+    import importlib.util
+    import sys
+    name = "pdb200_learned_oracle"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(name, Path(__file__).resolve().parent.parent / "oracle" /
+                                                      "learned_oracle.py")
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
+def test_learned_oracle_gradients_against_finite_differences():
+    """Pins the network restatement: exact-arithmetic gradients vs central differences."""
+    lo = _learned_oracle()
+    rng = np.random.default_rng(5)
+    flat = rng.normal(0, 0.3, 4096 + 128 + 16384 + 128 + 128 + 1)
+    X = rng.normal(0, 1, (6, 32))
+    ab = np.abs(rng.normal(0, 1, (6, 2)))
+    scale = 0.37
+    loss, g = lo.residual_loss_grads(flat, X, ab, scale, bf16_points=False)
+    idx = np.concatenate([rng.choice(4096, 6, replace=False), 4096 + rng.choice(128, 3, replace=False),
+                          4224 + rng.choice(16384, 6, replace=False), 20608 + rng.choice(128, 3, replace=False),
+                          20736 + rng.choice(128, 3, replace=False), [20864]])
+    h = 1e-6
+    for k in idx:
+        p, m = flat.copy(), flat.copy()
+        p[k] += h
+        m[k] -= h
+        fd = (lo.residual_loss_grads(p, X, ab, scale, False)[0] - lo.residual_loss_grads(m, X, ab, scale, False)[0]) / (2 * h)
+        assert abs(fd - g[k]) <= 1e-6 * max(1.0, abs(fd)), (k, fd, g[k])
+
+
+def test_learned_oracle_bf16_and_adam():
+    lo = _learned_oracle()
+    # round to nearest, ties to even, on the 8-bit bfloat16 mantissa
+    a = np.array([1.0, 1.0 + 2.0 ** -8, 1.0 + 3 * 2.0 ** -8, 1.0 + 2.0 ** -9, -2.5, 3.0e-3], np.float32)
+    r = lo.bf16(a)
+    assert r[0] == 1.0 and r[1] == 1.0 and r[2] == 1.0 + 2 * 2.0 ** -7 and r[3] == 1.0 and r[4] == -2.5
+    assert abs(r[5] - 3.0e-3) <= 2.0 ** -8 * 3.0e-3
+    p, m, v = lo.adam(np.ones(3), np.array([1.0, -2.0, 0.0]), np.zeros(3), np.zeros(3), 1, lr=0.1)
+    # first step: m_hat = g, v_hat = g^2, so the step is lr * sign(g) (up to eps)
+    assert np.allclose(p, [0.9, 1.1, 1.0], atol=1e-7)
