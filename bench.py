@@ -164,7 +164,9 @@ def time_pairs_kernel(pd, st, reps=50):
         b.record(s)
     b.synchronize()
     ms = a.elapsed_time(b) / reps
-    # clear the accumulated slot forces (a kick-free evaluation restores the state)
+    # the timed passes accumulated into the slot forces: a first kick-free evaluation consumes (and clears)
+    # them, a second one restores the forces of the current positions
+    st.evaluate_forces_into_f(False)
     st.evaluate_forces_into_f(False)
     return ms
 
@@ -284,6 +286,105 @@ def profiled_traffic(name: str):
     return int(m.group(1)) if m else None
 
 
+def time_md_steps(st, dt, steps, warmup, flush, no_flush):
+    """Device time per captured NVE step (CUDA events on the step stream, L2 flushed between steps)."""
+    import torch
+    s = st.stream
+    st.step(warmup, use_graph=True)
+    st.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    torch.cuda.synchronize()
+    with torch.cuda.stream(s):
+        for k in range(steps):
+            if not no_flush:
+                flush.fill_(float(k))
+            starts[k].record(s)
+            st.engine.step(1, dt, energy_last=False, use_graph=True, stream=s)
+            ends[k].record(s)
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in zip(starts, ends)) / steps
+
+
+def run_learned_form(pd, args, st, system, dt, flush):
+    """The learned coarse-mesh form on the same melt.
+
+    Training data: ``args.snapshots`` snapshots of the running fine-mesh simulation ``st`` (one every
+    ``args.snapshot_stride`` steps), target = fine-mesh minus coarse-mesh (2.0 A, order 4) forces; the radial
+    weight is fitted by least squares, the network trained by Adam (fused tensor-core training kernel).  Held-out
+    snapshots later in the run give the relative RMS electrostatic force error of each form against the FP64
+    Ewald sum on the GPU.  Then the NVE step of coarse PME + correction (and of coarse PME alone) is timed like
+    the plain step."""
+    import torch
+    n, box = st.n, st.box
+    spec = st.solver.spec
+    st.evaluate_forces_into_f(False)
+    t0 = time.perf_counter()
+    tr = pd.learned.CoarseMeshTrainer(n, box, st.q, st.typ, spec, coarse_spacing=2.0, coarse_order=4, seed=SEED)
+    for _ in range(args.snapshots):
+        st.step(args.snapshot_stride, use_graph=True)
+        st.synchronize()
+        tr.add_snapshot(st.x, st.y, st.z)
+    torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    coef = tr.fit_radial()
+    tr.build_dataset()
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    losses = tr.train(epochs=args.epochs, lr=2e-3)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    # held-out snapshots: relative RMS electrostatic force error vs the FP64 Ewald sum
+    ones = pd.learned.MLPNetwork(pd.learned.init_params(0, s0=1.0, out_scale=0.0))
+    q = st.q.double()
+    errs = {"plain_fine": [], "coarse": [], "coarse_radial": [], "learned": []}
+    for _ in range(args.heldout):
+        st.step(100, use_graph=True)
+        st.synchronize()
+        x, y, z = st.x, st.y, st.z
+        rq = torch.stack([x.double(), y.double(), z.double(), q], 1).contiguous()
+        Fk, _ = pd.learned.ewald_oracle(rq, box, spec.C, spec.alpha, digits=10, parts=2)
+        Ft, _ = pd.learned.ewald_oracle(rq, box, spec.C, spec.alpha, digits=10, parts=3)
+        den = torch.sqrt((Ft ** 2).sum())
+        fine = tr.mesh_forces(tr.fine, x, y, z).double()
+        coarse = tr.mesh_forces(tr.coarse, x, y, z).double()
+        forms = {"plain_fine": fine, "coarse": coarse,
+                 "coarse_radial": coarse + tr.corr.correction(ones, x, y, z, tr.q, tr.typ)[:, :3].double(),
+                 "learned": coarse + tr.corr.correction(tr.net, x, y, z, tr.q, tr.typ)[:, :3].double()}
+        for k, f in forms.items():
+            errs[k].append(float(torch.sqrt(((f - Fk) ** 2).sum()) / den))
+    err = {k: float(np.mean(v)) for k, v in errs.items()}
+    # the timed learned step, from the current state of the fine-mesh run
+    el = pd.PME(coulomb_prefactor=pd.synthetic.COULOMB_EV_A, real_cutoff=RC, real_space_tolerance=1e-5,
+                mesh_spacing=2.0, order=4)
+    sys2 = pd.ParticleSystem(st.positions(), box, types=system.types, typeids=system.typeids, masses=system.masses,
+                             charges=system.charges, velocities=st.velocities())
+    forces2 = forces(pd, args.buffer, args.prune)[:1] + [el]
+    st2 = pd.Simulation(sys2, pd.Integrator(dt=dt, forces=forces2)).state
+    st2.evaluate_forces_into_f(False)
+    ms_coarse = time_md_steps(st2, dt, args.steps, args.warmup, flush, args.no_flush)
+    st2.engine.set_learned(tr.corr, tr.net)
+    st2.evaluate_forces_into_f(False)
+    ms_learned = time_md_steps(st2, dt, args.steps, args.warmup, flush, args.no_flush)
+    lst = tr.corr.status()
+    if tr.net.error() or lst["error"]:
+        raise RuntimeError(f"learned correction failed during the timed run (network {tr.net.error()}, rows {lst})")
+    return {"ms_per_step": ms_learned, "value": ns_per_day(ms_learned),
+            "coarse_only": {"ms_per_step": ms_coarse, "value": ns_per_day(ms_coarse)},
+            "force_error_vs_fp64_ewald": err,
+            "error_note": "relative RMS electrostatic force error (mesh part of each form against the FP64 "
+                          "reciprocal Ewald sum, over the RMS of the full Ewald force; the real-space part is "
+                          "common to all forms)",
+            "mesh": "coarse PME 2.0 A (60^3), order 4; fine 1.0 A (120^3), order 5",
+            "training": {"snapshots": args.snapshots, "stride_steps": args.snapshot_stride, "epochs": args.epochs,
+                         "mse_per_epoch": losses, "radial_coef": [float(c) for c in coef],
+                         "seconds": {"snapshots": t_gen, "dataset": t_data, "adam": t_train},
+                         "heldout_snapshots": args.heldout},
+            "descriptor_rows": {"builds": lst["builds"], "cap": lst["cap"]}}
+
+
 def run_reference(args, world, rank):
     """--impl reference: the CPU restatement on the host cores (rank 0 only)."""
     if rank != 0:
@@ -333,6 +434,11 @@ def main():
     ap.add_argument("--workload", default="melt64k", choices=["melt64k", "lj1m", "wca2d1m", "lj4k"],
                     help="melt64k: the headline run; lj4k / lj1m (3D LJ fluid, ELL route, NVE) and wca2d1m (2D WCA "
                          "disks, ELL route, Langevin) time the other configurations (not the headline metric)")
+    ap.add_argument("--snapshots", type=int, default=2000, help="training snapshots of the learned form")
+    ap.add_argument("--snapshot-stride", type=int, default=2, help="fine-mesh steps between training snapshots")
+    ap.add_argument("--epochs", type=int, default=4, help="Adam epochs of the learned form")
+    ap.add_argument("--heldout", type=int, default=4, help="held-out snapshots for the force errors")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned coarse-mesh form")
     ap.add_argument("--profile", action="store_true",
                     help="profiling run for ncu: the same workload, --warmup then --steps directly launched steps "
                          "(no graph, no timing, no baseline), so a launch list sees every kernel")
@@ -450,6 +556,20 @@ def main():
                 "pairs_within_rc": npairs, "flop_per_pair": flop_pair,
                 "peak_source": "nominal FP32 FMA rate at sm_max_mhz (MEASURED_PEAKS.json has no FP32 figure)"}
 
+    learned = None
+    if not args.no_learned:
+        learned = run_learned_form(pd, args, st, system, dt, flush)
+        learned["value"] = world * learned["value"]
+        learned["coarse_only"]["value"] = world * learned["coarse_only"]["value"]
+        learned["ms_per_step"] = max_over_ranks(world, learned["ms_per_step"])
+    # the headline is the learned form only where it reaches the plain form's force error
+    form = "plain: fine-mesh SPME (learned coarse-mesh form measured under forms.learned_coarse)"
+    if learned is not None:
+        e = learned["force_error_vs_fp64_ewald"]
+        if e["learned"] <= e["plain_fine"]:
+            value = learned["value"]
+            ms_step = learned["ms_per_step"]
+            form = "learned coarse-mesh: coarse SPME + network at or below the plain form's force error"
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         ora = ge.load_oracle()
@@ -462,11 +582,14 @@ def main():
                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded ionic melt, 1200 K start)",
                "config": {"workload": "ionic melt N=64000 (L=119.5 A) LJ+SPME r_c=9 A, 120^3 order 5, NVE dt=1 fs",
-                          "form": "plain (learned coarse-mesh form not built)", "parallelism": f"replicas x{world}",
+                          "form": form, "parallelism": f"replicas x{world}",
                           "list_buffer_A": args.buffer, "prune_buffer_A": args.prune,
                           "l2": "flushed (256 MiB write) before every timed step" if not args.no_flush else "warm",
                           "timed_builds": timed_builds, "timed_prunes": timed_prunes},
                "roofline": roofline, "cpu_baseline": cpu,
+               "forms": {"plain": {"value": world * ns_per_day(total_ms / args.steps), "unit": "ns/day",
+                                   "ms_per_step": total_ms / args.steps},
+                         "learned_coarse": learned},
                "e2e": {"value": world * ns_per_day(e2e_ms), "unit": "ns/day", "h2d_bytes_per_step": 24 * n,
                        "d2h_bytes_per_step": 24 * n, "ms_per_step": e2e_ms},
                "gpu_launches": gpu_launches,
