@@ -109,7 +109,7 @@ def adam(p, g, m, v, t, lr, beta1=0.9, beta2=0.999, eps=1e-8):
 def descriptors(pos, q, typ, box, *, rcut, mu0, dmu, sigma, nb, nu0, dnu, tau, coef=None):
     """Features (n, 32), V (n, 3) and the radial-term vectors Vb (nb, n, 3) by a direct pair loop.
 
-    Species 0 is type id 1, species 1 every other id; f_c(r) = (cos(pi r / rcut) + 1) / 2."""
+    Species 0 is type id 1, species 1 every other id; f_c(r) = (1 - r^2 / rcut^2)^2."""
     pos = np.asarray(pos, np.float64)
     q = np.asarray(q, np.float64)
     L = np.asarray(box, np.float64)
@@ -125,7 +125,7 @@ def descriptors(pos, q, typ, box, *, rcut, mu0, dmu, sigma, nb, nu0, dnu, tau, c
         sel = (r2 < rcut * rcut) & (r2 > 0)
         j = np.nonzero(sel)[0]
         r = np.sqrt(r2[j])
-        fc = 0.5 * (np.cos(np.pi * r / rcut) + 1.0)
+        fc = (1.0 - (r / rcut) ** 2) ** 2
         g = np.exp(-((r[:, None] - mu[None, :]) ** 2) / (2 * sigma * sigma))
         w = (q[j] * fc)[:, None] * g
         s1 = np.asarray(typ)[j] > 1

@@ -4,7 +4,7 @@
 // Model (rotation-equivariant by construction):
 //   features  x_i[16 s + k] = sum_{j in species s, r_ij < r_c} q_j g_k(r_ij) f_c(r_ij)
 //             g_k(r) = exp(-(r - mu_k)^2 / (2 sigma^2)), mu_k = mu0 + k dmu (k < 16),
-//             f_c(r) = (cos(pi r / r_c) + 1) / 2, two species: type id 1 and every other id
+//             f_c(r) = (1 - r^2 / r_c^2)^2, two species: type id 1 and every other id
 //             (1-based type ids; no type array: one species);
 //   scalar    s_i = MLP(x_i)  (32-128-128-1 SiLU, BF16 tensor cores, mlp.cu);
 //   residual  F_i = sum_j w_ij (r_i - r_j),  w_ij = s_i q_i q_j b(r_ij),
@@ -16,8 +16,8 @@
 //   environment-dependent scale s_i.
 //
 // Neighbour rows come from a device ELL list (ell.cu) of radius r_c + skin, rebuilt by its
-// own displacement decision; one thread per particle walks its row, keeps the 32 features
-// and V_i in registers and writes them once (no atomics).
+// own displacement decision; eight lanes per particle walk its row, keep partial features and
+// V_i in registers, reduce them by shuffles and write them once (no atomics).
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -32,14 +32,34 @@ namespace pdb {
 
 constexpr int DESC_THREADS = 256;
 constexpr int DESC_F = 16;   // Gaussians per species
+constexpr int DESC_LANES = 8; // lanes per particle
 
 struct DescParams {
     float Lx, Ly, Lz;
-    float rc2, inv_rc;
-    float mu0, dmu, inv2s2;
+    float rc2, inv_rc2;
+    float mu0, dmu, inv2s2, cmu;   // cmu = exp(-2 dmu^2 / (2 sigma^2)): ratio step of the feature run
     int nb;
-    float nu0, dnu, inv2t2;
+    float nu0, dnu, inv2t2, cnu;   // cnu: ratio step of the radial-term run
     float coef[PD_LEARNED_MAX_RADIAL];
+};
+
+// A run of equally spaced Gaussians g_k = exp(-a (r - c0 - k dc)^2) by products: g_{k+1} = g_k rho_k
+// with rho_k = exp(a dc (2 (r - c_k) - dc)) and rho_{k+1} = rho_k exp(-2 a dc^2) (two exponentials per
+// run).  Terms that underflow at the start of a run are below exp(-87) of their peak.
+struct GaussRun {
+    float g, rho, c;
+    __device__ __forceinline__ GaussRun(float r, float c0, float dc, float a, float step) {
+        const float d = r - c0;
+        g = __expf(-a * d * d);
+        rho = __expf(a * dc * (2.f * d - dc));
+        c = step;
+    }
+    __device__ __forceinline__ float next() {
+        const float v = g;
+        g *= rho;
+        rho *= c;
+        return v;
+    }
 };
 
 __device__ __forceinline__ float mic_d(float d, float L) {
@@ -49,18 +69,41 @@ __device__ __forceinline__ float mic_d(float d, float L) {
     return d;
 }
 
-// Features, V_i (or with BASIS the radial-term vectors V_i^(m), m < nb, at Vb[m n + i]).
-template <bool BASIS>
-__global__ void __launch_bounds__(DESC_THREADS) k_descriptors(const float *__restrict__ x, const float *__restrict__ y,
-                                                              const float *__restrict__ z, const float *__restrict__ q,
-                                                              const int *__restrict__ type, int n,
+// Packed neighbour record (x, y, z, q) with the species in the lowest mantissa bit of q (a change
+// of at most one ulp of the charge), so that a row entry costs one 16-byte gather.
+__global__ void k_desc_pack(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
+                            const float *__restrict__ q, const int *__restrict__ type, int n,
+                            float4 *__restrict__ xq) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int s1 = (type != nullptr && type[i] > 1) ? 1 : 0;
+    xq[i] = make_float4(x[i], y[i], z[i], __int_as_float((__float_as_int(q[i]) & ~1) | s1));
+}
+
+// Sum over the G consecutive lanes of a particle's group (butterfly: every lane gets the total).
+template <int G>
+__device__ __forceinline__ float group_sum(float v) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Features, V_i (or with BASIS the radial-term vectors V_i^(m), m < nb, at Vb[m n + i]).  G lanes per
+// particle stride its row (entries g, g + G, ...) and reduce their partial sums by shuffles; lane g < 4
+// of the group stores the g-th 16-byte chunk of the particle's BF16 features.
+template <bool BASIS, int G>
+__global__ void __launch_bounds__(DESC_THREADS, 4) k_descriptors(const float4 *__restrict__ xq, int n,
                                                               const int *__restrict__ rows,
                                                               const int *__restrict__ counts, int cap, DescParams p,
                                                               __nv_bfloat16 *__restrict__ X, float4 *__restrict__ V,
                                                               float4 *__restrict__ Vb) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float xi = x[i], yi = y[i], zi = z[i], qi = q[i];
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = tid / G, g = tid % G;
+    const bool live = i < n;   // whole groups are live or not (G divides the warp)
+    if (__all_sync(0xffffffffu, !live)) return;
+    const int ii = live ? i : 0;
+    const float4 pi = xq[ii];
+    const float xi = pi.x, yi = pi.y, zi = pi.z, qi = pi.w;
     float a0[DESC_F], a1[DESC_F];
 #pragma unroll
     for (int k = 0; k < DESC_F; ++k) a0[k] = a1[k] = 0.f;
@@ -68,34 +111,48 @@ __global__ void __launch_bounds__(DESC_THREADS) k_descriptors(const float *__res
     float bx[PD_LEARNED_MAX_RADIAL], by[PD_LEARNED_MAX_RADIAL], bz[PD_LEARNED_MAX_RADIAL];
 #pragma unroll
     for (int m = 0; m < PD_LEARNED_MAX_RADIAL; ++m) bx[m] = by[m] = bz[m] = 0.f;
-    const int cnt = min(counts[i], cap);
-    for (int t = 0; t < cnt; ++t) {
-        const int j = __ldg(rows + (size_t)t * n + i);
-        const float dx = mic_d(xi - __ldg(x + j), p.Lx);
-        const float dy = mic_d(yi - __ldg(y + j), p.Ly);
-        const float dz = mic_d(zi - __ldg(z + j), p.Lz);
+    const int cnt = live ? min(counts[ii], cap) : 0;
+    // one entry ahead: the row index and the neighbour record of the next entry are in flight
+    // while this one is evaluated
+    int jn = g < cnt ? __ldg(rows + (size_t)g * n + ii) : ii;
+    float4 pn = __ldg(xq + jn);
+    for (int t = g; t < cnt; t += G) {
+        const float4 pj = pn;
+        if (t + G < cnt) {
+            jn = __ldg(rows + (size_t)(t + G) * n + ii);
+            pn = __ldg(xq + jn);
+        }
+        const float dx = mic_d(xi - pj.x, p.Lx);
+        const float dy = mic_d(yi - pj.y, p.Ly);
+        const float dz = mic_d(zi - pj.z, p.Lz);
         const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
         if (!(r2 < p.rc2) || r2 == 0.f) continue;
-        const float r = sqrtf(r2);
-        const float fc = 0.5f * (cospif(r * p.inv_rc) + 1.f);
-        const float qj = __ldg(q + j);
-        const bool s1 = type != nullptr && __ldg(type + j) > 1;
+        const float r = r2 * rsqrtf(r2);
+        const float u2 = 1.f - r2 * p.inv_rc2;
+        const float fc = u2 * u2;
+        const float qj = pj.w;
+        const bool s1 = (__float_as_int(pj.w) & 1) != 0;
         const float wq = qj * fc;
         const float w0 = s1 ? 0.f : wq, w1 = s1 ? wq : 0.f;
+        {   // two runs of eight feature Gaussians, from centres 0 and 8
+            GaussRun lo(r, p.mu0, p.dmu, p.inv2s2, p.cmu);
+            GaussRun hi(r, fmaf(8.f, p.dmu, p.mu0), p.dmu, p.inv2s2, p.cmu);
 #pragma unroll
-        for (int k = 0; k < DESC_F; ++k) {
-            const float u = r - fmaf((float)k, p.dmu, p.mu0);
-            const float g = __expf(-u * u * p.inv2s2);
-            a0[k] = fmaf(g, w0, a0[k]);
-            a1[k] = fmaf(g, w1, a1[k]);
+            for (int k = 0; k < DESC_F / 2; ++k) {
+                const float el = lo.next(), eh = hi.next();
+                a0[k] = fmaf(el, w0, a0[k]);
+                a1[k] = fmaf(el, w1, a1[k]);
+                a0[k + DESC_F / 2] = fmaf(eh, w0, a0[k + DESC_F / 2]);
+                a1[k + DESC_F / 2] = fmaf(eh, w1, a1[k + DESC_F / 2]);
+            }
         }
         const float qq = qi * qj * fc;
+        GaussRun rad(r, p.nu0, p.dnu, p.inv2t2, p.cnu);
         if (BASIS) {
 #pragma unroll
             for (int m = 0; m < PD_LEARNED_MAX_RADIAL; ++m) {
                 if (m >= p.nb) break;
-                const float u = r - fmaf((float)m, p.dnu, p.nu0);
-                const float e = qq * __expf(-u * u * p.inv2t2);
+                const float e = qq * rad.next();
                 bx[m] = fmaf(e, dx, bx[m]);
                 by[m] = fmaf(e, dy, by[m]);
                 bz[m] = fmaf(e, dz, bz[m]);
@@ -105,8 +162,7 @@ __global__ void __launch_bounds__(DESC_THREADS) k_descriptors(const float *__res
 #pragma unroll
             for (int m = 0; m < PD_LEARNED_MAX_RADIAL; ++m) {
                 if (m >= p.nb) break;
-                const float u = r - fmaf((float)m, p.dnu, p.nu0);
-                b = fmaf(p.coef[m], __expf(-u * u * p.inv2t2), b);
+                b = fmaf(p.coef[m], rad.next(), b);
             }
             const float e = qq * b;
             vx = fmaf(e, dx, vx);
@@ -114,19 +170,39 @@ __global__ void __launch_bounds__(DESC_THREADS) k_descriptors(const float *__res
             vz = fmaf(e, dz, vz);
         }
     }
-    if (X) {
-        uint4 *dst = reinterpret_cast<uint4 *>(X + (size_t)i * 32);
+#pragma unroll
+    for (int k = 0; k < DESC_F; ++k) {
+        a0[k] = group_sum<G>(a0[k]);
+        a1[k] = group_sum<G>(a1[k]);
+    }
+    if (BASIS) {
+#pragma unroll
+        for (int m = 0; m < PD_LEARNED_MAX_RADIAL; ++m) {
+            if (m >= p.nb) break;   // p.nb is uniform: every lane takes the same shuffles
+            bx[m] = group_sum<G>(bx[m]);
+            by[m] = group_sum<G>(by[m]);
+            bz[m] = group_sum<G>(bz[m]);
+        }
+    } else {
+        vx = group_sum<G>(vx);
+        vy = group_sum<G>(vy);
+        vz = group_sum<G>(vz);
+    }
+    if (!live) return;
+    if (X && g < 4) {
+        __align__(16) __nv_bfloat16 h[8];
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            __align__(16) __nv_bfloat16 h[8];
+            if (c != g) continue;
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
                 const int f = 8 * c + k;
                 h[k] = __float2bfloat16_rn(f < DESC_F ? a0[f] : a1[f - DESC_F]);
             }
-            dst[c] = *reinterpret_cast<const uint4 *>(h);
         }
+        reinterpret_cast<uint4 *>(X + (size_t)i * 32)[g] = *reinterpret_cast<const uint4 *>(h);
     }
+    if (g != 0) return;
     if (BASIS) {
 #pragma unroll
         for (int m = 0; m < PD_LEARNED_MAX_RADIAL; ++m)
@@ -146,6 +222,7 @@ struct pd_learned {
     __nv_bfloat16 *X = nullptr;   // n x 32
     float4 *V = nullptr;          // n
     float4 *corr = nullptr;       // n: (s V, s)
+    float4 *xq = nullptr;         // n: packed (x, y, z, q | species bit)
 };
 
 namespace pdb {
@@ -157,14 +234,16 @@ static DescParams desc_params(const pd_learned *h) {
     d.Ly = (float)h->box[1];
     d.Lz = (float)h->box[2];
     d.rc2 = h->p.rcut * h->p.rcut;
-    d.inv_rc = 1.f / h->p.rcut;
+    d.inv_rc2 = 1.f / d.rc2;
     d.mu0 = h->p.mu0;
     d.dmu = h->p.dmu;
     d.inv2s2 = 0.5f / (h->p.sigma * h->p.sigma);
+    d.cmu = (float)exp(-2.0 * (double)d.inv2s2 * (double)d.dmu * (double)d.dmu);
     d.nb = h->p.nb;
     d.nu0 = h->p.nu0;
     d.dnu = h->p.dnu;
     d.inv2t2 = 0.5f / (h->p.tau * h->p.tau);
+    d.cnu = (float)exp(-2.0 * (double)d.inv2t2 * (double)d.dnu * (double)d.dnu);
     for (int m = 0; m < PD_LEARNED_MAX_RADIAL; ++m) d.coef[m] = h->p.coef[m];
     return d;
 }
@@ -177,11 +256,14 @@ static int descriptors_launch(pd_learned *h, const float *x, const float *y, con
     if ((rc = pd_ell_rows(h->ell, &rows, &counts))) return rc;
     const int cap = ell_capacity(h->ell);
     const DescParams d = desc_params(h);
-    const int blocks = (h->n + DESC_THREADS - 1) / DESC_THREADS;
+    k_desc_pack<<<(h->n + 255) / 256, 256, 0, s>>>(x, y, z, q, type, h->n, h->xq);
+    PD_LAUNCHED();
+    constexpr int G = DESC_LANES;
+    const int blocks = (int)(((long long)h->n * G + DESC_THREADS - 1) / DESC_THREADS);
     if (Vb)
-        k_descriptors<true><<<blocks, DESC_THREADS, 0, s>>>(x, y, z, q, type, h->n, rows, counts, cap, d, X, V, Vb);
+        k_descriptors<true, G><<<blocks, DESC_THREADS, 0, s>>>(h->xq, h->n, rows, counts, cap, d, X, V, Vb);
     else
-        k_descriptors<false><<<blocks, DESC_THREADS, 0, s>>>(x, y, z, q, type, h->n, rows, counts, cap, d, X, V, Vb);
+        k_descriptors<false, G><<<blocks, DESC_THREADS, 0, s>>>(h->xq, h->n, rows, counts, cap, d, X, V, Vb);
     PD_LAUNCHED();
     return PD_OK;
 }
@@ -202,6 +284,7 @@ static void learned_free(pd_learned *h) {
     dfree(h->X);
     dfree(h->V);
     dfree(h->corr);
+    dfree(h->xq);
 }
 
 }  // namespace pdb
@@ -236,7 +319,7 @@ int pd_learned_create(pd_learned **out, const pd_learned_params *p, int n, const
     ep.lanes = 1;
     int rc;
     if ((rc = pd_ell_create(&h->ell, &ep, box)) || (rc = dalloc(&h->X, (size_t)n * 32)) ||
-        (rc = dalloc(&h->V, (size_t)n)) || (rc = dalloc(&h->corr, (size_t)n))) {
+        (rc = dalloc(&h->V, (size_t)n)) || (rc = dalloc(&h->corr, (size_t)n)) || (rc = dalloc(&h->xq, (size_t)n))) {
         learned_free(h);
         delete h;
         return rc;

@@ -135,7 +135,8 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int k = 0; k < 32; ++k) v[k] = __uint_as_float(r[k]);
 }
 
-__device__ __forceinline__ float sigm(float z) { return 1.f / (1.f + expf(-z)); }
+// Logistic function with the fast exponential and division (relative error of a few ulp).
+__device__ __forceinline__ float sigm(float z) { return __fdividef(1.f, 1.f + __expf(-z)); }
 
 // Sums v[0..31] over the 32 lanes of the warp (recursive halving); lane l returns the total
 // of element l.
@@ -198,37 +199,51 @@ __device__ __forceinline__ void load_weights(unsigned char *sm, uint32_t ow1, ui
 // Shared-memory plan of the inference kernel (bytes).
 constexpr int FW_X = 0, FW_W1 = FW_X + MLP_TILE * MLP_IN * 2, FW_W2 = FW_W1 + MLP_H * MLP_IN * 2,
               FW_H1 = FW_W2 + MLP_H * MLP_H * 2, FW_BYTES = FW_H1 + MLP_TILE * MLP_H * 2;
+constexpr int FW_THREADS = 256;
 
 // Inference over one 128-row tile: s = w3 . silu(W2 h1 + b2) + b3 with h1 = bf16(silu(W1 x + b1)).
 // out_s[r] = s, and with V given corr[r] = (s V.x, s V.y, s V.z, s): the force residual s_i V_i
-// of the learned correction.
-__global__ void __launch_bounds__(MLP_THREADS) k_mlp_forward(const __nv_bfloat16 *__restrict__ X, int n,
-                                                            MlpWeights wt, float *__restrict__ out_s,
-                                                            const float4 *__restrict__ V,
-                                                            float4 *__restrict__ corr, int *__restrict__ err) {
+// of the learned correction.  Two warpgroups: warp w reads TMEM lanes 32 (w % 4) .. (its rows)
+// and the column half w / 4 of each accumulator; the two halves of s meet in shared memory.
+__global__ void __launch_bounds__(FW_THREADS) k_mlp_forward(const __nv_bfloat16 *__restrict__ X, int n,
+                                                           MlpWeights wt, float *__restrict__ out_s,
+                                                           const float4 *__restrict__ V,
+                                                           float4 *__restrict__ corr, int *__restrict__ err) {
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tmem_base;
     __shared__ float sb1[MLP_H], sb2[MLP_H], sw3[MLP_H];
-    const int t = threadIdx.x, w = t >> 5;
+    __shared__ float spart[MLP_TILE];
+    const int t = threadIdx.x, w = t >> 5, lane = t & 31;
     const int row0 = blockIdx.x * MLP_TILE;
+    const int rt = t & 127, half = t >> 7;   // load role: row rt, half of its chunks
     if (w == 0) tmem_alloc(smem_u32(&tmem_base), 128);
     if (t == 0) mbar_init(smem_u32(&bar), 1);
-    sb1[t] = __ldg(wt.b1 + t);
-    sb2[t] = __ldg(wt.b2 + t);
-    sw3[t] = __ldg(wt.w3 + t);
-    const int r = row0 + t;   // thread t: tile row t (= TMEM lane t)
+    if (t < MLP_H) {
+        sb1[t] = __ldg(wt.b1 + t);
+        sb2[t] = __ldg(wt.b2 + t);
+        sw3[t] = __ldg(wt.w3 + t);
+    }
     {
+        const int r = row0 + rt;
         const uint4 zero = make_uint4(0, 0, 0, 0);
 #pragma unroll
-        for (int c = 0; c < MLP_IN / 8; ++c)
-            *reinterpret_cast<uint4 *>(sm + FW_X + cm_off(t, 8 * c, MLP_IN)) =
+        for (int c = 2 * half; c < 2 * half + 2; ++c) {
+            *reinterpret_cast<uint4 *>(sm + FW_X + cm_off(rt, 8 * c, MLP_IN)) =
                 r < n ? __ldg(reinterpret_cast<const uint4 *>(X + (size_t)r * MLP_IN) + c) : zero;
-        load_weights(sm, FW_W1, FW_W2, wt, t);
+            *reinterpret_cast<uint4 *>(sm + FW_W1 + cm_off(rt, 8 * c, MLP_IN)) =
+                __ldg(reinterpret_cast<const uint4 *>(wt.w1 + (size_t)rt * MLP_IN) + c);
+        }
+#pragma unroll 4
+        for (int c = 8 * half; c < 8 * half + 8; ++c)
+            *reinterpret_cast<uint4 *>(sm + FW_W2 + cm_off(rt, 8 * c, MLP_H)) =
+                __ldg(reinterpret_cast<const uint4 *>(wt.w2 + (size_t)rt * MLP_H) + c);
     }
     tc_sync();
     const uint32_t tm = tmem_base, b = smem_u32(&bar), base = smem_u32(sm);
-    const uint32_t lane_addr = tm + ((uint32_t)(32 * w) << 16);
+    const int m = 32 * (w & 3) + lane;   // tile row (TMEM lane) of this thread in the epilogues
+    const int c_lo = 64 * (w >> 2);      // its column half
+    const uint32_t lane_addr = tm + ((uint32_t)(32 * (w & 3)) << 16);
     if (t == 0) {
         gemm_issue(tm, base + FW_X, base + FW_W1, MLP_IN, MLP_TILE, MLP_H, false);
         umma_commit(b);
@@ -237,7 +252,7 @@ __global__ void __launch_bounds__(MLP_THREADS) k_mlp_forward(const __nv_bfloat16
     if (ok) {
         tc_fence_after();
 #pragma unroll 1
-        for (int c0 = 0; c0 < MLP_H; c0 += 32) {
+        for (int c0 = c_lo; c0 < c_lo + 64; c0 += 32) {
             float v[32];
             tmem_ld32(lane_addr + c0, v);
 #pragma unroll
@@ -246,20 +261,21 @@ __global__ void __launch_bounds__(MLP_THREADS) k_mlp_forward(const __nv_bfloat16
                 v[k] = z * sigm(z);
             }
 #pragma unroll
-            for (int g = 0; g < 4; ++g) st8(sm + FW_H1, cm_off(t, c0 + 8 * g, MLP_H), v + 8 * g);
+            for (int g = 0; g < 4; ++g) st8(sm + FW_H1, cm_off(m, c0 + 8 * g, MLP_H), v + 8 * g);
         }
     }
+    ok = __syncthreads_and(ok);
     tc_sync();
     if (t == 0 && ok) {
         gemm_issue(tm, base + FW_H1, base + FW_W2, MLP_H, MLP_TILE, MLP_H, false);
         umma_commit(b);
     }
     ok = ok && mbar_wait(b, 1);
+    float acc = 0.f;
     if (ok) {
         tc_fence_after();
-        float acc = 0.f;
 #pragma unroll 1
-        for (int c0 = 0; c0 < MLP_H; c0 += 32) {
+        for (int c0 = c_lo; c0 < c_lo + 64; c0 += 32) {
             float v[32];
             tmem_ld32(lane_addr + c0, v);
 #pragma unroll
@@ -268,7 +284,12 @@ __global__ void __launch_bounds__(MLP_THREADS) k_mlp_forward(const __nv_bfloat16
                 acc = fmaf(z * sigm(z), sw3[c0 + k], acc);
             }
         }
-        const float s = acc + __ldg(wt.b3);
+    }
+    if (w >= 4) spart[m] = acc;
+    ok = __syncthreads_and(ok);
+    if (ok && w < 4) {
+        const float s = acc + spart[m] + __ldg(wt.b3);
+        const int r = row0 + m;
         if (r < n) {
             if (out_s) out_s[r] = s;
             if (corr) {
@@ -276,9 +297,8 @@ __global__ void __launch_bounds__(MLP_THREADS) k_mlp_forward(const __nv_bfloat16
                 corr[r] = make_float4(s * vv.x, s * vv.y, s * vv.z, s);
             }
         }
-    } else if (t == 0) {
-        atomicExch(err, 1);
     }
+    if (!ok && t == 0) atomicExch(err, 1);
     tc_fence_before();
     __syncthreads();
     if (w == 0) tmem_dealloc(tm, 128);
@@ -601,7 +621,7 @@ int mlp_forward_launch(const pd_mlp *q, const void *X, int n, float *s, const fl
                        cudaStream_t st) {
     if (n <= 0) return PD_OK;
     const int tiles = (n + MLP_TILE - 1) / MLP_TILE;
-    k_mlp_forward<<<tiles, MLP_THREADS, FW_BYTES, st>>>(static_cast<const __nv_bfloat16 *>(X), n, mlp_weights(q), s, V,
+    k_mlp_forward<<<tiles, FW_THREADS, FW_BYTES, st>>>(static_cast<const __nv_bfloat16 *>(X), n, mlp_weights(q), s, V,
                                                          corr, q->err);
     PD_LAUNCHED();
     return PD_OK;

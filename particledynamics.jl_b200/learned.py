@@ -5,7 +5,7 @@ fine-mesh PME of the same system.  PME runs on a mesh twice as coarse (2.0 A, or
 1.0 A, order 5) and the force residual of the coarse mesh is predicted per particle:
 
 * descriptors ``x_i`` (32 features): 2 species x 16 Gaussian radial bases of neighbour charge
-  within ``rcut`` (6 A), with a cosine cutoff;
+  within ``rcut`` (6 A), with the smooth cutoff ``(1 - r^2 / rcut^2)^2``;
 * a scalar ``s_i`` from a 32-128-128-1 SiLU network (BF16 weights and activations, FP32
   accumulation, tcgen05 tensor cores);
 * the residual ``F_i = s_i V_i`` with ``V_i = sum_j q_i q_j b(r_ij) (r_i - r_j)``: the network's
