@@ -385,6 +385,32 @@ def run_learned_form(pd, args, st, system, dt, flush):
             "descriptor_rows": {"builds": lst["builds"], "cap": lst["cap"]}}
 
 
+def profile_learned(pd, args, system, box, dt):
+    """Profiling run of the learned form (no timing): coarse PME (2.0 A, order 4) with the correction attached,
+    --warmup then --steps directly launched steps, each followed by one fused training batch and an Adam step
+    over that step's descriptors, so that a launch list or a capture sees every learned-form kernel."""
+    import torch
+    el = pd.PME(coulomb_prefactor=pd.synthetic.COULOMB_EV_A, real_cutoff=RC, real_space_tolerance=1e-5,
+                mesh_spacing=2.0, order=4)
+    st = pd.Simulation(system, pd.Integrator(dt=dt, forces=forces(pd, args.buffer, args.prune)[:1] + [el])).state
+    lc = pd.learned.LearnedCorrection(st.n, box)
+    lc.set_radial(np.linspace(0.01, -0.02, lc.nb))
+    net = pd.learned.MLPNetwork(pd.learned.init_params(SEED, s0=1.0, out_scale=0.1))
+    st.engine.set_learned(lc, net)
+    st.evaluate_forces_into_f(False)
+    ab = torch.stack([torch.rand(st.n, device="cuda"), torch.randn(st.n, device="cuda")], 1).contiguous()
+    X = torch.empty((st.n, 32), dtype=torch.bfloat16, device="cuda")
+    for k in range(args.warmup + args.steps):
+        st.step(1, use_graph=False)
+        st.synchronize()
+        lc.descriptors(st.x, st.y, st.z, st.q, st.typ, X=X)
+        net.train_batch(X, ab, 2.0 / (3 * st.n))
+        net.adam(1e-4)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile": "melt64k learned-form eager steps + training batches", "steps": args.steps,
+                      "warmup": args.warmup, "rows": lc.status(), "network_error": net.error()}))
+
+
 def run_reference(args, world, rank):
     """--impl reference: the CPU restatement on the host cores (rank 0 only)."""
     if rank != 0:
@@ -439,6 +465,8 @@ def main():
     ap.add_argument("--epochs", type=int, default=4, help="Adam epochs of the learned form")
     ap.add_argument("--heldout", type=int, default=4, help="held-out snapshots for the force errors")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned coarse-mesh form")
+    ap.add_argument("--form", default="plain", choices=["plain", "learned"],
+                    help="with --profile: profile the plain step or the learned coarse-mesh step")
     ap.add_argument("--profile", action="store_true",
                     help="profiling run for ncu: the same workload, --warmup then --steps directly launched steps "
                          "(no graph, no timing, no baseline), so a launch list sees every kernel")
@@ -469,6 +497,9 @@ def main():
     st = sim.state
     s = st.stream
     pd.evaluate_forces_into_f(sim, energy=False)
+    if args.profile and args.form == "learned":
+        profile_learned(pd, args, system, box, dt)
+        return
     if args.profile:
         st.step(args.warmup, use_graph=False)
         st.synchronize()

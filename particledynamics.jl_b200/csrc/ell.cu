@@ -396,6 +396,121 @@ __global__ void __launch_bounds__(ELL_THREADS) k_ell_rows(
     }
 }
 
+// Row construction, cell-staged: one warp per cell.  The warp walks the same stencil segments
+// in the same order as k_ell_rows (z, then y offsets; x cells in range order; each cell's
+// particles in id order), stages the candidates (x, y, z, id) in shared memory once for the
+// whole cell, and every lane (a particle of the cell) scans them with the same arithmetic as
+// k_ell_rows, so the rows are identical entry by entry.  Chunks of ROWS_CAP candidates are
+// scanned in turn when the stencil holds more.
+constexpr int ROWS_WARPS = 4, ROWS_CAP = 640;   // 40 KB of staging per block (below the 48 KB default)
+constexpr int ROWS_MIN_PER_CELL = 8;            // mean cell occupancy from which the cell-staged kernel is used
+
+template <int D>
+__global__ void __launch_bounds__(32 * ROWS_WARPS) k_ell_rows_cells(
+    const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z, int n,
+    const int *__restrict__ sorted, const int *__restrict__ cell_off, float Lx, float Ly, float Lz, int nx, int ny,
+    int nz, float rl2, int cap, int *__restrict__ rows, int *__restrict__ counts, float4 *__restrict__ ref,
+    long long *__restrict__ st) {
+    if (!ell_requested(st)) return;
+    extern __shared__ float4 ell_stage[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ncell = nx * ny * nz;
+    const int c = blockIdx.x * ROWS_WARPS + w;
+    float4 *sw = ell_stage + w * ROWS_CAP;
+    unsigned fmax = 0;
+    if (c < ncell) {   // warp-uniform
+        const float hLx = 0.5f * Lx, hLy = 0.5f * Ly, hLz = 0.5f * Lz;
+        const float rl = sqrtf(rl2);
+        const float hx = Lx / (float)nx, hy = Ly / (float)ny, hz = Lz / (float)nz;
+        const int Sx = ell_reach(rl, Lx, nx), Sy = ell_reach(rl, Ly, ny);
+        const int Sz = D == 3 ? ell_reach(rl, Lz, nz) : 0;
+        const int cx = c % nx, tmp = c / nx, cy = tmp % ny, cz = tmp / ny;
+        const int p0 = cell_off[c], pn = cell_off[c + 1] - p0;
+        for (int pg = 0; pg < pn; pg += 32) {
+            const bool has = pg + lane < pn;
+            const int i = has ? sorted[p0 + pg + lane] : -1;
+            const float xi = has ? x[i] : 0.f, yi = has ? y[i] : 0.f, zi = (has && D == 3) ? z[i] : 0.f;
+            int found = 0;
+            int fill = 0;
+            auto scan = [&]() {
+                __syncwarp();
+                if (has) {
+                    for (int t = 0; t < fill; ++t) {
+                        const float4 cj = sw[t];
+                        const int j = __float_as_int(cj.w);
+                        if (j == i) continue;
+                        const float dx = mic_fast(cj.x - xi, hLx, Lx);
+                        const float dy = mic_fast(cj.y - yi, hLy, Ly);
+                        float r2;
+                        if (D == 3) {
+                            const float dz = mic_fast(cj.z - zi, hLz, Lz);
+                            r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        } else {
+                            r2 = fmaf(dx, dx, dy * dy);
+                        }
+                        if (r2 <= rl2) {
+                            if (found < cap) rows[(size_t)found * n + i] = j;
+                            ++found;
+                        }
+                    }
+                }
+                __syncwarp();
+                fill = 0;
+            };
+            auto stage = [&](int ka, int kb) {
+                for (int k0 = ka; k0 < kb; k0 += 32) {
+                    const int cnt = min(32, kb - k0);
+                    if (fill + cnt > ROWS_CAP) scan();
+                    if (lane < cnt) {
+                        const int j = sorted[k0 + lane];
+                        sw[fill + lane] = make_float4(x[j], y[j], D == 3 ? z[j] : 0.f, __int_as_float(j));
+                    }
+                    fill += cnt;
+                }
+            };
+            for (int oz = -Sz; oz <= Sz; ++oz) {
+                int cz2 = cz + oz;
+                cz2 -= cz2 >= nz ? nz : 0;
+                cz2 += cz2 < 0 ? nz : 0;
+                const float gz = (float)max(abs(oz) - 1, 0) * hz;
+                for (int oy = -Sy; oy <= Sy; ++oy) {
+                    int cy2 = cy + oy;
+                    cy2 -= cy2 >= ny ? ny : 0;
+                    cy2 += cy2 < 0 ? ny : 0;
+                    const float gy = (float)max(abs(oy) - 1, 0) * hy;
+                    const float g2 = fmaf(gy, gy, gz * gz);
+                    if (g2 > rl2) continue;
+                    const int row = (cz2 * ny + cy2) * nx;
+                    int a1, b1, a2, b2;
+                    ell_row_ranges(cx, g2, rl2, hx, Sx, nx, a1, b1, a2, b2);
+                    stage(cell_off[row + a1], cell_off[row + b1 + 1]);
+                    if (a2 <= b2) stage(cell_off[row + a2], cell_off[row + b2 + 1]);
+                }
+            }
+            scan();
+            if (has) {
+                counts[i] = found;
+                ref[i] = make_float4(xi, yi, zi, 0.f);
+            }
+            fmax = max(fmax, (unsigned)found);
+        }
+    }
+    if (ell_block_max_last(fmax, st, E_RMAX, E_TICKET_R)) {
+        const long long largest = st[E_RMAX];
+        st[E_RMAX] = 0;
+        st[E_TICKET_R] = 0;
+        st[E_REQUIRED] = largest;
+        if (largest > cap) {
+            st[E_ERROR] = E_ERR_CAPACITY;
+            st[E_VALID] = 0;
+        } else {
+            st[E_VALID] = 1;
+            st[E_LAST_BUILD] = st[E_STEP];
+            st[E_BUILDS] += 1;
+        }
+    }
+}
+
 // Packed coordinates (x, y, z, 0) for the pair kernel's 16-byte neighbour loads.
 template <int D>
 __global__ void k_ell_pack(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
@@ -585,14 +700,24 @@ int ell_rebuild_launch(pd_ell *e, const float *x, const float *y, const float *z
     k_ell_rows<DD, AP><<<blocks, ELL_THREADS, 0, s>>>(x, y, z, n, e->sorted, e->cell_of, e->cell_off, Lx, Ly, Lz,    \
                                                       e->nx, e->ny, e->nz, e->rl2, e->cap, e->rows, e->counts, e->ref, \
                                                       e->st)
+#define PD_ELL_ROWS_CELLS(DD)                                                                                         \
+    k_ell_rows_cells<DD><<<(e->ncell + ROWS_WARPS - 1) / ROWS_WARPS, 32 * ROWS_WARPS,                                \
+                           sizeof(float4) * ROWS_WARPS * ROWS_CAP, s>>>(x, y, z, n, e->sorted, e->cell_off, Lx, Ly,  \
+                                                                        Lz, e->nx, e->ny, e->nz, e->rl2, e->cap,     \
+                                                                        e->rows, e->counts, e->ref, e->st)
+    // a warp per cell pays off once cells hold enough particles to occupy its lanes
+    const bool cells = !e->allpairs && n >= ROWS_MIN_PER_CELL * e->ncell;
     if (e->dim == 3) {
         if (e->allpairs) PD_ELL_ROWS(3, true);
+        else if (cells) PD_ELL_ROWS_CELLS(3);
         else PD_ELL_ROWS(3, false);
     } else {
         if (e->allpairs) PD_ELL_ROWS(2, true);
+        else if (cells) PD_ELL_ROWS_CELLS(2);
         else PD_ELL_ROWS(2, false);
     }
 #undef PD_ELL_ROWS
+#undef PD_ELL_ROWS_CELLS
     PD_LAUNCHED();
     return PD_OK;
 }
