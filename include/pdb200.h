@@ -410,6 +410,41 @@ int pd_learned_resize(pd_learned *h, int cap);
  * third stream beside the pair pass and the mesh). */
 int pd_md_set_learned(pd_md *md, pd_learned *h, pd_mlp *net);
 
+/* ------------------------------------------------------------------------------------------
+ * Batched replicas (no reference counterpart: the reference steps one system per engine).
+ * Hundreds of independent 3D LJ / WCA systems of uneven size, each with its own cubic or
+ * orthorhombic box and pair model, concatenated (replica r owns the particles after those of
+ * replicas 0..r-1) and stepped together: one launch per stage over all replicas, the NVE step
+ * captured into one CUDA graph.  Rows follow the ELL route (radius max r_c + skin, one rebuild
+ * decision for the whole batch).
+ * ------------------------------------------------------------------------------------------ */
+typedef struct pd_batch pd_batch;
+typedef struct {
+    double box[3];          /* each length above twice the list radius */
+    int n;                  /* particles */
+    int kind;               /* PD_PAIR_LJ or PD_PAIR_WCA (UniformLJ / UniformWCA, PairModels.jl:13-49) */
+    float eps, sigma, rc2;  /* rc2: squared cutoff (WCA: 1.2599211 sigma^2) */
+    float eshift;           /* LJ energy shift at the cutoff (0 unshifted); WCA adds eps */
+} pd_batch_replica;
+
+int pd_batch_create(pd_batch **out, const pd_batch_replica *reps, int nrep, float skin, int cap, int lanes);
+int pd_batch_destroy(pd_batch *b);
+int pd_batch_count(pd_batch *b, int *n, int *ncell);
+/* Lanes per row of the pair kernel (1, 2, 4, 8), the autotuner's choice. */
+int pd_batch_set_lanes(pd_batch *b, int lanes);
+/* Displacement decision and the flag-gated rebuild at centred coordinates (all replicas). */
+int pd_batch_update(pd_batch *b, const float *x, const float *y, const float *z, pd_stream_t st);
+/* Forces (stored) and, with energy, the per-particle energy (half of each pair). */
+int pd_batch_forces(pd_batch *b, const float *x, const float *y, const float *z, float *fx, float *fy, float *fz,
+                    float *epot, int energy, pd_stream_t st);
+int pd_batch_status(pd_batch *b, pd_ell_stats *out);
+int pd_batch_rows(pd_batch *b, int **rows, int **counts);
+/* Step state (x, v, f, per-particle inverse masses, optional epot) of all replicas, concatenated. */
+int pd_batch_bind(pd_batch *b, const pd_md_state *st);
+int pd_batch_evaluate(pd_batch *b, int energy, pd_stream_t st);
+/* nsteps velocity-Verlet NVE steps: drift (+ decision), IF rebuild, pairs (+ closing half kick). */
+int pd_batch_step(pd_batch *b, int nsteps, float dt, int use_graph, pd_stream_t st);
+
 /* FP64 Ewald sum on the GPU (ewald_reference, test/ewald_reference.jl:50-127, restated): rq4 =
  * n x (x, y, z, q) doubles on the device; real space over minimum images within x / alpha
  * (must be below half the smallest box length), reciprocal space within |k| < 2 alpha x,

@@ -18,7 +18,7 @@ LIB = HERE / "libpdb200.so"
 ROOT = HERE.parent
 
 SOURCES = ["cluster_list.cu", "cluster_pairs.cu", "mesh.cu", "md.cu", "noalloc.cu", "ell.cu", "mlp.cu", "learned.cu",
-           "ewald.cu"]
+           "ewald.cu", "batch.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

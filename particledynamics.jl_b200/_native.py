@@ -92,6 +92,13 @@ class EllStats(C.Structure):
     ]
 
 
+class BatchReplica(C.Structure):
+    _fields_ = [
+        ("box", C.c_double * 3), ("n", C.c_int), ("kind", C.c_int),
+        ("eps", C.c_float), ("sigma", C.c_float), ("rc2", C.c_float), ("eshift", C.c_float),
+    ]
+
+
 class LearnedParams(C.Structure):
     _fields_ = [
         ("rcut", C.c_float), ("skin", C.c_float), ("cap", C.c_int),
@@ -174,6 +181,17 @@ _SIGS = {
     "pd_learned_status": (C.c_int, [_p, C.POINTER(EllStats)]),
     "pd_learned_resize": (C.c_int, [_p, C.c_int]),
     "pd_md_set_learned": (C.c_int, [_p, _p, _p]),
+    "pd_batch_create": (C.c_int, [C.POINTER(_p), C.POINTER(BatchReplica), C.c_int, C.c_float, C.c_int, C.c_int]),
+    "pd_batch_destroy": (C.c_int, [_p]),
+    "pd_batch_count": (C.c_int, [_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "pd_batch_set_lanes": (C.c_int, [_p, C.c_int]),
+    "pd_batch_update": (C.c_int, [_p, _fp, _fp, _fp, _p]),
+    "pd_batch_forces": (C.c_int, [_p, _fp, _fp, _fp, _fp, _fp, _fp, _fp, C.c_int, _p]),
+    "pd_batch_status": (C.c_int, [_p, C.POINTER(EllStats)]),
+    "pd_batch_rows": (C.c_int, [_p, C.POINTER(_p), C.POINTER(_p)]),
+    "pd_batch_bind": (C.c_int, [_p, C.POINTER(MDState)]),
+    "pd_batch_evaluate": (C.c_int, [_p, C.c_int, _p]),
+    "pd_batch_step": (C.c_int, [_p, C.c_int, C.c_float, C.c_int, _p]),
     "pd_ewald_oracle": (C.c_int, [C.c_int, _fp, C.POINTER(C.c_double), C.c_double, C.c_double, C.c_double, C.c_int,
                                   _fp, C.POINTER(C.c_double)]),
 }

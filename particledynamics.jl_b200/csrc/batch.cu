@@ -1,0 +1,643 @@
+// Batched replicas of libpdb200: hundreds of independent LJ / WCA systems of uneven size (their
+// own box, density and pair model) stepped together, one launch per stage over all replicas,
+// the whole velocity-Verlet step captured into one CUDA graph.
+//
+// The replicas' particles are concatenated (replica r owns [first_r, first_r + N_r)); every
+// replica has its own cell grid, and the grids are concatenated too (global cell = cell_base_r +
+// local cell), so the counting sort of the ELL route (scan, scatter, id order per cell) serves
+// all replicas in one pass.  Per-replica geometry and pair model sit in a small device table
+// read through the read-only cache.  Stages per step:
+//   1. k_batch_drift: half kick, drift, centred wrap in the replica's box, displacement maximum
+//      since the last build; the last block decides the rebuild for all replicas at once and
+//      sets the graph's IF condition;
+//   2. the rebuild (IF node): k_batch_bin, the shared counting sort, k_batch_rows (one warp per
+//      cell, the replica's stencil staged in shared memory, rows identical to the single-system
+//      kernels'), the capacity commit by the last block;
+//   3. k_batch_pairs<G>: G lanes per row (G chosen by the caller's autotuner), the replica's LJ or
+//      WCA model, the closing half kick fused, the device step advanced.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "ell_common.cuh"
+#include "internal.hpp"
+
+using namespace pdb;
+
+namespace pdb {
+
+constexpr int B_THREADS = 256;
+constexpr int BROWS_WARPS = 4, BROWS_CAP = 640;
+
+struct BatchRep {
+    float L[3];
+    int nx, ny, nz, cell_base;
+    int kind;
+    float eps, sig2, rc2, eshift;
+};
+
+__device__ __forceinline__ float wrap_centred(float x, float L) {
+    x -= (x >= 0.5f * L) ? L : 0.f;
+    x += (x < -0.5f * L) ? L : 0.f;
+    return x;
+}
+
+// Half kick, drift, wrap and displacement (DRIFT), or the displacement of the current coordinates
+// alone; the last block decides for all replicas.
+template <bool DRIFT, bool COND>
+__global__ void __launch_bounds__(B_THREADS) k_batch_drift(int n, float *__restrict__ x, float *__restrict__ y,
+                                                           float *__restrict__ z, float *__restrict__ vx,
+                                                           float *__restrict__ vy, float *__restrict__ vz,
+                                                           const float *__restrict__ fx, const float *__restrict__ fy,
+                                                           const float *__restrict__ fz,
+                                                           const float *__restrict__ inv_mass, float dt,
+                                                           const int *__restrict__ rep_of,
+                                                           const BatchRep *__restrict__ reps,
+                                                           const float4 *__restrict__ ref, float threshold,
+                                                           long long *__restrict__ st, cudaGraphConditionalHandle h) {
+    if (st[E_ERROR] != 0) {
+        if (COND && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h, 0u);
+        return;
+    }
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float v = 0.f;
+    if (i < n) {
+        const BatchRep &R = reps[__ldg(rep_of + i)];
+        const float L[3] = {R.L[0], R.L[1], R.L[2]};
+        float p[3] = {x[i], y[i], z[i]};
+        if (DRIFT) {
+            const float c = 0.5f * dt * inv_mass[i];
+            const float u[3] = {fmaf(c, fx[i], vx[i]), fmaf(c, fy[i], vy[i]), fmaf(c, fz[i], vz[i])};
+            vx[i] = u[0];
+            vy[i] = u[1];
+            vz[i] = u[2];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) p[d] = wrap_centred(fmaf(dt, u[d], p[d]), L[d]);
+            x[i] = p[0];
+            y[i] = p[1];
+            z[i] = p[2];
+        }
+        v = ell_displacement<3>(p, ref[i], L, st[E_VALID] != 0);
+    }
+    if (ell_block_max_last(__float_as_uint(v), st, E_DMAX, E_TICKET_D)) {
+        const float largest = __uint_as_float((unsigned)st[E_DMAX]);
+        st[E_DMAX] = 0;
+        st[E_TICKET_D] = 0;
+        ell_decide<COND>(st, largest, threshold, h);
+    }
+}
+
+// Global cell of every particle (its replica's grid) and the cell histogram.
+__global__ void k_batch_bin(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
+                            int n, const int *__restrict__ rep_of, const BatchRep *__restrict__ reps,
+                            int *__restrict__ cell_of, int *__restrict__ cell_count, const long long *__restrict__ st) {
+    if (!ell_requested(st)) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const BatchRep &R = reps[__ldg(rep_of + i)];
+    const float p[3] = {x[i], y[i], z[i]};
+    const int ng[3] = {R.nx, R.ny, R.nz};
+    int cc[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        float u = p[d] + 0.5f * R.L[d];
+        u -= floorf(u / R.L[d]) * R.L[d];
+        cc[d] = min(max((int)floorf(u * ((float)ng[d] / R.L[d])), 0), ng[d] - 1);
+    }
+    const int c = R.cell_base + (cc[2] * R.ny + cc[1]) * R.nx + cc[0];
+    cell_of[i] = c;
+    atomicAdd(&cell_count[c], 1);
+}
+
+// Rows, one warp per global cell: the replica's stencil (same visiting order as the single-system
+// row kernels) staged in shared memory, each lane a particle of the cell.
+__global__ void __launch_bounds__(32 * BROWS_WARPS) k_batch_rows(
+    const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z, int n, int ncell,
+    const int *__restrict__ cell_rep, const BatchRep *__restrict__ reps, const int *__restrict__ sorted,
+    const int *__restrict__ cell_off, float rl2, int cap, int *__restrict__ rows, int *__restrict__ counts,
+    float4 *__restrict__ ref, long long *__restrict__ st) {
+    if (!ell_requested(st)) return;
+    extern __shared__ float4 batch_stage[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = blockIdx.x * BROWS_WARPS + w;
+    float4 *sw = batch_stage + w * BROWS_CAP;
+    unsigned fmax = 0;
+    if (c < ncell) {   // warp-uniform
+        const BatchRep &R = reps[__ldg(cell_rep + c)];
+        const float Lx = R.L[0], Ly = R.L[1], Lz = R.L[2];
+        const int nx = R.nx, ny = R.ny, nz = R.nz, base = R.cell_base;
+        const float hLx = 0.5f * Lx, hLy = 0.5f * Ly, hLz = 0.5f * Lz;
+        const float rl = sqrtf(rl2);
+        const float hx = Lx / (float)nx, hy = Ly / (float)ny, hz = Lz / (float)nz;
+        const int Sx = ell_reach(rl, Lx, nx), Sy = ell_reach(rl, Ly, ny), Sz = ell_reach(rl, Lz, nz);
+        const int lc = c - base;
+        const int cx = lc % nx, tmp = lc / nx, cy = tmp % ny, cz = tmp / ny;
+        const int p0 = cell_off[c], pn = cell_off[c + 1] - p0;
+        for (int pg = 0; pg < pn; pg += 32) {
+            const bool has = pg + lane < pn;
+            const int i = has ? sorted[p0 + pg + lane] : -1;
+            const float xi = has ? x[i] : 0.f, yi = has ? y[i] : 0.f, zi = has ? z[i] : 0.f;
+            int found = 0;
+            int fill = 0;
+            auto scan = [&]() {
+                __syncwarp();
+                if (has) {
+                    for (int t = 0; t < fill; ++t) {
+                        const float4 cj = sw[t];
+                        const int j = __float_as_int(cj.w);
+                        if (j == i) continue;
+                        const float dx = mic_fast(cj.x - xi, hLx, Lx);
+                        const float dy = mic_fast(cj.y - yi, hLy, Ly);
+                        const float dz = mic_fast(cj.z - zi, hLz, Lz);
+                        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        if (r2 <= rl2) {
+                            if (found < cap) rows[(size_t)found * n + i] = j;
+                            ++found;
+                        }
+                    }
+                }
+                __syncwarp();
+                fill = 0;
+            };
+            auto stage = [&](int ka, int kb) {
+                for (int k0 = ka; k0 < kb; k0 += 32) {
+                    const int cnt = min(32, kb - k0);
+                    if (fill + cnt > BROWS_CAP) scan();
+                    if (lane < cnt) {
+                        const int j = sorted[k0 + lane];
+                        sw[fill + lane] = make_float4(x[j], y[j], z[j], __int_as_float(j));
+                    }
+                    fill += cnt;
+                }
+            };
+            for (int oz = -Sz; oz <= Sz; ++oz) {
+                int cz2 = cz + oz;
+                cz2 -= cz2 >= nz ? nz : 0;
+                cz2 += cz2 < 0 ? nz : 0;
+                const float gz = (float)max(abs(oz) - 1, 0) * hz;
+                for (int oy = -Sy; oy <= Sy; ++oy) {
+                    int cy2 = cy + oy;
+                    cy2 -= cy2 >= ny ? ny : 0;
+                    cy2 += cy2 < 0 ? ny : 0;
+                    const float gy = (float)max(abs(oy) - 1, 0) * hy;
+                    const float g2 = fmaf(gy, gy, gz * gz);
+                    if (g2 > rl2) continue;
+                    const int row = base + (cz2 * ny + cy2) * nx;
+                    int a1, b1, a2, b2;
+                    ell_row_ranges(cx, g2, rl2, hx, Sx, nx, a1, b1, a2, b2);
+                    stage(cell_off[row + a1], cell_off[row + b1 + 1]);
+                    if (a2 <= b2) stage(cell_off[row + a2], cell_off[row + b2 + 1]);
+                }
+            }
+            scan();
+            if (has) {
+                counts[i] = found;
+                ref[i] = make_float4(xi, yi, zi, 0.f);
+            }
+            fmax = max(fmax, (unsigned)found);
+        }
+    }
+    if (ell_block_max_last(fmax, st, E_RMAX, E_TICKET_R)) {
+        const long long largest = st[E_RMAX];
+        st[E_RMAX] = 0;
+        st[E_TICKET_R] = 0;
+        st[E_REQUIRED] = largest;
+        if (largest > cap) {
+            st[E_ERROR] = E_ERR_CAPACITY;
+            st[E_VALID] = 0;
+        } else {
+            st[E_VALID] = 1;
+            st[E_LAST_BUILD] = st[E_STEP];
+            st[E_BUILDS] += 1;
+        }
+    }
+}
+
+__global__ void k_batch_pack(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
+                             int n, float4 *__restrict__ xq) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) xq[i] = make_float4(x[i], y[i], z[i], 0.f);
+}
+
+struct BatchKick {
+    float *vx, *vy, *vz;
+    const float *inv_mass;
+    float half_dt;
+    int on;
+};
+
+// Row pair kernel over all replicas: the model of particle i's replica (LJ or WCA, the ELL route's
+// UniformLJ / UniformWCA arithmetic), forces stored, optional energy (half of each pair), the
+// closing half kick fused.  The packed coordinates are refreshed by the pack of the same stage.
+template <int G, bool ENERGY>
+__global__ void __launch_bounds__(B_THREADS) k_batch_pairs(const float4 *__restrict__ xq, int n,
+                                                           const int *__restrict__ rows,
+                                                           const int *__restrict__ counts,
+                                                           const int *__restrict__ rep_of,
+                                                           const BatchRep *__restrict__ reps, float *__restrict__ fx,
+                                                           float *__restrict__ fy, float *__restrict__ fz,
+                                                           float *__restrict__ epot, BatchKick kick,
+                                                           long long *__restrict__ st, int advance) {
+    if (st[E_VALID] == 0) return;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = tid / G, lane = tid % G;
+    float a[3] = {0.f, 0.f, 0.f}, e = 0.f;
+    if (i < n) {
+        const BatchRep &R = reps[__ldg(rep_of + i)];
+        const float Lx = R.L[0], Ly = R.L[1], Lz = R.L[2];
+        const float hLx = 0.5f * Lx, hLy = 0.5f * Ly, hLz = 0.5f * Lz;
+        const float eps = R.eps, sig2 = R.sig2, rc2 = R.rc2;
+        const float eoff = R.kind == PD_PAIR_WCA ? R.eps : -R.eshift;
+        const float4 pi = xq[i];
+        const int cnt = counts[i];
+        auto pair = [&](float4 pj) {
+            const float dx = periodic_delta(pi.x, pj.x, hLx, Lx);
+            const float dy = periodic_delta(pi.y, pj.y, hLy, Ly);
+            const float dz = periodic_delta(pi.z, pj.z, hLz, Lz);
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            if (r2 > 0.f && r2 < rc2) {
+                const float ir2 = 1.f / r2;
+                const float s2 = sig2 * ir2;
+                const float s6 = s2 * s2 * s2;
+                const float s12 = s6 * s6;
+                const float fr = 24.f * eps * (2.f * s12 - s6) * ir2;
+                a[0] += fr * dx;
+                a[1] += fr * dy;
+                a[2] += fr * dz;
+                if (ENERGY) e += 0.5f * (4.f * eps * (s12 - s6) + eoff);
+            }
+        };
+        int slot = lane;
+        for (; slot + G < cnt; slot += 2 * G) {
+            const float4 p1 = xq[rows[(size_t)slot * n + i]];
+            const float4 p2 = xq[rows[(size_t)(slot + G) * n + i]];
+            pair(p1);
+            pair(p2);
+        }
+        for (; slot < cnt; slot += G) pair(xq[rows[(size_t)slot * n + i]]);
+    }
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) a[d] += __shfl_down_sync(0xffffffffu, a[d], off, G);
+        if (ENERGY) e += __shfl_down_sync(0xffffffffu, e, off, G);
+    }
+    if (lane == 0 && i < n) {
+        fx[i] = a[0];
+        fy[i] = a[1];
+        fz[i] = a[2];
+        if (ENERGY) epot[i] = e;
+        if (kick.on) {
+            const float c = kick.half_dt * kick.inv_mass[i];
+            kick.vx[i] = fmaf(c, a[0], kick.vx[i]);
+            kick.vy[i] = fmaf(c, a[1], kick.vy[i]);
+            kick.vz[i] = fmaf(c, a[2], kick.vz[i]);
+        }
+    }
+    if (advance && blockIdx.x == 0 && threadIdx.x == 0) st[E_STEP] += 1;
+}
+
+}  // namespace pdb
+
+struct pd_batch {
+    int nrep = 0, n = 0, ncell = 0, cap = 0, lanes = 4;
+    float rl2 = 0.f, threshold = 0.f;
+    std::vector<BatchRep> hreps;
+    std::vector<int> first;
+    BatchRep *reps = nullptr;
+    int *rep_of = nullptr, *cell_rep = nullptr;
+    long long *st = nullptr;
+    int *cell_of = nullptr, *cell_count = nullptr, *cell_off = nullptr, *sorted = nullptr, *tmp = nullptr;
+    int *rows = nullptr, *counts = nullptr;
+    float4 *ref = nullptr, *xq = nullptr;
+    // bound state (pd_batch_bind)
+    pd_md_state state;
+    bool bound = false;
+    cudaStream_t body = nullptr;
+    bool cond_nodes = true;
+    cudaGraphExec_t exec = nullptr;
+    float exec_dt = 0.f;
+    int exec_lanes = 0;
+    cudaStream_t exec_stream = nullptr;
+};
+
+namespace pdb {
+
+static void batch_free(pd_batch *b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+    if (b->body) cudaStreamDestroy(b->body);
+    b->body = nullptr;
+    dfree(b->reps);
+    dfree(b->rep_of);
+    dfree(b->cell_rep);
+    dfree(b->st);
+    dfree(b->cell_of);
+    dfree(b->cell_count);
+    dfree(b->cell_off);
+    dfree(b->sorted);
+    dfree(b->tmp);
+    dfree(b->rows);
+    dfree(b->counts);
+    dfree(b->ref);
+    dfree(b->xq);
+}
+
+static int batch_rebuild_launch(pd_batch *b, const float *x, const float *y, const float *z, cudaStream_t s) {
+    const int blocks = (b->n + B_THREADS - 1) / B_THREADS;
+    k_batch_bin<<<blocks, B_THREADS, 0, s>>>(x, y, z, b->n, b->rep_of, b->reps, b->cell_of, b->cell_count, b->st);
+    PD_LAUNCHED();
+    int rc;
+    if ((rc = ell_sort_cells_launch(b->cell_of, b->n, b->ncell, b->cell_count, b->cell_off, b->sorted, b->tmp, b->st,
+                                    s)))
+        return rc;
+    k_batch_rows<<<(b->ncell + BROWS_WARPS - 1) / BROWS_WARPS, 32 * BROWS_WARPS,
+                   sizeof(float4) * BROWS_WARPS * BROWS_CAP, s>>>(x, y, z, b->n, b->ncell, b->cell_rep, b->reps,
+                                                                  b->sorted, b->cell_off, b->rl2, b->cap, b->rows,
+                                                                  b->counts, b->ref, b->st);
+    PD_LAUNCHED();
+    return PD_OK;
+}
+
+static int batch_pairs_launch(pd_batch *b, const float *x, const float *y, const float *z, float *fx, float *fy,
+                              float *fz, float *epot, int energy, BatchKick kick, int advance, cudaStream_t s) {
+    k_batch_pack<<<(b->n + B_THREADS - 1) / B_THREADS, B_THREADS, 0, s>>>(x, y, z, b->n, b->xq);
+    PD_LAUNCHED();
+    const int G = b->lanes;
+    const int blocks = (int)(((long long)b->n * G + B_THREADS - 1) / B_THREADS);
+#define PD_BP(GG)                                                                                                      \
+    if (energy)                                                                                                        \
+        k_batch_pairs<GG, true><<<blocks, B_THREADS, 0, s>>>(b->xq, b->n, b->rows, b->counts, b->rep_of, b->reps, fx, \
+                                                              fy, fz, epot, kick, b->st, advance);                     \
+    else                                                                                                               \
+        k_batch_pairs<GG, false><<<blocks, B_THREADS, 0, s>>>(b->xq, b->n, b->rows, b->counts, b->rep_of, b->reps, fx, \
+                                                               fy, fz, epot, kick, b->st, advance);
+    switch (G) {
+        case 1: PD_BP(1) break;
+        case 2: PD_BP(2) break;
+        case 4: PD_BP(4) break;
+        default: PD_BP(8) break;
+    }
+#undef PD_BP
+    PD_LAUNCHED();
+    return PD_OK;
+}
+
+static int batch_enqueue_step(pd_batch *b, float dt, cudaStream_t s, int cond) {
+    const pd_md_state &S = b->state;
+    const int blocks = (b->n + B_THREADS - 1) / B_THREADS;
+    cudaGraphConditionalHandle h = 0;
+    if (cond) {
+        cudaStreamCaptureStatus status;
+        cudaGraph_t g = nullptr;
+        PD_CUDA(cudaStreamGetCaptureInfo(s, &status, nullptr, &g, nullptr, nullptr));
+        PD_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+        k_batch_drift<true, true><<<blocks, B_THREADS, 0, s>>>(b->n, S.x, S.y, S.z, S.vx, S.vy, S.vz, S.fx, S.fy, S.fz,
+                                                               S.inv_mass, dt, b->rep_of, b->reps, b->ref,
+                                                               b->threshold, b->st, h);
+    } else {
+        k_batch_drift<true, false><<<blocks, B_THREADS, 0, s>>>(b->n, S.x, S.y, S.z, S.vx, S.vy, S.vz, S.fx, S.fy,
+                                                                S.fz, S.inv_mass, dt, b->rep_of, b->reps, b->ref,
+                                                                b->threshold, b->st, 0);
+    }
+    PD_LAUNCHED();
+    int rc;
+    if (cond) {
+        if ((rc = capture_if_body(s, b->body, h, [&](cudaStream_t cs) {
+                 return batch_rebuild_launch(b, S.x, S.y, S.z, cs);
+             })))
+            return rc;
+    } else if ((rc = batch_rebuild_launch(b, S.x, S.y, S.z, s))) {
+        return rc;
+    }
+    BatchKick kick;
+    kick.vx = S.vx;
+    kick.vy = S.vy;
+    kick.vz = S.vz;
+    kick.inv_mass = S.inv_mass;
+    kick.half_dt = 0.5f * dt;
+    kick.on = 1;
+    return batch_pairs_launch(b, S.x, S.y, S.z, S.fx, S.fy, S.fz, S.epot, 0, kick, 1, s);
+}
+
+}  // namespace pdb
+
+extern "C" {
+
+int pd_batch_create(pd_batch **out, const pd_batch_replica *reps, int nrep, float skin, int cap, int lanes) {
+    PD_CHECK(out && reps && nrep > 0, PD_EINVAL, "pd_batch_create: bad argument");
+    PD_CHECK(cap > 0, PD_EINVAL, "pd_batch_create: row capacity must be positive");
+    PD_CHECK(lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8, PD_EINVAL, "pd_batch_create: lanes 1, 2, 4 or 8");
+    PD_CHECK(std::isfinite(skin) && skin >= 0.f, PD_EINVAL, "pd_batch_create: skin must be finite and nonnegative");
+    *out = nullptr;
+    float rmax = 0.f;
+    for (int r = 0; r < nrep; ++r) {
+        const pd_batch_replica &R = reps[r];
+        PD_CHECK(R.n > 0, PD_EINVAL, "pd_batch_create: replica %d is empty", r);
+        PD_CHECK(R.kind == PD_PAIR_LJ || R.kind == PD_PAIR_WCA, PD_EINVAL, "pd_batch_create: replica %d pair model", r);
+        PD_CHECK(R.rc2 > 0.f && R.eps >= 0.f && R.sigma > 0.f, PD_EINVAL, "pd_batch_create: replica %d parameters", r);
+        rmax = fmaxf(rmax, sqrtf(R.rc2));
+    }
+    const float rl = rmax + skin;
+    pd_batch *b = new pd_batch();
+    b->nrep = nrep;
+    b->cap = cap;
+    b->lanes = lanes;
+    b->rl2 = rl * rl;
+    b->threshold = 0.25f * skin * skin;
+    std::vector<int> rep_of, cell_rep;
+    for (int r = 0; r < nrep; ++r) {
+        const pd_batch_replica &R = reps[r];
+        BatchRep h;
+        memset(&h, 0, sizeof h);
+        int ng[3];
+        for (int d = 0; d < 3; ++d) {
+            if (!(std::isfinite(R.box[d]) && R.box[d] > 2.0 * rl)) {
+                delete b;
+                set_error("pd_batch_create: replica %d box length %g is not above twice the list radius %g", r,
+                          R.box[d], 2.0 * rl);
+                return PD_EINVAL;
+            }
+            h.L[d] = (float)R.box[d];
+            // cells at least r_list wide; at least three per dimension (then the stencil spans the box)
+            ng[d] = std::max(3, (int)std::floor(h.L[d] / rl));
+        }
+        h.nx = ng[0];
+        h.ny = ng[1];
+        h.nz = ng[2];
+        h.cell_base = b->ncell;
+        h.kind = R.kind;
+        h.eps = R.eps;
+        h.sig2 = R.sigma * R.sigma;
+        h.rc2 = R.rc2;
+        h.eshift = R.eshift;
+        b->hreps.push_back(h);
+        b->first.push_back(b->n);
+        b->n += R.n;
+        const int nc = ng[0] * ng[1] * ng[2];
+        b->ncell += nc;
+        rep_of.insert(rep_of.end(), R.n, r);
+        cell_rep.insert(cell_rep.end(), nc, r);
+    }
+    int rc;
+    const size_t n = (size_t)b->n;
+    if ((rc = dalloc(&b->reps, (size_t)nrep)) || (rc = dalloc(&b->rep_of, n)) ||
+        (rc = dalloc(&b->cell_rep, (size_t)b->ncell)) || (rc = dalloc(&b->st, (size_t)E_LEN)) ||
+        (rc = dalloc(&b->cell_of, n)) || (rc = dalloc(&b->cell_count, (size_t)b->ncell)) ||
+        (rc = dalloc(&b->cell_off, (size_t)b->ncell + 1)) || (rc = dalloc(&b->sorted, n)) ||
+        (rc = dalloc(&b->tmp, n)) || (rc = dalloc(&b->rows, n * (size_t)cap)) || (rc = dalloc(&b->counts, n)) ||
+        (rc = dalloc(&b->ref, n)) || (rc = dalloc(&b->xq, n))) {
+        batch_free(b);
+        delete b;
+        return rc;
+    }
+    long long init[E_LEN] = {0};
+    init[E_INTERVAL] = 100;
+    if (cudaMemcpy(b->reps, b->hreps.data(), sizeof(BatchRep) * nrep, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->rep_of, rep_of.data(), sizeof(int) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->cell_rep, cell_rep.data(), sizeof(int) * b->ncell, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->st, init, sizeof init, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(b->cell_count, 0, sizeof(int) * (size_t)b->ncell) != cudaSuccess ||
+        cudaMemset(b->counts, 0, sizeof(int) * n) != cudaSuccess ||
+        cudaMemset(b->ref, 0, sizeof(float4) * n) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->body, cudaStreamNonBlocking) != cudaSuccess) {
+        batch_free(b);
+        delete b;
+        set_error("pd_batch_create: device initialisation failed");
+        return PD_ECUDA;
+    }
+    *out = b;
+    return PD_OK;
+}
+
+int pd_batch_destroy(pd_batch *b) {
+    if (!b) return PD_OK;
+    batch_free(b);
+    delete b;
+    return PD_OK;
+}
+
+int pd_batch_count(pd_batch *b, int *n, int *ncell) {
+    PD_CHECK(b, PD_EINVAL, "pd_batch_count: null handle");
+    if (n) *n = b->n;
+    if (ncell) *ncell = b->ncell;
+    return PD_OK;
+}
+
+int pd_batch_set_lanes(pd_batch *b, int lanes) {
+    PD_CHECK(b, PD_EINVAL, "pd_batch_set_lanes: null handle");
+    PD_CHECK(lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8, PD_EINVAL, "pd_batch_set_lanes: lanes 1, 2, 4 or 8");
+    b->lanes = lanes;
+    return PD_OK;
+}
+
+int pd_batch_update(pd_batch *b, const float *x, const float *y, const float *z, pd_stream_t sp) {
+    PD_CHECK(b && x && y && z, PD_EINVAL, "pd_batch_update: null argument");
+    cudaStream_t s = (cudaStream_t)sp;
+    k_batch_drift<false, false><<<(b->n + B_THREADS - 1) / B_THREADS, B_THREADS, 0, s>>>(
+        b->n, const_cast<float *>(x), const_cast<float *>(y), const_cast<float *>(z), nullptr, nullptr, nullptr,
+        nullptr, nullptr, nullptr, nullptr, 0.f, b->rep_of, b->reps, b->ref, b->threshold, b->st, 0);
+    PD_LAUNCHED();
+    return batch_rebuild_launch(b, x, y, z, s);
+}
+
+int pd_batch_forces(pd_batch *b, const float *x, const float *y, const float *z, float *fx, float *fy, float *fz,
+                    float *epot, int energy, pd_stream_t sp) {
+    PD_CHECK(b && x && y && z && fx && fy && fz, PD_EINVAL, "pd_batch_forces: null argument");
+    PD_CHECK(!energy || epot, PD_EINVAL, "pd_batch_forces: energy needs epot");
+    BatchKick kick;
+    memset(&kick, 0, sizeof kick);
+    return batch_pairs_launch(b, x, y, z, fx, fy, fz, epot, energy, kick, 0, (cudaStream_t)sp);
+}
+
+int pd_batch_status(pd_batch *b, pd_ell_stats *out) {
+    PD_CHECK(b && out, PD_EINVAL, "pd_batch_status: null argument");
+    long long h[E_LEN];
+    PD_CUDA(cudaMemcpy(h, b->st, sizeof h, cudaMemcpyDeviceToHost));
+    memset(out, 0, sizeof *out);
+    out->valid = h[E_VALID] != 0;
+    out->error = (int)h[E_ERROR];
+    out->requested = h[E_REQUEST] != 0;
+    out->step = h[E_STEP];
+    out->last_build = h[E_LAST_BUILD];
+    out->interval = h[E_INTERVAL];
+    out->checks = h[E_CHECKS];
+    out->builds = h[E_BUILDS];
+    out->required = h[E_REQUIRED];
+    out->cap = b->cap;
+    out->lanes = b->lanes;
+    return PD_OK;
+}
+
+int pd_batch_bind(pd_batch *b, const pd_md_state *st) {
+    PD_CHECK(b && st, PD_EINVAL, "pd_batch_bind: null argument");
+    PD_CHECK(st->n == b->n, PD_EINVAL, "pd_batch_bind: state has %d particles, the batch %d", st->n, b->n);
+    PD_CHECK(st->x && st->y && st->z && st->vx && st->vy && st->vz && st->fx && st->fy && st->fz && st->inv_mass,
+             PD_EINVAL, "pd_batch_bind: state arrays missing (per-particle inverse masses required)");
+    b->state = *st;
+    b->bound = true;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+    return PD_OK;
+}
+
+int pd_batch_evaluate(pd_batch *b, int energy, pd_stream_t sp) {
+    PD_CHECK(b && b->bound, PD_ESTATE, "pd_batch_evaluate: no state bound");
+    const pd_md_state &S = b->state;
+    int rc;
+    if ((rc = pd_batch_update(b, S.x, S.y, S.z, sp))) return rc;
+    PD_CHECK(!energy || S.epot, PD_EINVAL, "pd_batch_evaluate: energy needs epot in the state");
+    return pd_batch_forces(b, S.x, S.y, S.z, S.fx, S.fy, S.fz, S.epot, energy, sp);
+}
+
+int pd_batch_step(pd_batch *b, int nsteps, float dt, int use_graph, pd_stream_t sp) {
+    PD_CHECK(b && b->bound, PD_ESTATE, "pd_batch_step: no state bound");
+    PD_CHECK(nsteps >= 0, PD_EINVAL, "pd_batch_step: negative step count");
+    cudaStream_t s = (cudaStream_t)sp;
+    for (int k = 0; k < nsteps; ++k) {
+        if (!use_graph) {
+            int rc = batch_enqueue_step(b, dt, s, 0);
+            if (rc) return rc;
+            continue;
+        }
+        if (!b->exec || b->exec_dt != dt || b->exec_stream != s || b->exec_lanes != b->lanes) {
+            if (b->exec) {
+                cudaGraphExecDestroy(b->exec);
+                b->exec = nullptr;
+            }
+            PD_CHECK(s != nullptr, PD_EINVAL, "pd_batch_step: graph replay needs a non-default stream");
+            for (int attempt = 0; attempt < 2 && !b->exec; ++attempt) {
+                const int cond = b->cond_nodes ? 1 : 0;
+                cudaGraph_t g = nullptr;
+                PD_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+                const int rc = batch_enqueue_step(b, dt, s, cond);
+                cudaError_t err = cudaStreamEndCapture(s, &g);
+                if (rc == PD_OK && err == cudaSuccess) err = cudaGraphInstantiate(&b->exec, g, 0);
+                if (g) cudaGraphDestroy(g);
+                if (rc == PD_OK && err == cudaSuccess) break;
+                b->exec = nullptr;
+                cudaGetLastError();
+                if (!cond) {
+                    if (rc) return rc;
+                    PD_CHECK(false, PD_ECUDA, "batch step capture failed: %s", cudaGetErrorString(err));
+                }
+                b->cond_nodes = false;
+            }
+            b->exec_dt = dt;
+            b->exec_stream = s;
+            b->exec_lanes = b->lanes;
+        }
+        PD_CUDA(cudaGraphLaunch(b->exec, s));
+    }
+    return PD_OK;
+}
+
+int pd_batch_rows(pd_batch *b, int **rows, int **counts) {
+    PD_CHECK(b && rows && counts, PD_EINVAL, "pd_batch_rows: null argument");
+    *rows = b->rows;
+    *counts = b->counts;
+    return PD_OK;
+}
+
+}  // extern "C"

@@ -165,4 +165,34 @@ int mlp_forward_launch(const pd_mlp *q, const void *X, int n, float *s, const fl
 int learned_correction_launch(pd_learned *h, const pd_mlp *net, const float *x, const float *y, const float *z,
                               const float *q, const int *type, float4 *corr, cudaStream_t s);
 const float4 *learned_corr(const pd_learned *h);
+int ell_sort_cells_launch(const int *cell_of, int n, int ncell, int *cell_count, int *cell_off, int *sorted, int *tmp,
+                          long long *st, cudaStream_t s);
+
+// Append an IF node on handle h to the graph being captured on s, capture body(cs) into its body
+// graph on the helper stream cs, and continue s after the node.
+template <typename F>
+inline int capture_if_body(cudaStream_t s, cudaStream_t cs, cudaGraphConditionalHandle h, F &&body) {
+    cudaStreamCaptureStatus status;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    PD_CUDA(cudaStreamGetCaptureInfo(s, &status, nullptr, &g, &deps, &ndeps));
+    PD_CHECK(status == cudaStreamCaptureStatusActive, PD_ESTATE, "conditional node outside a capture");
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeIf;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    PD_CUDA(cudaGraphAddNode(&node, g, deps, ndeps, &p));
+    PD_CUDA(cudaStreamBeginCaptureToGraph(cs, p.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeRelaxed));
+    const int rc = body(cs);
+    cudaGraph_t done = nullptr;
+    const cudaError_t err = cudaStreamEndCapture(cs, &done);
+    if (rc) return rc;
+    PD_CHECK(err == cudaSuccess, PD_ECUDA, "conditional body capture failed: %s", cudaGetErrorString(err));
+    PD_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    return PD_OK;
+}
 }  // namespace pdb
