@@ -122,3 +122,31 @@ def ionic_melt(n: int, L: float, min_sep: float = 2.2, seed: int = 2026, batch: 
 def melt_masses(q, m_plus: float = 22.99, m_minus: float = 35.45):
     q = np.asarray(q)
     return np.where(q > 0, m_plus, m_minus)
+
+
+def fcc_fill(n: int, rho: float, jitter: float = 0.05, seed: int = 0):
+    """n particles on the sites of the smallest cubic fcc lattice with at least n sites (a seeded
+    random subset), scaled to number density rho, plus uniform jitter; centred coordinates."""
+    rng = np.random.default_rng(seed)
+    m = int(math.ceil((n / 4.0) ** (1.0 / 3.0) - 1e-9))
+    L = (n / rho) ** (1.0 / 3.0)
+    a = L / m
+    basis = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    g = np.stack(np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij"), -1).reshape(-1, 3)
+    sites = ((g[:, None, :] + basis[None, :, :]).reshape(-1, 3) + 0.25) * a
+    pick = np.sort(rng.choice(len(sites), n, replace=False))
+    pos = sites[pick] + rng.uniform(-jitter, jitter, (n, 3))
+    pos -= L * np.floor(pos / L + 0.5)
+    return pos, (L, L, L)
+
+
+def replica_set(nrep: int, n_lo: int = 500, n_hi: int = 20000, rho=(0.70, 0.90), T=(0.6, 1.2), seed: int = 4):
+    """Independent 3D LJ / WCA systems (even replicas LJ, odd WCA): N log-uniform in [n_lo, n_hi],
+    reduced density and temperature uniform in the given ranges, seeded per replica."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for r in range(nrep):
+        n = int(round(math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))))
+        out.append(dict(n=n, rho=float(rng.uniform(*rho)), T=float(rng.uniform(*T)),
+                        kind="lj" if r % 2 == 0 else "wca", seed=int(rng.integers(1 << 31))))
+    return out
