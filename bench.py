@@ -424,6 +424,13 @@ def run_batch_workload(pd, args, world, rank):
     dt = 0.005
     b = pd.batch.BatchedReplicas(systems, skin=0.3)
     b.evaluate()
+    if args.profile:
+        b.step(args.warmup, dt, use_graph=False)
+        b.step(args.steps, dt, use_graph=False)
+        b.synchronize()
+        if rank == 0:
+            print(json.dumps({"profile": "batch512 eager steps", "steps": args.steps, "rows": b.status()}))
+        return
     tune = b.autotune_lanes()
     b.step(args.warmup, dt)
     b.synchronize()

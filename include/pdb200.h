@@ -438,7 +438,10 @@ int pd_batch_update(pd_batch *b, const float *x, const float *y, const float *z,
 int pd_batch_forces(pd_batch *b, const float *x, const float *y, const float *z, float *fx, float *fy, float *fz,
                     float *epot, int energy, pd_stream_t st);
 int pd_batch_status(pd_batch *b, pd_ell_stats *out);
-int pd_batch_rows(pd_batch *b, int **rows, int **counts);
+/* Device pointers of the rows (cap x n ints, slot t of the particle at cell-order position k at
+ * t * n + k, entries are cell-order positions), their lengths (n, by position) and the cell order
+ * (n particle indices). */
+int pd_batch_rows(pd_batch *b, int **rows, int **counts, int **order);
 /* Step state (x, v, f, per-particle inverse masses, optional epot) of all replicas, concatenated. */
 int pd_batch_bind(pd_batch *b, const pd_md_state *st);
 int pd_batch_evaluate(pd_batch *b, int energy, pd_stream_t st);

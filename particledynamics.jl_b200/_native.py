@@ -188,7 +188,7 @@ _SIGS = {
     "pd_batch_update": (C.c_int, [_p, _fp, _fp, _fp, _p]),
     "pd_batch_forces": (C.c_int, [_p, _fp, _fp, _fp, _fp, _fp, _fp, _fp, C.c_int, _p]),
     "pd_batch_status": (C.c_int, [_p, C.POINTER(EllStats)]),
-    "pd_batch_rows": (C.c_int, [_p, C.POINTER(_p), C.POINTER(_p)]),
+    "pd_batch_rows": (C.c_int, [_p, C.POINTER(_p), C.POINTER(_p), C.POINTER(_p)]),
     "pd_batch_bind": (C.c_int, [_p, C.POINTER(MDState)]),
     "pd_batch_evaluate": (C.c_int, [_p, C.c_int, _p]),
     "pd_batch_step": (C.c_int, [_p, C.c_int, C.c_float, C.c_int, _p]),

@@ -7,14 +7,20 @@
 // local cell), so the counting sort of the ELL route (scan, scatter, id order per cell) serves
 // all replicas in one pass.  Per-replica geometry and pair model sit in a small device table
 // read through the read-only cache.  Stages per step:
-//   1. k_batch_drift: half kick, drift, centred wrap in the replica's box, displacement maximum
-//      since the last build; the last block decides the rebuild for all replicas at once and
-//      sets the graph's IF condition;
-//   2. the rebuild (IF node): k_batch_bin, the shared counting sort, k_batch_rows (one warp per
-//      cell, the replica's stencil staged in shared memory, rows identical to the single-system
-//      kernels'), the capacity commit by the last block;
-//   3. k_batch_pairs<G>: G lanes per row (G chosen by the caller's autotuner), the replica's LJ or
-//      WCA model, the closing half kick fused, the device step advanced.
+//   1. k_batch_drift: half kick, drift, centred wrap in the replica's box, per-replica
+//      displacement maxima since each replica's last build; the last block flags the replicas to
+//      rebuild and sets the graph's IF condition when there is one;
+//   2. the rebuild (IF node): k_batch_bin (flagged replicas re-binned, the others keep their
+//      cells), the shared counting sort (which leaves the others' cell order unchanged),
+//      k_batch_rows for the flagged replicas' cells only (one warp per cell, the replica's
+//      stencil staged in shared memory, rows identical to the single-system kernels'), the
+//      capacity commit by the last block;
+//   3. k_batch_pack (coordinates in cell order) and k_batch_pairs<G>: G lanes per row (G chosen by
+//      the caller's autotuner), the replica's LJ or WCA model, the closing half kick fused, the
+//      device step advanced.
+// Rows live in cell order (slot t of the particle at position k of the cell order at t * N + k,
+// entries are cell-order positions), so row stores and loads are contiguous per warp and the
+// neighbours' packed records of a row sit in nearby cells.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -43,8 +49,44 @@ __device__ __forceinline__ float wrap_centred(float x, float L) {
     return x;
 }
 
+// Rebuild decision per replica, taken by the whole last block of the drift kernel: replica r is
+// rebuilt when one of its particles moved more than skin / 2 since its last build, and every replica
+// when the list is invalid or the rebuild interval is reached.  Sets the device request (and the
+// graph's IF condition) when any replica is rebuilt.
+template <bool COND>
+__device__ void batch_decide(long long *st, unsigned *rep_dmax, int *rep_flag, int nrep, float threshold,
+                             bool thread0, cudaGraphConditionalHandle h) {
+    __shared__ int any, all, bad;
+    if (thread0) {
+        st[E_CHECKS] += 1;
+        st[E_REQUEST] = 0;
+        bad = !isfinite(__uint_as_float((unsigned)st[E_DMAX]));
+        all = st[E_VALID] == 0 || st[E_STEP] - st[E_LAST_BUILD] >= st[E_INTERVAL];
+        any = 0;
+        st[E_DMAX] = 0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < nrep; r += blockDim.x) {
+        const int f = (all || __uint_as_float(rep_dmax[r]) > threshold) ? 1 : 0;
+        rep_flag[r] = f;
+        rep_dmax[r] = 0u;
+        if (f) any = 1;   // benign race: every writer stores 1
+    }
+    __syncthreads();
+    if (thread0) {
+        if (bad) {
+            st[E_ERROR] = E_ERR_COORD;
+            st[E_VALID] = 0;
+        } else if (any) {
+            st[E_REQUEST] = 1;
+            st[E_VALID] = 0;
+        }
+        if (COND) cudaGraphSetConditional(h, ell_requested(st) ? 1u : 0u);
+    }
+}
+
 // Half kick, drift, wrap and displacement (DRIFT), or the displacement of the current coordinates
-// alone; the last block decides for all replicas.
+// alone; per-replica displacement maxima, the decision by the last block.
 template <bool DRIFT, bool COND>
 __global__ void __launch_bounds__(B_THREADS) k_batch_drift(int n, float *__restrict__ x, float *__restrict__ y,
                                                            float *__restrict__ z, float *__restrict__ vx,
@@ -55,15 +97,19 @@ __global__ void __launch_bounds__(B_THREADS) k_batch_drift(int n, float *__restr
                                                            const int *__restrict__ rep_of,
                                                            const BatchRep *__restrict__ reps,
                                                            const float4 *__restrict__ ref, float threshold,
-                                                           long long *__restrict__ st, cudaGraphConditionalHandle h) {
+                                                           unsigned *__restrict__ rep_dmax, int *__restrict__ rep_flag,
+                                                           int nrep, long long *__restrict__ st,
+                                                           cudaGraphConditionalHandle h) {
     if (st[E_ERROR] != 0) {
         if (COND && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(h, 0u);
         return;
     }
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     float v = 0.f;
+    int r = -1;
     if (i < n) {
-        const BatchRep &R = reps[__ldg(rep_of + i)];
+        r = __ldg(rep_of + i);
+        const BatchRep &R = reps[r];
         const float L[3] = {R.L[0], R.L[1], R.L[2]};
         float p[3] = {x[i], y[i], z[i]};
         if (DRIFT) {
@@ -80,22 +126,43 @@ __global__ void __launch_bounds__(B_THREADS) k_batch_drift(int n, float *__restr
         }
         v = ell_displacement<3>(p, ref[i], L, st[E_VALID] != 0);
     }
-    if (ell_block_max_last(__float_as_uint(v), st, E_DMAX, E_TICKET_D)) {
-        const float largest = __uint_as_float((unsigned)st[E_DMAX]);
-        st[E_DMAX] = 0;
-        st[E_TICKET_D] = 0;
-        ell_decide<COND>(st, largest, threshold, h);
+    // per-replica maximum: one atomic per warp where the warp's particles share a replica
+    const unsigned bits = __float_as_uint(v);
+    const int r0 = __shfl_sync(0xffffffffu, r, 0);
+    if (__all_sync(0xffffffffu, r == r0)) {
+        const unsigned m = __reduce_max_sync(0xffffffffu, bits);
+        if ((threadIdx.x & 31) == 0 && r0 >= 0) atomicMax(rep_dmax + r0, m);
+    } else if (r >= 0) {
+        atomicMax(rep_dmax + r, bits);
+    }
+    __threadfence();   // the per-replica maxima are visible before this block's ticket
+    __shared__ bool last_block;
+    const bool t0last = ell_block_max_last(bits, st, E_DMAX, E_TICKET_D);
+    if (threadIdx.x == 0) last_block = t0last;
+    __syncthreads();
+    if (last_block) {
+        __threadfence();
+        if (threadIdx.x == 0) st[E_TICKET_D] = 0;
+        batch_decide<COND>(st, rep_dmax, rep_flag, nrep, threshold, threadIdx.x == 0, h);
     }
 }
 
 // Global cell of every particle (its replica's grid) and the cell histogram.
+// Particles of replicas that are not rebuilt keep their cells, so that their cell-order positions,
+// and with them their rows, stay valid through the counting sort.
 __global__ void k_batch_bin(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
                             int n, const int *__restrict__ rep_of, const BatchRep *__restrict__ reps,
-                            int *__restrict__ cell_of, int *__restrict__ cell_count, const long long *__restrict__ st) {
+                            const int *__restrict__ rep_flag, int *__restrict__ cell_of, int *__restrict__ cell_count,
+                            const long long *__restrict__ st) {
     if (!ell_requested(st)) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const BatchRep &R = reps[__ldg(rep_of + i)];
+    const int r = __ldg(rep_of + i);
+    if (!rep_flag[r]) {
+        atomicAdd(&cell_count[cell_of[i]], 1);
+        return;
+    }
+    const BatchRep &R = reps[r];
     const float p[3] = {x[i], y[i], z[i]};
     const int ng[3] = {R.nx, R.ny, R.nz};
     int cc[3];
@@ -111,19 +178,21 @@ __global__ void k_batch_bin(const float *__restrict__ x, const float *__restrict
 }
 
 // Rows, one warp per global cell: the replica's stencil (same visiting order as the single-system
-// row kernels) staged in shared memory, each lane a particle of the cell.
+// row kernels) staged in shared memory, each lane a particle of the cell.  Rows, their lengths and
+// their entries are in cell order (positions in `sorted`), so the row stores of a warp and the pair
+// kernel's row loads are contiguous and neighbours' packed records sit close together.
 __global__ void __launch_bounds__(32 * BROWS_WARPS) k_batch_rows(
     const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z, int n, int ncell,
-    const int *__restrict__ cell_rep, const BatchRep *__restrict__ reps, const int *__restrict__ sorted,
-    const int *__restrict__ cell_off, float rl2, int cap, int *__restrict__ rows, int *__restrict__ counts,
-    float4 *__restrict__ ref, long long *__restrict__ st) {
+    const int *__restrict__ cell_rep, const BatchRep *__restrict__ reps, const int *__restrict__ rep_flag,
+    const int *__restrict__ sorted, const int *__restrict__ cell_off, float rl2, int cap, int *__restrict__ rows,
+    int *__restrict__ counts, float4 *__restrict__ ref, long long *__restrict__ st) {
     if (!ell_requested(st)) return;
     extern __shared__ float4 batch_stage[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c = blockIdx.x * BROWS_WARPS + w;
     float4 *sw = batch_stage + w * BROWS_CAP;
     unsigned fmax = 0;
-    if (c < ncell) {   // warp-uniform
+    if (c < ncell && rep_flag[__ldg(cell_rep + c)]) {   // warp-uniform; only replicas being rebuilt
         const BatchRep &R = reps[__ldg(cell_rep + c)];
         const float Lx = R.L[0], Ly = R.L[1], Lz = R.L[2];
         const int nx = R.nx, ny = R.ny, nz = R.nz, base = R.cell_base;
@@ -136,7 +205,8 @@ __global__ void __launch_bounds__(32 * BROWS_WARPS) k_batch_rows(
         const int p0 = cell_off[c], pn = cell_off[c + 1] - p0;
         for (int pg = 0; pg < pn; pg += 32) {
             const bool has = pg + lane < pn;
-            const int i = has ? sorted[p0 + pg + lane] : -1;
+            const int kp = p0 + pg + lane;   // this lane's particle: its position in cell order
+            const int i = has ? sorted[kp] : -1;
             const float xi = has ? x[i] : 0.f, yi = has ? y[i] : 0.f, zi = has ? z[i] : 0.f;
             int found = 0;
             int fill = 0;
@@ -145,14 +215,14 @@ __global__ void __launch_bounds__(32 * BROWS_WARPS) k_batch_rows(
                 if (has) {
                     for (int t = 0; t < fill; ++t) {
                         const float4 cj = sw[t];
-                        const int j = __float_as_int(cj.w);
-                        if (j == i) continue;
+                        const int kc = __float_as_int(cj.w);
+                        if (kc == kp) continue;
                         const float dx = mic_fast(cj.x - xi, hLx, Lx);
                         const float dy = mic_fast(cj.y - yi, hLy, Ly);
                         const float dz = mic_fast(cj.z - zi, hLz, Lz);
                         const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                         if (r2 <= rl2) {
-                            if (found < cap) rows[(size_t)found * n + i] = j;
+                            if (found < cap) rows[(size_t)found * n + kp] = kc;
                             ++found;
                         }
                     }
@@ -166,7 +236,7 @@ __global__ void __launch_bounds__(32 * BROWS_WARPS) k_batch_rows(
                     if (fill + cnt > BROWS_CAP) scan();
                     if (lane < cnt) {
                         const int j = sorted[k0 + lane];
-                        sw[fill + lane] = make_float4(x[j], y[j], z[j], __int_as_float(j));
+                        sw[fill + lane] = make_float4(x[j], y[j], z[j], __int_as_float(k0 + lane));
                     }
                     fill += cnt;
                 }
@@ -192,7 +262,7 @@ __global__ void __launch_bounds__(32 * BROWS_WARPS) k_batch_rows(
             }
             scan();
             if (has) {
-                counts[i] = found;
+                counts[kp] = found;
                 ref[i] = make_float4(xi, yi, zi, 0.f);
             }
             fmax = max(fmax, (unsigned)found);
@@ -214,10 +284,15 @@ __global__ void __launch_bounds__(32 * BROWS_WARPS) k_batch_rows(
     }
 }
 
+// Packed coordinates in cell order: xq[k] = (x, y, z) of particle sorted[k].
 __global__ void k_batch_pack(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
-                             int n, float4 *__restrict__ xq) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) xq[i] = make_float4(x[i], y[i], z[i], 0.f);
+                             const int *__restrict__ sorted, int n, float4 *__restrict__ xq,
+                             const long long *__restrict__ st) {
+    if (st[E_VALID] == 0) return;   // no rows: the pair kernel will not read the packed records
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = sorted[k];
+    xq[k] = make_float4(x[i], y[i], z[i], 0.f);
 }
 
 struct BatchKick {
@@ -234,6 +309,7 @@ template <int G, bool ENERGY>
 __global__ void __launch_bounds__(B_THREADS) k_batch_pairs(const float4 *__restrict__ xq, int n,
                                                            const int *__restrict__ rows,
                                                            const int *__restrict__ counts,
+                                                           const int *__restrict__ sorted,
                                                            const int *__restrict__ rep_of,
                                                            const BatchRep *__restrict__ reps, float *__restrict__ fx,
                                                            float *__restrict__ fy, float *__restrict__ fz,
@@ -241,16 +317,17 @@ __global__ void __launch_bounds__(B_THREADS) k_batch_pairs(const float4 *__restr
                                                            long long *__restrict__ st, int advance) {
     if (st[E_VALID] == 0) return;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = tid / G, lane = tid % G;
+    const int k = tid / G, lane = tid % G;   // position in cell order
+    const int i = k < n ? sorted[k] : -1;
     float a[3] = {0.f, 0.f, 0.f}, e = 0.f;
-    if (i < n) {
+    if (k < n) {
         const BatchRep &R = reps[__ldg(rep_of + i)];
         const float Lx = R.L[0], Ly = R.L[1], Lz = R.L[2];
         const float hLx = 0.5f * Lx, hLy = 0.5f * Ly, hLz = 0.5f * Lz;
         const float eps = R.eps, sig2 = R.sig2, rc2 = R.rc2;
         const float eoff = R.kind == PD_PAIR_WCA ? R.eps : -R.eshift;
-        const float4 pi = xq[i];
-        const int cnt = counts[i];
+        const float4 pi = xq[k];
+        const int cnt = counts[k];
         auto pair = [&](float4 pj) {
             const float dx = periodic_delta(pi.x, pj.x, hLx, Lx);
             const float dy = periodic_delta(pi.y, pj.y, hLy, Ly);
@@ -270,12 +347,12 @@ __global__ void __launch_bounds__(B_THREADS) k_batch_pairs(const float4 *__restr
         };
         int slot = lane;
         for (; slot + G < cnt; slot += 2 * G) {
-            const float4 p1 = xq[rows[(size_t)slot * n + i]];
-            const float4 p2 = xq[rows[(size_t)(slot + G) * n + i]];
+            const float4 p1 = xq[rows[(size_t)slot * n + k]];
+            const float4 p2 = xq[rows[(size_t)(slot + G) * n + k]];
             pair(p1);
             pair(p2);
         }
-        for (; slot < cnt; slot += G) pair(xq[rows[(size_t)slot * n + i]]);
+        for (; slot < cnt; slot += G) pair(xq[rows[(size_t)slot * n + k]]);
     }
 #pragma unroll
     for (int off = G / 2; off > 0; off >>= 1) {
@@ -283,7 +360,7 @@ __global__ void __launch_bounds__(B_THREADS) k_batch_pairs(const float4 *__restr
         for (int d = 0; d < 3; ++d) a[d] += __shfl_down_sync(0xffffffffu, a[d], off, G);
         if (ENERGY) e += __shfl_down_sync(0xffffffffu, e, off, G);
     }
-    if (lane == 0 && i < n) {
+    if (lane == 0 && k < n) {
         fx[i] = a[0];
         fy[i] = a[1];
         fz[i] = a[2];
@@ -307,6 +384,8 @@ struct pd_batch {
     std::vector<int> first;
     BatchRep *reps = nullptr;
     int *rep_of = nullptr, *cell_rep = nullptr;
+    int *rep_flag = nullptr;         // replicas rebuilt by the current decision
+    unsigned *rep_dmax = nullptr;    // per-replica displacement maxima (float bits)
     long long *st = nullptr;
     int *cell_of = nullptr, *cell_count = nullptr, *cell_off = nullptr, *sorted = nullptr, *tmp = nullptr;
     int *rows = nullptr, *counts = nullptr;
@@ -332,6 +411,8 @@ static void batch_free(pd_batch *b) {
     dfree(b->reps);
     dfree(b->rep_of);
     dfree(b->cell_rep);
+    dfree(b->rep_flag);
+    dfree(b->rep_dmax);
     dfree(b->st);
     dfree(b->cell_of);
     dfree(b->cell_count);
@@ -346,7 +427,8 @@ static void batch_free(pd_batch *b) {
 
 static int batch_rebuild_launch(pd_batch *b, const float *x, const float *y, const float *z, cudaStream_t s) {
     const int blocks = (b->n + B_THREADS - 1) / B_THREADS;
-    k_batch_bin<<<blocks, B_THREADS, 0, s>>>(x, y, z, b->n, b->rep_of, b->reps, b->cell_of, b->cell_count, b->st);
+    k_batch_bin<<<blocks, B_THREADS, 0, s>>>(x, y, z, b->n, b->rep_of, b->reps, b->rep_flag, b->cell_of,
+                                             b->cell_count, b->st);
     PD_LAUNCHED();
     int rc;
     if ((rc = ell_sort_cells_launch(b->cell_of, b->n, b->ncell, b->cell_count, b->cell_off, b->sorted, b->tmp, b->st,
@@ -354,24 +436,27 @@ static int batch_rebuild_launch(pd_batch *b, const float *x, const float *y, con
         return rc;
     k_batch_rows<<<(b->ncell + BROWS_WARPS - 1) / BROWS_WARPS, 32 * BROWS_WARPS,
                    sizeof(float4) * BROWS_WARPS * BROWS_CAP, s>>>(x, y, z, b->n, b->ncell, b->cell_rep, b->reps,
-                                                                  b->sorted, b->cell_off, b->rl2, b->cap, b->rows,
-                                                                  b->counts, b->ref, b->st);
+                                                                  b->rep_flag, b->sorted, b->cell_off, b->rl2, b->cap,
+                                                                  b->rows, b->counts, b->ref, b->st);
     PD_LAUNCHED();
     return PD_OK;
 }
 
 static int batch_pairs_launch(pd_batch *b, const float *x, const float *y, const float *z, float *fx, float *fy,
                               float *fz, float *epot, int energy, BatchKick kick, int advance, cudaStream_t s) {
-    k_batch_pack<<<(b->n + B_THREADS - 1) / B_THREADS, B_THREADS, 0, s>>>(x, y, z, b->n, b->xq);
+    k_batch_pack<<<(b->n + B_THREADS - 1) / B_THREADS, B_THREADS, 0, s>>>(x, y, z, b->sorted, b->n, b->xq,
+                                                                          b->st);
     PD_LAUNCHED();
     const int G = b->lanes;
     const int blocks = (int)(((long long)b->n * G + B_THREADS - 1) / B_THREADS);
 #define PD_BP(GG)                                                                                                      \
     if (energy)                                                                                                        \
-        k_batch_pairs<GG, true><<<blocks, B_THREADS, 0, s>>>(b->xq, b->n, b->rows, b->counts, b->rep_of, b->reps, fx, \
+        k_batch_pairs<GG, true><<<blocks, B_THREADS, 0, s>>>(b->xq, b->n, b->rows, b->counts, b->sorted, b->rep_of, \
+                                                              b->reps, fx, \
                                                               fy, fz, epot, kick, b->st, advance);                     \
     else                                                                                                               \
-        k_batch_pairs<GG, false><<<blocks, B_THREADS, 0, s>>>(b->xq, b->n, b->rows, b->counts, b->rep_of, b->reps, fx, \
+        k_batch_pairs<GG, false><<<blocks, B_THREADS, 0, s>>>(b->xq, b->n, b->rows, b->counts, b->sorted, b->rep_of, \
+                                                               b->reps, fx, \
                                                                fy, fz, epot, kick, b->st, advance);
     switch (G) {
         case 1: PD_BP(1) break;
@@ -395,11 +480,13 @@ static int batch_enqueue_step(pd_batch *b, float dt, cudaStream_t s, int cond) {
         PD_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
         k_batch_drift<true, true><<<blocks, B_THREADS, 0, s>>>(b->n, S.x, S.y, S.z, S.vx, S.vy, S.vz, S.fx, S.fy, S.fz,
                                                                S.inv_mass, dt, b->rep_of, b->reps, b->ref,
-                                                               b->threshold, b->st, h);
+                                                               b->threshold, b->rep_dmax, b->rep_flag, b->nrep,
+                                                               b->st, h);
     } else {
         k_batch_drift<true, false><<<blocks, B_THREADS, 0, s>>>(b->n, S.x, S.y, S.z, S.vx, S.vy, S.vz, S.fx, S.fy,
                                                                 S.fz, S.inv_mass, dt, b->rep_of, b->reps, b->ref,
-                                                                b->threshold, b->st, 0);
+                                                                b->threshold, b->rep_dmax, b->rep_flag, b->nrep,
+                                                                b->st, 0);
     }
     PD_LAUNCHED();
     int rc;
@@ -484,6 +571,7 @@ int pd_batch_create(pd_batch **out, const pd_batch_replica *reps, int nrep, floa
     const size_t n = (size_t)b->n;
     if ((rc = dalloc(&b->reps, (size_t)nrep)) || (rc = dalloc(&b->rep_of, n)) ||
         (rc = dalloc(&b->cell_rep, (size_t)b->ncell)) || (rc = dalloc(&b->st, (size_t)E_LEN)) ||
+        (rc = dalloc(&b->rep_flag, (size_t)nrep)) || (rc = dalloc(&b->rep_dmax, (size_t)nrep)) ||
         (rc = dalloc(&b->cell_of, n)) || (rc = dalloc(&b->cell_count, (size_t)b->ncell)) ||
         (rc = dalloc(&b->cell_off, (size_t)b->ncell + 1)) || (rc = dalloc(&b->sorted, n)) ||
         (rc = dalloc(&b->tmp, n)) || (rc = dalloc(&b->rows, n * (size_t)cap)) || (rc = dalloc(&b->counts, n)) ||
@@ -494,11 +582,17 @@ int pd_batch_create(pd_batch **out, const pd_batch_replica *reps, int nrep, floa
     }
     long long init[E_LEN] = {0};
     init[E_INTERVAL] = 100;
+    std::vector<int> iota(n);
+    for (size_t k = 0; k < n; ++k) iota[k] = (int)k;   // a valid cell order before the first build
     if (cudaMemcpy(b->reps, b->hreps.data(), sizeof(BatchRep) * nrep, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(b->sorted, iota.data(), sizeof(int) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(b->rep_of, rep_of.data(), sizeof(int) * n, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(b->cell_rep, cell_rep.data(), sizeof(int) * b->ncell, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(b->st, init, sizeof init, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(b->cell_count, 0, sizeof(int) * (size_t)b->ncell) != cudaSuccess ||
+        cudaMemset(b->rep_flag, 0, sizeof(int) * (size_t)nrep) != cudaSuccess ||
+        cudaMemset(b->rep_dmax, 0, sizeof(unsigned) * (size_t)nrep) != cudaSuccess ||
+        cudaMemset(b->cell_of, 0, sizeof(int) * n) != cudaSuccess ||
         cudaMemset(b->counts, 0, sizeof(int) * n) != cudaSuccess ||
         cudaMemset(b->ref, 0, sizeof(float4) * n) != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->body, cudaStreamNonBlocking) != cudaSuccess) {
@@ -537,7 +631,8 @@ int pd_batch_update(pd_batch *b, const float *x, const float *y, const float *z,
     cudaStream_t s = (cudaStream_t)sp;
     k_batch_drift<false, false><<<(b->n + B_THREADS - 1) / B_THREADS, B_THREADS, 0, s>>>(
         b->n, const_cast<float *>(x), const_cast<float *>(y), const_cast<float *>(z), nullptr, nullptr, nullptr,
-        nullptr, nullptr, nullptr, nullptr, 0.f, b->rep_of, b->reps, b->ref, b->threshold, b->st, 0);
+        nullptr, nullptr, nullptr, nullptr, 0.f, b->rep_of, b->reps, b->ref, b->threshold, b->rep_dmax, b->rep_flag,
+        b->nrep, b->st, 0);
     PD_LAUNCHED();
     return batch_rebuild_launch(b, x, y, z, s);
 }
@@ -633,10 +728,11 @@ int pd_batch_step(pd_batch *b, int nsteps, float dt, int use_graph, pd_stream_t 
     return PD_OK;
 }
 
-int pd_batch_rows(pd_batch *b, int **rows, int **counts) {
+int pd_batch_rows(pd_batch *b, int **rows, int **counts, int **order) {
     PD_CHECK(b && rows && counts, PD_EINVAL, "pd_batch_rows: null argument");
     *rows = b->rows;
     *counts = b->counts;
+    if (order) *order = b->sorted;
     return PD_OK;
 }
 

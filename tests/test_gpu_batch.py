@@ -19,16 +19,24 @@ def test_batch_rows_match_oracle(pd, ora, cuda):
     st = b.status()
     assert st["valid"] and st["error"] == 0 and st["builds"] == 1
     import ctypes as C
-    rows_p, counts_p = C.c_void_p(), C.c_void_p()
-    pd._native.call("pd_batch_rows", b.handle, C.byref(rows_p), C.byref(counts_p))
+    rows_p, counts_p, order_p = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    pd._native.call("pd_batch_rows", b.handle, C.byref(rows_p), C.byref(counts_p), C.byref(order_p))
     import torch
     n = b.n
     rows = torch.empty(128 * n, dtype=torch.int32, device="cuda")
     counts = torch.empty(n, dtype=torch.int32, device="cuda")
+    order = torch.empty(n, dtype=torch.int32, device="cuda")
     pd.engine._memcpy_d2d(rows.data_ptr(), rows_p.value, 4 * 128 * n)
     pd.engine._memcpy_d2d(counts.data_ptr(), counts_p.value, 4 * n)
-    rows = rows.view(128, n).t().cpu().numpy()
-    counts = counts.cpu().numpy()
+    pd.engine._memcpy_d2d(order.data_ptr(), order_p.value, 4 * n)
+    # rows by cell-order position -> rows by particle index
+    order = order.cpu().numpy()
+    pos_of = np.empty(n, np.int64)
+    pos_of[order] = np.arange(n)
+    rows_k = rows.view(128, n).t().cpu().numpy()
+    counts_k = counts.cpu().numpy()
+    rows = order[rows_k[pos_of]]
+    counts = counts_k[pos_of]
     rl = 2.5 + 0.3
     for k, s in enumerate(systems):
         a = int(b.first[k])
