@@ -142,3 +142,25 @@ def make_systems(specs, mass: float = 1.0):
         out.append(dict(n=sp["n"], box=box, kind=sp["kind"], positions=pos, velocities=vel, masses=mass,
                         T=sp["T"], rho=sp["rho"]))
     return out
+
+
+def replica_cost(spec) -> float:
+    """Work estimate of one replica per step: N times its neighbours per particle (N rho r_list^3)."""
+    return float(spec["n"]) * float(spec["rho"]) * (LJ_RC + 0.3) ** 3
+
+
+def partition_by_cost(specs, world: int):
+    """Replicas split across `world` ranks by cost (longest-processing-time greedy): every rank gets a
+    list of replica indices; the lists are disjoint, cover every replica and depend only on the specs,
+    so every rank computes the same partition without communication."""
+    if world < 1:
+        raise ValueError("world must be at least 1")
+    order = sorted(range(len(specs)), key=lambda k: (-replica_cost(specs[k]), k))
+    load = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for k in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(k)
+        load[r] += replica_cost(specs[k])
+    return [sorted(p) for p in parts]
+
