@@ -263,35 +263,6 @@ static int enqueue_forces(pd_md *md, int energy, float half_dt, cudaStream_t s) 
     return PD_OK;
 }
 
-// Append an IF node on `h` to the graph being captured on s and capture body(cs) into
-// its body graph on the helper stream cs; s then continues after the IF node.
-template <typename F>
-static int capture_if(cudaStream_t s, cudaStream_t cs, cudaGraphConditionalHandle h, F &&body) {
-    cudaStreamCaptureStatus status;
-    cudaGraph_t g = nullptr;
-    const cudaGraphNode_t *deps = nullptr;
-    size_t ndeps = 0;
-    unsigned long long id = 0;
-    PD_CUDA(cudaStreamGetCaptureInfo(s, &status, &id, &g, &deps, &ndeps));
-    PD_CHECK(status == cudaStreamCaptureStatusActive, PD_ESTATE, "conditional node outside a capture");
-    cudaGraphNodeParams p = {};
-    p.type = cudaGraphNodeTypeConditional;
-    p.conditional.handle = h;
-    p.conditional.type = cudaGraphCondTypeIf;
-    p.conditional.size = 1;
-    cudaGraphNode_t node;
-    PD_CUDA(cudaGraphAddNode(&node, g, deps, ndeps, &p));
-    cudaGraph_t bodyg = p.conditional.phGraph_out[0];
-    PD_CUDA(cudaStreamBeginCaptureToGraph(cs, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-    const int rc = body(cs);
-    cudaGraph_t done = nullptr;
-    const cudaError_t e = cudaStreamEndCapture(cs, &done);
-    if (rc) return rc;
-    PD_CHECK(e == cudaSuccess, PD_ECUDA, "conditional body capture failed: %s", cudaGetErrorString(e));
-    PD_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
-    return PD_OK;
-}
-
 // One full step, device-decided.  cond = 1 (inside a stream capture): the build and
 // prune bodies become IF nodes of the captured graph; otherwise their kernels are
 // launched and return at once when the device flags are clear.
@@ -313,7 +284,7 @@ static int enqueue_step(pd_md *md, float dt, int energy, cudaStream_t s, int con
                                               c->slot_of, c->xq, c->ref_build, c->ref_prune, hb * hb, hp * hp,
                                               c->counts, c->p.nstlist, c->p.nstprune, hbuild);
         PD_LAUNCHED();
-        if ((rc = capture_if(s, md->body, hbuild, [&](cudaStream_t cs) {
+        if ((rc = capture_if_body(s, md->body, hbuild, [&](cudaStream_t cs) {
                  return cluster_build_launch(c, st.x, st.y, st.z, q, st.type, 1, cs);
              })))
             return rc;
@@ -496,10 +467,13 @@ int pd_md_step_host(pd_md *md, float *host_xyz, float *host_v, int nsteps, float
     pd_md_state &st = md->st;
     const size_t nb = sizeof(float) * (size_t)st.n;
     float *dx[3] = {st.x, st.y, st.z}, *dv[3] = {st.vx, st.vy, st.vz};
-    for (int d = 0; d < 3; ++d) {
-        PD_CUDA(cudaMemcpyAsync(dx[d], host_xyz + (size_t)d * st.n, nb, cudaMemcpyHostToDevice, s));
-        PD_CUDA(cudaMemcpyAsync(dv[d], host_v + (size_t)d * st.n, nb, cudaMemcpyHostToDevice, s));
-    }
+    // one copy per array triple when the caller keeps its components in one block
+    const bool xblock = st.y == st.x + st.n && st.z == st.y + st.n;
+    const bool vblock = st.vy == st.vx + st.n && st.vz == st.vy + st.n;
+    for (int d = 0; d < (xblock ? 1 : 3); ++d)
+        PD_CUDA(cudaMemcpyAsync(dx[d], host_xyz + (size_t)d * st.n, xblock ? 3 * nb : nb, cudaMemcpyHostToDevice, s));
+    for (int d = 0; d < (vblock ? 1 : 3); ++d)
+        PD_CUDA(cudaMemcpyAsync(dv[d], host_v + (size_t)d * st.n, vblock ? 3 * nb : nb, cudaMemcpyHostToDevice, s));
     int rc = pd_md_step(md, nsteps, dt, epot_sum ? 1 : 0, 1, sp);
     if (rc) return rc;
     if (epot_sum) {
@@ -508,10 +482,10 @@ int pd_md_step_host(pd_md *md, float *host_xyz, float *host_v, int nsteps, float
         PD_LAUNCHED();
         PD_CUDA(cudaMemcpyAsync(epot_sum, md->esum, sizeof(double), cudaMemcpyDeviceToHost, s));
     }
-    for (int d = 0; d < 3; ++d) {
-        PD_CUDA(cudaMemcpyAsync(host_xyz + (size_t)d * st.n, dx[d], nb, cudaMemcpyDeviceToHost, s));
-        PD_CUDA(cudaMemcpyAsync(host_v + (size_t)d * st.n, dv[d], nb, cudaMemcpyDeviceToHost, s));
-    }
+    for (int d = 0; d < (xblock ? 1 : 3); ++d)
+        PD_CUDA(cudaMemcpyAsync(host_xyz + (size_t)d * st.n, dx[d], xblock ? 3 * nb : nb, cudaMemcpyDeviceToHost, s));
+    for (int d = 0; d < (vblock ? 1 : 3); ++d)
+        PD_CUDA(cudaMemcpyAsync(host_v + (size_t)d * st.n, dv[d], vblock ? 3 * nb : nb, cudaMemcpyDeviceToHost, s));
     PD_CUDA(cudaStreamSynchronize(s));
     return PD_OK;
 }
