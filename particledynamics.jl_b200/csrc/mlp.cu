@@ -23,6 +23,7 @@
 // word, skips the remaining work and the tensor memory is still released.
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -196,63 +197,96 @@ __device__ __forceinline__ void load_weights(unsigned char *sm, uint32_t ow1, ui
             __ldg(reinterpret_cast<const uint4 *>(wt.w2 + (size_t)t * MLP_H) + c);
 }
 
-// Shared-memory plan of the inference kernel (bytes).
-constexpr int FW_X = 0, FW_W1 = FW_X + MLP_TILE * MLP_IN * 2, FW_W2 = FW_W1 + MLP_H * MLP_IN * 2,
-              FW_H1 = FW_W2 + MLP_H * MLP_H * 2, FW_BYTES = FW_H1 + MLP_TILE * MLP_H * 2;
-constexpr int FW_THREADS = 256;
+// Inference kernel: persistent, one CTA per SM with four warpgroups; each warpgroup owns one 128-row
+// tile at a time (its own X and H1 buffers, 128 TMEM columns and mbarrier), the weights are staged
+// once per CTA and shared, so four tiles' load -> MMA -> epilogue chains overlap on every SM.
+constexpr int FW_WG = 4, FW_THREADS = 128 * FW_WG;
+constexpr int FW_W1 = 0, FW_W2 = FW_W1 + MLP_H * MLP_IN * 2, FW_TILES = FW_W2 + MLP_H * MLP_H * 2;
+constexpr int FW_X = 0, FW_H1 = FW_X + MLP_TILE * MLP_IN * 2, FW_TILE_BYTES = FW_H1 + MLP_TILE * MLP_H * 2;
+constexpr int FW_BYTES = FW_TILES + FW_WG * FW_TILE_BYTES;
 
-// Inference over one 128-row tile: s = w3 . silu(W2 h1 + b2) + b3 with h1 = bf16(silu(W1 x + b1)).
-// out_s[r] = s, and with V given corr[r] = (s V.x, s V.y, s V.z, s): the force residual s_i V_i
-// of the learned correction.  Two warpgroups: warp w reads TMEM lanes 32 (w % 4) .. (its rows)
-// and the column half w / 4 of each accumulator; the two halves of s meet in shared memory.
-__global__ void __launch_bounds__(FW_THREADS) k_mlp_forward(const __nv_bfloat16 *__restrict__ X, int n,
-                                                           MlpWeights wt, float *__restrict__ out_s,
-                                                           const float4 *__restrict__ V,
-                                                           float4 *__restrict__ corr, int *__restrict__ err) {
+__device__ __forceinline__ void wg_barrier(int g) {   // the 128 threads of warpgroup g
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(128) : "memory");
+}
+// Barrier of warpgroup g that also returns whether every thread's flag is set (a uniform decision).
+__device__ __forceinline__ bool wg_and(int g, bool flag) {
+    uint32_t res;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.b32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, %2, %3, p;\n\t"
+        "selp.b32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(res)
+        : "r"((uint32_t)flag), "r"(1 + g), "r"(128)
+        : "memory");
+    return res != 0;
+}
+__device__ __forceinline__ void wg_tc_sync(int g) {
+    fence_async_smem();
+    tc_fence_before();
+    wg_barrier(g);
+    tc_fence_after();
+}
+
+// s = w3 . silu(W2 h1 + b2) + b3 with h1 = bf16(silu(W1 x + b1)) for every row; out_s[r] = s and,
+// with V given, corr[r] = (s V.x, s V.y, s V.z, s): the force residual s_i V_i of the learned
+// correction.  Thread t of warpgroup g owns tile row t (TMEM lane t) in both epilogues.
+__global__ void __launch_bounds__(FW_THREADS, 1) k_mlp_forward(const __nv_bfloat16 *__restrict__ X, int n,
+                                                              MlpWeights wt, float *__restrict__ out_s,
+                                                              const float4 *__restrict__ V,
+                                                              float4 *__restrict__ corr, int *__restrict__ err) {
     extern __shared__ __align__(1024) unsigned char sm[];
-    __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(8) uint64_t bars[FW_WG];
     __shared__ uint32_t tmem_base;
     __shared__ float sb1[MLP_H], sb2[MLP_H], sw3[MLP_H];
-    __shared__ float spart[MLP_TILE];
     const int t = threadIdx.x, w = t >> 5, lane = t & 31;
-    const int row0 = blockIdx.x * MLP_TILE;
-    const int rt = t & 127, half = t >> 7;   // load role: row rt, half of its chunks
-    if (w == 0) tmem_alloc(smem_u32(&tmem_base), 128);
-    if (t == 0) mbar_init(smem_u32(&bar), 1);
+    const int g = t >> 7, tl = t & 127;   // warpgroup, thread (= tile row) within it
+    if (w == 0) tmem_alloc(smem_u32(&tmem_base), 128 * FW_WG);
+    if (t < FW_WG) mbar_init(smem_u32(&bars[t]), 1);
     if (t < MLP_H) {
         sb1[t] = __ldg(wt.b1 + t);
         sb2[t] = __ldg(wt.b2 + t);
         sw3[t] = __ldg(wt.w3 + t);
     }
-    {
-        const int r = row0 + rt;
-        const uint4 zero = make_uint4(0, 0, 0, 0);
+    // weights once per CTA: row t % 128 of W1 and W2, the chunks split over the four warpgroups
 #pragma unroll
-        for (int c = 2 * half; c < 2 * half + 2; ++c) {
-            *reinterpret_cast<uint4 *>(sm + FW_X + cm_off(rt, 8 * c, MLP_IN)) =
-                r < n ? __ldg(reinterpret_cast<const uint4 *>(X + (size_t)r * MLP_IN) + c) : zero;
-            *reinterpret_cast<uint4 *>(sm + FW_W1 + cm_off(rt, 8 * c, MLP_IN)) =
-                __ldg(reinterpret_cast<const uint4 *>(wt.w1 + (size_t)rt * MLP_IN) + c);
-        }
-#pragma unroll 4
-        for (int c = 8 * half; c < 8 * half + 8; ++c)
-            *reinterpret_cast<uint4 *>(sm + FW_W2 + cm_off(rt, 8 * c, MLP_H)) =
-                __ldg(reinterpret_cast<const uint4 *>(wt.w2 + (size_t)rt * MLP_H) + c);
-    }
+    for (int c = g; c < MLP_IN / 8; c += FW_WG)
+        *reinterpret_cast<uint4 *>(sm + FW_W1 + cm_off(tl, 8 * c, MLP_IN)) =
+            __ldg(reinterpret_cast<const uint4 *>(wt.w1 + (size_t)tl * MLP_IN) + c);
+#pragma unroll
+    for (int c = g; c < MLP_H / 8; c += FW_WG)
+        *reinterpret_cast<uint4 *>(sm + FW_W2 + cm_off(tl, 8 * c, MLP_H)) =
+            __ldg(reinterpret_cast<const uint4 *>(wt.w2 + (size_t)tl * MLP_H) + c);
     tc_sync();
-    const uint32_t tm = tmem_base, b = smem_u32(&bar), base = smem_u32(sm);
-    const int m = 32 * (w & 3) + lane;   // tile row (TMEM lane) of this thread in the epilogues
-    const int c_lo = 64 * (w >> 2);      // its column half
-    const uint32_t lane_addr = tm + ((uint32_t)(32 * (w & 3)) << 16);
-    if (t == 0) {
-        gemm_issue(tm, base + FW_X, base + FW_W1, MLP_IN, MLP_TILE, MLP_H, false);
-        umma_commit(b);
-    }
-    bool ok = mbar_wait(b, 0);
-    if (ok) {
+    const float b3 = __ldg(wt.b3);
+    const uint32_t base = smem_u32(sm), bar = smem_u32(&bars[g]);
+    const uint32_t tm = tmem_base + 128u * g;                          // this group's columns
+    const uint32_t lane_addr = tm + ((uint32_t)(32 * (w & 3)) << 16);  // this warp's lane quarter
+    unsigned char *tile_sm = sm + FW_TILES + g * FW_TILE_BYTES;
+    const uint32_t tile_base = base + FW_TILES + g * FW_TILE_BYTES;
+    const int ntiles = (n + MLP_TILE - 1) / MLP_TILE;
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int tile = blockIdx.x * FW_WG + g; tile < ntiles; tile += gridDim.x * FW_WG) {
+        const int r = tile * MLP_TILE + tl;
+        {
+            const uint4 zero = make_uint4(0, 0, 0, 0);
+#pragma unroll
+            for (int c = 0; c < MLP_IN / 8; ++c)
+                *reinterpret_cast<uint4 *>(tile_sm + FW_X + cm_off(tl, 8 * c, MLP_IN)) =
+                    r < n ? __ldg(reinterpret_cast<const uint4 *>(X + (size_t)r * MLP_IN) + c) : zero;
+        }
+        wg_tc_sync(g);
+        if (tl == 0) {
+            gemm_issue(tm, tile_base + FW_X, base + FW_W1, MLP_IN, MLP_TILE, MLP_H, false);
+            umma_commit(bar);
+        }
+        ok = wg_and(g, mbar_wait(bar, phase));
+        phase ^= 1;
+        if (!ok) break;
         tc_fence_after();
 #pragma unroll 1
-        for (int c0 = c_lo; c0 < c_lo + 64; c0 += 32) {
+        for (int c0 = 0; c0 < MLP_H; c0 += 32) {
             float v[32];
             tmem_ld32(lane_addr + c0, v);
 #pragma unroll
@@ -261,21 +295,20 @@ __global__ void __launch_bounds__(FW_THREADS) k_mlp_forward(const __nv_bfloat16 
                 v[k] = z * sigm(z);
             }
 #pragma unroll
-            for (int g = 0; g < 4; ++g) st8(sm + FW_H1, cm_off(m, c0 + 8 * g, MLP_H), v + 8 * g);
+            for (int q = 0; q < 4; ++q) st8(tile_sm + FW_H1, cm_off(tl, c0 + 8 * q, MLP_H), v + 8 * q);
         }
-    }
-    ok = __syncthreads_and(ok);
-    tc_sync();
-    if (t == 0 && ok) {
-        gemm_issue(tm, base + FW_H1, base + FW_W2, MLP_H, MLP_TILE, MLP_H, false);
-        umma_commit(b);
-    }
-    ok = ok && mbar_wait(b, 1);
-    float acc = 0.f;
-    if (ok) {
+        wg_tc_sync(g);
+        if (tl == 0) {
+            gemm_issue(tm, tile_base + FW_H1, base + FW_W2, MLP_H, MLP_TILE, MLP_H, false);
+            umma_commit(bar);
+        }
+        ok = wg_and(g, mbar_wait(bar, phase));
+        phase ^= 1;
+        if (!ok) break;
         tc_fence_after();
+        float acc = 0.f;
 #pragma unroll 1
-        for (int c0 = c_lo; c0 < c_lo + 64; c0 += 32) {
+        for (int c0 = 0; c0 < MLP_H; c0 += 32) {
             float v[32];
             tmem_ld32(lane_addr + c0, v);
 #pragma unroll
@@ -284,12 +317,7 @@ __global__ void __launch_bounds__(FW_THREADS) k_mlp_forward(const __nv_bfloat16 
                 acc = fmaf(z * sigm(z), sw3[c0 + k], acc);
             }
         }
-    }
-    if (w >= 4) spart[m] = acc;
-    ok = __syncthreads_and(ok);
-    if (ok && w < 4) {
-        const float s = acc + spart[m] + __ldg(wt.b3);
-        const int r = row0 + m;
+        const float s = acc + b3;
         if (r < n) {
             if (out_s) out_s[r] = s;
             if (corr) {
@@ -297,11 +325,13 @@ __global__ void __launch_bounds__(FW_THREADS) k_mlp_forward(const __nv_bfloat16 
                 corr[r] = make_float4(s * vv.x, s * vv.y, s * vv.z, s);
             }
         }
+        // the next tile's first product overwrites this group's accumulator and X
+        wg_tc_sync(g);
     }
-    if (!ok && t == 0) atomicExch(err, 1);
+    if (!ok && tl == 0) atomicExch(err, 1);
     tc_fence_before();
     __syncthreads();
-    if (w == 0) tmem_dealloc(tm, 128);
+    if (w == 0) tmem_dealloc(tmem_base, 128 * FW_WG);
 }
 
 struct MlpGrads {
@@ -621,8 +651,9 @@ int mlp_forward_launch(const pd_mlp *q, const void *X, int n, float *s, const fl
                        cudaStream_t st) {
     if (n <= 0) return PD_OK;
     const int tiles = (n + MLP_TILE - 1) / MLP_TILE;
-    k_mlp_forward<<<tiles, FW_THREADS, FW_BYTES, st>>>(static_cast<const __nv_bfloat16 *>(X), n, mlp_weights(q), s, V,
-                                                         corr, q->err);
+    const int ctas = std::min(sm_count(), (tiles + FW_WG - 1) / FW_WG);
+    k_mlp_forward<<<ctas, FW_THREADS, FW_BYTES, st>>>(static_cast<const __nv_bfloat16 *>(X), n, mlp_weights(q), s, V,
+                                                        corr, q->err);
     PD_LAUNCHED();
     return PD_OK;
 }
