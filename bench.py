@@ -731,7 +731,8 @@ def main():
                "roofline": roofline, "cpu_baseline": cpu,
                "forms": {"plain": {"value": world * ns_per_day(total_ms / args.steps), "unit": "ns/day",
                                    "ms_per_step": total_ms / args.steps,
-                                   "mesh": "SPME 1.0 A (120x120x120), order 5 (the configuration's settings)"},
+                                   "mesh": f"SPME 1.0 A ({'x'.join(str(k) for k in st.solver.mesh)}), order 5 "
+                                           "(the configuration's settings)"},
                          "plain_at_1e-5_vs_ewald": learned.pop("plain_e5") if learned else None,
                          "learned_coarse": learned},
                "e2e": {"value": world * ns_per_day(e2e_ms), "unit": "ns/day", "h2d_bytes_per_step": 24 * n,
