@@ -420,3 +420,51 @@ def baoab_drift(pos, vel, force, inv_mass, box, *, dt, gamma, kT, seed, step):
                       _p(im, _f), float(dt), float(gamma), float(noise), int(seed) & 0xFFFFFFFFFFFFFFFF, int(step),
                       _p(b))
     return np.stack(p[:dim], 1), np.stack(v[:dim], 1)
+
+
+def gjf_step_parts(pos, vel, force, inv_mass, box, *, dt, gamma, kT, seed, step):
+    """Grønbech-Jensen-Farago positions (_gjf_pos_kernel!, src/engine/Langevin.jl:164-181) of Float32 state
+    arrays (N x D): returns (new positions, the draw beta per particle) -- the velocity update
+    (gjf_velocity) takes the same beta.  Coefficients in Float32 as the reference (gjf_pos_coefs,
+    src/engine/Masses.jl:47-56)."""
+    f32 = np.float32
+    pos = np.asarray(pos, f32)
+    n, dim = pos.shape
+    vel = np.asarray(vel, f32)
+    force = np.asarray(force, f32)
+    im = np.broadcast_to(np.asarray(inv_mass, f32), (n,))
+    dt32, g32 = f32(dt), f32(gamma)
+    noise = f32(np.sqrt(2.0 * float(gamma) * float(kT) * float(dt32)))
+    L = np.asarray(box, f32)
+    out = pos.copy()
+    beta = np.zeros((n, dim), f32)
+    for i in range(n):
+        q = f32(g32 * dt32 * im[i] / f32(2))
+        b = f32(f32(1) / (f32(1) + q))
+        coef = f32(b * dt32 * im[i] / f32(2))
+        xi, _ = philox_normals4(seed, step, i + 1, 0)
+        for d in range(dim):
+            beta[i, d] = f32(noise * xi[d])
+            dp = f32(f32(b * dt32) * vel[i, d] + coef * f32(dt32 * force[i, d] + beta[i, d]))
+            x = f32(pos[i, d] + dp)
+            x = f32(x - L[d]) if x >= f32(0.5) * L[d] else x
+            x = f32(x + L[d]) if x < -f32(0.5) * L[d] else x
+            out[i, d] = x
+    return out, beta
+
+
+def gjf_velocity(vel, f_old, f_new, inv_mass, beta, *, dt, gamma):
+    """Grønbech-Jensen-Farago velocities (_gjf_vel_kernel!, src/engine/Langevin.jl:183-208):
+    v = a v + dt/(2m) (a f_old + f_new) + (b/m) beta in FP64 with a, b from Float32 q."""
+    f32 = np.float32
+    vel = np.asarray(vel, np.float64)
+    n = vel.shape[0]
+    im32 = np.broadcast_to(np.asarray(inv_mass, f32), (n,))
+    q = (f32(gamma) * f32(dt) * im32 / f32(2)).astype(f32)
+    a = ((f32(1) - q) / (f32(1) + q)).astype(f32).astype(np.float64)[:, None]
+    b = (f32(1) / (f32(1) + q)).astype(f32).astype(np.float64)[:, None]
+    kf = (float(f32(dt)) * im32.astype(np.float64) / 2.0)[:, None]
+    nf = b * im32.astype(np.float64)[:, None]
+    return (a * vel + kf * (a * np.asarray(f_old, np.float64) + np.asarray(f_new, np.float64))
+            + nf * np.asarray(beta, np.float64)).astype(f32)
+

@@ -905,9 +905,10 @@ struct EllStepArgs {
     float inv_mass_uniform;
     float L[3];
     float dt;
-    // Langevin (BAOAB)
+    // Langevin (BAOAB, GJF)
     float gamma, noise;   // friction and noise scale sqrt(2 gamma kT dt)
     unsigned long long seed;
+    float *f0x, *f0y, *f0z;   // GJF: the previous step's force
     float4 *xq;
     const float4 *ref;
     float threshold;
@@ -943,6 +944,24 @@ __global__ void __launch_bounds__(ELL_THREADS) k_ell_drift(EllStepArgs a, long l
                 v[d] = fmaf(c, f[d], v[d]);
                 p[d] = wrap_half(fmaf(a.dt, v[d], p[d]), a.L[d]);
             }
+        } else if (MODE == 2) {
+            // GJF positions (_gjf_pos_kernel!, Langevin.jl:164-181; gjf_pos_coefs, Masses.jl:47-56):
+            // q = g dt / (2m), b = 1 / (1 + q), x += b dt v + b dt / (2m) (dt f + beta); the force is
+            // kept as the old force of the velocity update
+            const float q = a.gamma * a.dt * im / 2.f;
+            const float b = 1.f / (1.f + q);
+            const float coef = b * a.dt * im / 2.f;
+            float xi[4];
+            philox_normals4(a.seed, (unsigned long long)st[E_STEP], (unsigned)(i + 1), 0u, xi);
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+                const float beta = a.noise * xi[d];
+                const float dp = b * a.dt * v[d] + coef * (a.dt * f[d] + beta);
+                p[d] = wrap_half(p[d] + dp, a.L[d]);
+            }
+            a.f0x[i] = f[0];
+            a.f0y[i] = f[1];
+            if (D == 3) a.f0z[i] = f[2];
         } else {
             const double dt = a.dt, imA = im, g = a.gamma;
             const double hk = dt * imA / 2.0;
@@ -983,6 +1002,33 @@ __global__ void __launch_bounds__(ELL_THREADS) k_ell_drift(EllStepArgs a, long l
     }
 }
 
+// GJF velocities (_gjf_vel_kernel!, Langevin.jl:183-208; gjf_q, gjf_vel_coefs, Masses.jl:58-70):
+// a = (1 - q) / (1 + q), b = 1 / (1 + q), v = a v + dt / (2m) (a f_old + f) + (b / m) beta with the
+// same draw beta as the positions (same device step), in FP64; then the device step advances.
+template <int D>
+__global__ void __launch_bounds__(ELL_THREADS) k_ell_gjf_vel(EllStepArgs a, long long *__restrict__ st) {
+    if (st[E_ERROR] != 0 || st[E_VALID] == 0) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < a.n) {
+        const float im = a.inv_mass ? a.inv_mass[i] : a.inv_mass_uniform;
+        const float q = a.gamma * a.dt * im / 2.f;
+        const double aA = (double)((1.f - q) / (1.f + q)), bA = (double)(1.f / (1.f + q));
+        const double kf = (double)a.dt * (double)im / 2.0, nf = bA * (double)im;
+        float xi[4];
+        philox_normals4(a.seed, (unsigned long long)st[E_STEP], (unsigned)(i + 1), 0u, xi);
+        float *v[3] = {a.vx, a.vy, a.vz};
+        const float *f[3] = {a.fx, a.fy, a.fz};
+        const float *f0[3] = {a.f0x, a.f0y, a.f0z};
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            const double beta = (double)(a.noise * xi[d]);
+            const double vn = aA * (double)v[d][i] + kf * (aA * (double)f0[d][i] + (double)f[d][i]) + nf * beta;
+            v[d][i] = (float)vn;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) st[E_STEP] += 1;
+}
+
 }  // namespace pdb
 
 struct pd_ell_md {
@@ -990,10 +1036,11 @@ struct pd_ell_md {
     pd_md_state st;
     cudaStream_t body = nullptr;
     bool cond_nodes = true;
-    // graphs: [mode (0 NVE, 1 Langevin)][energy]
-    cudaGraphExec_t exec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
-    EllStepArgs key[2][2];
-    cudaStream_t exec_stream[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    // graphs: [mode (0 NVE, 1 Langevin BAOAB, 2 Langevin GJF)][energy]
+    cudaGraphExec_t exec[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+    EllStepArgs key[3][2];
+    cudaStream_t exec_stream[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
+    float *f0 = nullptr;   // GJF old forces, 3 n
 };
 
 namespace pdb {
@@ -1022,6 +1069,11 @@ static EllStepArgs ell_step_args(pd_ell_md *md, float dt, float gamma, float kT,
     a.xq = e->xq;
     a.ref = e->ref;
     a.threshold = e->threshold;
+    if (md->f0) {
+        a.f0x = md->f0;
+        a.f0y = md->f0 + e->n;
+        a.f0z = md->f0 + 2 * (size_t)e->n;
+    }
     return a;
 }
 
@@ -1038,13 +1090,16 @@ static int ell_enqueue_step(pd_ell_md *md, const EllStepArgs &a, int mode, int e
         PD_CUDA(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
     }
 #define PD_ELL_DRIFT(DD, MM, CC) k_ell_drift<DD, MM, CC><<<blocks, ELL_THREADS, 0, s>>>(a, e->st, h)
+#define PD_ELL_DRIFT_D(DD)                                                        \
+    if (mode == 0) { if (cond) PD_ELL_DRIFT(DD, 0, true); else PD_ELL_DRIFT(DD, 0, false); } \
+    else if (mode == 1) { if (cond) PD_ELL_DRIFT(DD, 1, true); else PD_ELL_DRIFT(DD, 1, false); } \
+    else { if (cond) PD_ELL_DRIFT(DD, 2, true); else PD_ELL_DRIFT(DD, 2, false); }
     if (e->dim == 3) {
-        if (mode == 0) { if (cond) PD_ELL_DRIFT(3, 0, true); else PD_ELL_DRIFT(3, 0, false); }
-        else { if (cond) PD_ELL_DRIFT(3, 1, true); else PD_ELL_DRIFT(3, 1, false); }
+        PD_ELL_DRIFT_D(3)
     } else {
-        if (mode == 0) { if (cond) PD_ELL_DRIFT(2, 0, true); else PD_ELL_DRIFT(2, 0, false); }
-        else { if (cond) PD_ELL_DRIFT(2, 1, true); else PD_ELL_DRIFT(2, 1, false); }
+        PD_ELL_DRIFT_D(2)
     }
+#undef PD_ELL_DRIFT_D
 #undef PD_ELL_DRIFT
     PD_LAUNCHED();
     int rc;
@@ -1057,6 +1112,16 @@ static int ell_enqueue_step(pd_ell_md *md, const EllStepArgs &a, int mode, int e
         if ((rc = ell_rebuild_launch(e, md->st.x, md->st.y, md->st.z, s))) return rc;
     }
     EllKick kick;
+    memset(&kick, 0, sizeof kick);
+    if (mode == 2) {
+        // GJF: forces without a kick, then the velocity update (which advances the step)
+        if ((rc = ell_pairs_launch(e, md->st.fx, md->st.fy, md->st.fz, md->st.epot, md->st.vir6, energy, kick, s)))
+            return rc;
+        if (e->dim == 3) k_ell_gjf_vel<3><<<blocks, ELL_THREADS, 0, s>>>(a, e->st);
+        else k_ell_gjf_vel<2><<<blocks, ELL_THREADS, 0, s>>>(a, e->st);
+        PD_LAUNCHED();
+        return PD_OK;
+    }
     kick.vx = md->st.vx;
     kick.vy = md->st.vy;
     kick.vz = md->st.vz;
@@ -1134,10 +1199,11 @@ int pd_ell_md_create(pd_ell_md **out, pd_ell *e, const pd_md_state *st) {
 
 int pd_ell_md_destroy(pd_ell_md *md) {
     if (!md) return PD_OK;
-    for (int m = 0; m < 2; ++m)
+    for (int m = 0; m < 3; ++m)
         for (int k = 0; k < 2; ++k)
             if (md->exec[m][k]) cudaGraphExecDestroy(md->exec[m][k]);
     if (md->body) cudaStreamDestroy(md->body);
+    dfree(md->f0);
     delete md;
     return PD_OK;
 }
@@ -1174,6 +1240,21 @@ int pd_ell_md_langevin(pd_ell_md *md, int nsteps, float dt, float gamma, float k
     PD_CHECK(!energy_last || (md->st.epot && md->st.vir6), PD_EINVAL,
              "pd_ell_md_langevin: energy needs epot and vir6");
     return ell_run(md, 1, nsteps, dt, gamma, kT, seed, energy_last, use_graph, (cudaStream_t)s);
+}
+
+int pd_ell_md_gjf(pd_ell_md *md, int nsteps, float dt, float gamma, float kT, unsigned long long seed,
+                  int energy_last, int use_graph, pd_stream_t s) {
+    PD_CHECK(md, PD_EINVAL, "pd_ell_md_gjf: null handle");
+    PD_CHECK(nsteps >= 0, PD_EINVAL, "pd_ell_md_gjf: negative step count");
+    PD_CHECK(gamma > 0.f && std::isfinite(gamma), PD_EINVAL, "Langevin friction gamma must be positive");
+    PD_CHECK(kT >= 0.f && std::isfinite(kT), PD_EINVAL, "Langevin temperature must be finite and nonnegative");
+    PD_CHECK(!energy_last || (md->st.epot && md->st.vir6), PD_EINVAL, "pd_ell_md_gjf: energy needs epot and vir6");
+    if (!md->f0) {   // host boundary: the old-force storage is allocated on first use
+        int rc = dalloc(&md->f0, 3 * (size_t)md->e->n);
+        if (rc) return rc;
+        PD_CUDA(cudaMemset(md->f0, 0, sizeof(float) * 3 * (size_t)md->e->n));
+    }
+    return ell_run(md, 2, nsteps, dt, gamma, kT, seed, energy_last, use_graph, (cudaStream_t)s);
 }
 
 }  // extern "C"

@@ -551,6 +551,10 @@ class ELLDeviceEngine:
                _stream(stream))
 
     def langevin(self, nsteps: int, dt: float, gamma: float, kT: float, seed: int, energy_last=False,
-                 use_graph=True, stream=None):
-        N.call("pd_ell_md_langevin", self.handle, int(nsteps), float(dt), float(gamma), float(kT),
+                 use_graph=True, stream=None, scheme: str = "baoab"):
+        """Langevin steps: ``scheme`` "baoab" (BAOAB splitting) or "gjf" (Grønbech-Jensen-Farago)."""
+        name = {"baoab": "pd_ell_md_langevin", "gjf": "pd_ell_md_gjf"}.get(scheme)
+        if name is None:
+            raise ValueError(f"unknown Langevin scheme {scheme!r}")
+        N.call(name, self.handle, int(nsteps), float(dt), float(gamma), float(kT),
                int(seed) & 0xFFFFFFFFFFFFFFFF, int(bool(energy_last)), int(bool(use_graph)), _stream(stream))

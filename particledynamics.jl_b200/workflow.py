@@ -152,7 +152,7 @@ class ConstantVolume:
 @dataclass
 class Langevin:
     """Langevin method on a group (the whole system) with friction gamma and bath temperature kT
-    (src/workflow/Integrator.jl:57-66), integrated by BAOAB."""
+    (src/workflow/Integrator.jl:57-66), integrated by BAOAB, or by GJF under the VelocityVerlet scheme."""
     group: object = None
     gamma: float = 1.0
     kT: float = 1.0
@@ -243,6 +243,7 @@ class SimulationState:
         self.epot = torch.zeros(n, **f32)
         self.vir6 = torch.zeros((n, 6 if D == 3 else 3), **f32)
         self.langevin = None
+        self.langevin_scheme = "baoab"
         for m in methods or []:
             if isinstance(m, Langevin):
                 if float(m.gamma) <= 0:
@@ -396,7 +397,8 @@ class SimulationState:
             self.evaluate_forces_into_f(False)
         if self.langevin is not None:
             self.engine.langevin(nsteps, self.dt, self.langevin[0], self.langevin[1], self.seed,
-                                 energy_last=energy_last, use_graph=use_graph, stream=self.stream)
+                                 energy_last=energy_last, use_graph=use_graph, stream=self.stream,
+                                 scheme=self.langevin_scheme)
         else:
             self.engine.step(nsteps, self.dt, energy_last=energy_last, use_graph=use_graph, stream=self.stream)
         self.step_count += nsteps
@@ -449,13 +451,17 @@ class Simulation:
         m = integrator.methods[0]
         if isinstance(m, ConstantVolume) and m.thermostat is not None:
             raise NotImplementedError("thermostats other than Langevin are not part of this build")
-        if isinstance(m, Langevin) and integrator.scheme not in (None, BAOAB) and not isinstance(integrator.scheme,
-                                                                                                  BAOAB):
-            raise NotImplementedError("Langevin integrates with the BAOAB scheme in this build")
+        sch = integrator.scheme
+        vv = sch is VelocityVerlet or isinstance(sch, VelocityVerlet)
+        if isinstance(m, Langevin) and not (sch is None or sch is BAOAB or isinstance(sch, BAOAB) or vv):
+            raise NotImplementedError("Langevin integrates with the BAOAB or the velocity-Verlet (GJF) scheme")
         self.system = system
         self.integrator = integrator
         self.seed = seed
         self.state = SimulationState(system, integrator.forces, integrator.dt, methods=integrator.methods, seed=seed)
+        # Langevin under the velocity-Verlet scheme is the Grønbech-Jensen-Farago integrator
+        # (the reference's Langevin/GJF `velocityverlet` path, IntegratorSpecs.jl:158)
+        self.state.langevin_scheme = "gjf" if vv else "baoab"
 
 
 def state(sim: Simulation) -> SimulationState:

@@ -314,3 +314,45 @@ def test_philox_normals(pd, ora, cuda):
     xi = np.array([ora.philox_normals4(99, 0, i + 1)[0][:2] for i in range(n)])
     assert np.max(np.abs(v - r * noise * xi)) < 1e-5
     torch.cuda.synchronize()
+
+
+def _gjf(pd, seed, n_side=40):
+    """The 2D WCA disks of _system under Langevin with the velocity-Verlet scheme (GJF)."""
+    base = _system(pd, 2, [pd.Langevin(gamma=50.0, kT=1.0)], 2e-4, seed=seed, n_side=n_side)
+    return pd.Simulation(base.system, pd.Integrator(dt=2e-4, forces=base.integrator.forces,
+                                                    methods=[pd.Langevin(gamma=50.0, kT=1.0)],
+                                                    scheme=pd.VelocityVerlet), seed=seed)
+
+
+def test_gjf_step_matches_oracle(pd, ora, cuda):
+    # _gjf_pos_kernel! / _gjf_vel_kernel! (Langevin.jl:164-208): Langevin under the velocity-Verlet scheme
+    sim = _gjf(pd, 321)
+    st = sim.state
+    assert st.langevin_scheme == "gjf"
+    pd.evaluate_forces_into_f(sim)
+    p0, v0, f0 = st.positions(), st.velocities(), st.forces()
+    st.step(1, use_graph=False)
+    p1, v1, f1 = st.positions(), st.velocities(), st.forces()
+    pr, beta = ora.gjf_step_parts(p0, v0, f0, 1.0, st.box, dt=2e-4, gamma=50.0, kT=1.0, seed=321, step=0)
+    assert np.max(np.abs(p1 - pr)) < 1e-5
+    vr = ora.gjf_velocity(v0, f0, f1, 1.0, beta, dt=2e-4, gamma=50.0)
+    assert np.max(np.abs(v1 - vr)) < 1e-5 * max(1.0, np.max(np.abs(vr)))
+    assert st._ell_check()["step"] == 1
+
+
+def test_gjf_temperature_and_graph(pd, cuda):
+    make = lambda seed: _gjf(pd, seed, n_side=32)   # noqa: E731
+    a, b = make(7), make(7)
+    for s in (a, b):
+        pd.evaluate_forces_into_f(s)
+    a.state.step(40, use_graph=True)
+    b.state.step(40, use_graph=False)
+    assert np.max(np.abs(a.state.positions() - b.state.positions())) < 1e-5
+    st = a.state
+    st.step(3000)
+    temps = []
+    for _ in range(20):
+        st.step(100)
+        temps.append(st.kinetic_energy() / st.n)
+    st._ell_check()
+    assert abs(np.mean(temps) - 1.0) < 0.05
