@@ -345,6 +345,10 @@ int pd_ell_md_step(pd_ell_md *md, int nsteps, float dt, int energy_last, int use
  * noise from Philox4x32-10 keyed on (particle id, device step) and seed (src/engine/Philox.jl). */
 int pd_ell_md_langevin(pd_ell_md *md, int nsteps, float dt, float gamma, float kT, unsigned long long seed,
                        int energy_last, int use_graph, pd_stream_t s);
+/* nsteps Langevin BAOA steps (_baoa_kernel!, Langevin.jl:51-80 with kick = 2 dt): B1 with the full
+ * dt, A O A, the forces, no trailing half kick. */
+int pd_ell_md_baoa(pd_ell_md *md, int nsteps, float dt, float gamma, float kT, unsigned long long seed,
+                   int energy_last, int use_graph, pd_stream_t s);
 /* nsteps Langevin steps of the Grønbech-Jensen-Farago velocity-Verlet scheme (_gjf_pos_kernel!,
  * _gjf_vel_kernel!, Langevin.jl:164-208): positions from v, f and beta, the forces, then velocities
  * from the old and new forces and the same beta (Philox on particle id and device step). */

@@ -9,7 +9,7 @@ from . import _native, batch, learned, splits, synthetic  # noqa: F401
 from .engine import (ClusterPairEngine, DeviceEngine, ELLDeviceEngine, ELLEngine, ElectrostaticsSolver,  # noqa: F401
                      ElectrostaticsSpec)
 from .workflow import (  # noqa: F401
-    BAOAB, PME, PPPM, WCA, CellList, ClusterPairList, ConstantVolume, Integrator, Langevin, LennardJones,
+    BAOA, BAOAB, PME, PPPM, WCA, CellList, ClusterPairList, ConstantVolume, Integrator, Langevin, LennardJones,
     ParticleSystem, Simulation, SimulationState, Stage, VelocityVerlet, electrostatics_spec, evaluate_forces_into_f,
     run, state, step,
 )

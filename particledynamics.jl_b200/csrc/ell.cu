@@ -909,6 +909,7 @@ struct EllStepArgs {
     float gamma, noise;   // friction and noise scale sqrt(2 gamma kT dt)
     unsigned long long seed;
     float *f0x, *f0y, *f0z;   // GJF: the previous step's force
+    float kick;               // BAOAB / BAOA: the B1 kick length, dt (BAOAB) or 2 dt (BAOA, no B2)
     float4 *xq;
     const float4 *ref;
     float threshold;
@@ -964,7 +965,7 @@ __global__ void __launch_bounds__(ELL_THREADS) k_ell_drift(EllStepArgs a, long l
             if (D == 3) a.f0z[i] = f[2];
         } else {
             const double dt = a.dt, imA = im, g = a.gamma;
-            const double hk = dt * imA / 2.0;
+            const double hk = (double)a.kick * imA / 2.0;   // kick = dt (BAOAB) or 2 dt (BAOA)
             double v1[3], x1[3];
 #pragma unroll
             for (int d = 0; d < D; ++d) {
@@ -1045,7 +1046,8 @@ struct pd_ell_md {
 
 namespace pdb {
 
-static EllStepArgs ell_step_args(pd_ell_md *md, float dt, float gamma, float kT, unsigned long long seed) {
+static EllStepArgs ell_step_args(pd_ell_md *md, float dt, float gamma, float kT, unsigned long long seed,
+                                 float kick) {
     EllStepArgs a;
     memset(&a, 0, sizeof a);
     pd_ell *e = md->e;
@@ -1066,6 +1068,7 @@ static EllStepArgs ell_step_args(pd_ell_md *md, float dt, float gamma, float kT,
     a.gamma = gamma;
     a.noise = gamma > 0.f ? (float)std::sqrt(2.0 * (double)gamma * (double)kT * (double)dt) : 0.f;
     a.seed = seed;
+    a.kick = kick;
     a.xq = e->xq;
     a.ref = e->ref;
     a.threshold = e->threshold;
@@ -1127,14 +1130,15 @@ static int ell_enqueue_step(pd_ell_md *md, const EllStepArgs &a, int mode, int e
     kick.vz = md->st.vz;
     kick.inv_mass = md->st.inv_mass;
     kick.inv_mass_uniform = md->st.inv_mass_uniform;
-    kick.half_dt = 0.5f * a.dt;
+    // the closing half kick: dt / 2 (NVE, BAOAB), none for BAOA (its B1 kicked the full 2 dt / 2)
+    kick.half_dt = mode == 1 ? 0.5f * (2.f * a.dt - a.kick) : 0.5f * a.dt;
     kick.advance = 1;
     return ell_pairs_launch(e, md->st.fx, md->st.fy, md->st.fz, md->st.epot, md->st.vir6, energy, kick, s);
 }
 
 static int ell_run(pd_ell_md *md, int mode, int nsteps, float dt, float gamma, float kT, unsigned long long seed,
-                   int energy_last, int use_graph, cudaStream_t s) {
-    const EllStepArgs a = ell_step_args(md, dt, gamma, kT, seed);
+                   int energy_last, int use_graph, cudaStream_t s, float kick = 0.f) {
+    const EllStepArgs a = ell_step_args(md, dt, gamma, kT, seed, kick > 0.f ? kick : dt);
     for (int k = 0; k < nsteps; ++k) {
         const int energy = (energy_last && k == nsteps - 1) ? 1 : 0;
         if (!use_graph) {
@@ -1240,6 +1244,16 @@ int pd_ell_md_langevin(pd_ell_md *md, int nsteps, float dt, float gamma, float k
     PD_CHECK(!energy_last || (md->st.epot && md->st.vir6), PD_EINVAL,
              "pd_ell_md_langevin: energy needs epot and vir6");
     return ell_run(md, 1, nsteps, dt, gamma, kT, seed, energy_last, use_graph, (cudaStream_t)s);
+}
+
+int pd_ell_md_baoa(pd_ell_md *md, int nsteps, float dt, float gamma, float kT, unsigned long long seed,
+                   int energy_last, int use_graph, pd_stream_t s) {
+    PD_CHECK(md, PD_EINVAL, "pd_ell_md_baoa: null handle");
+    PD_CHECK(nsteps >= 0, PD_EINVAL, "pd_ell_md_baoa: negative step count");
+    PD_CHECK(gamma > 0.f && std::isfinite(gamma), PD_EINVAL, "Langevin friction gamma must be positive");
+    PD_CHECK(kT >= 0.f && std::isfinite(kT), PD_EINVAL, "Langevin temperature must be finite and nonnegative");
+    PD_CHECK(!energy_last || (md->st.epot && md->st.vir6), PD_EINVAL, "pd_ell_md_baoa: energy needs epot and vir6");
+    return ell_run(md, 1, nsteps, dt, gamma, kT, seed, energy_last, use_graph, (cudaStream_t)s, 2.f * dt);
 }
 
 int pd_ell_md_gjf(pd_ell_md *md, int nsteps, float dt, float gamma, float kT, unsigned long long seed,

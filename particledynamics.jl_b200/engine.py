@@ -552,8 +552,8 @@ class ELLDeviceEngine:
 
     def langevin(self, nsteps: int, dt: float, gamma: float, kT: float, seed: int, energy_last=False,
                  use_graph=True, stream=None, scheme: str = "baoab"):
-        """Langevin steps: ``scheme`` "baoab" (BAOAB splitting) or "gjf" (Grønbech-Jensen-Farago)."""
-        name = {"baoab": "pd_ell_md_langevin", "gjf": "pd_ell_md_gjf"}.get(scheme)
+        """Langevin steps: ``scheme`` "baoab" (BAOAB splitting), "baoa" (BAOA) or "gjf" (Grønbech-Jensen-Farago)."""
+        name = {"baoab": "pd_ell_md_langevin", "baoa": "pd_ell_md_baoa", "gjf": "pd_ell_md_gjf"}.get(scheme)
         if name is None:
             raise ValueError(f"unknown Langevin scheme {scheme!r}")
         N.call(name, self.handle, int(nsteps), float(dt), float(gamma), float(kT),

@@ -166,6 +166,10 @@ class BAOAB:
     """BAOAB Langevin splitting (Integrator.jl:8-9)."""
 
 
+class BAOA:
+    """BAOA Langevin splitting, no trailing half kick (Integrator.jl:10-11)."""
+
+
 @dataclass
 class Integrator:
     dt: float
@@ -453,15 +457,16 @@ class Simulation:
             raise NotImplementedError("thermostats other than Langevin are not part of this build")
         sch = integrator.scheme
         vv = sch is VelocityVerlet or isinstance(sch, VelocityVerlet)
-        if isinstance(m, Langevin) and not (sch is None or sch is BAOAB or isinstance(sch, BAOAB) or vv):
-            raise NotImplementedError("Langevin integrates with the BAOAB or the velocity-Verlet (GJF) scheme")
+        baoa = sch is BAOA or isinstance(sch, BAOA)
+        if isinstance(m, Langevin) and not (sch is None or sch is BAOAB or isinstance(sch, BAOAB) or vv or baoa):
+            raise NotImplementedError("Langevin integrates with the BAOAB, BAOA or velocity-Verlet (GJF) scheme")
         self.system = system
         self.integrator = integrator
         self.seed = seed
         self.state = SimulationState(system, integrator.forces, integrator.dt, methods=integrator.methods, seed=seed)
         # Langevin under the velocity-Verlet scheme is the Grønbech-Jensen-Farago integrator
         # (the reference's Langevin/GJF `velocityverlet` path, IntegratorSpecs.jl:158)
-        self.state.langevin_scheme = "gjf" if vv else "baoab"
+        self.state.langevin_scheme = "gjf" if vv else ("baoa" if baoa else "baoab")
 
 
 def state(sim: Simulation) -> SimulationState:

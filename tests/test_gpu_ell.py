@@ -356,3 +356,22 @@ def test_gjf_temperature_and_graph(pd, cuda):
         temps.append(st.kinetic_energy() / st.n)
     st._ell_check()
     assert abs(np.mean(temps) - 1.0) < 0.05
+
+
+def test_baoa_step_matches_oracle(pd, ora, cuda):
+    # BAOA (_baoa_kernel! with kick = 2 dt, no trailing B): equal to the BAOAB drift started from
+    # v + dt/2 f/m, without the closing half kick
+    base = _system(pd, 2, [pd.Langevin(gamma=50.0, kT=1.0)], 2e-4, seed=77)
+    sim = pd.Simulation(base.system, pd.Integrator(dt=2e-4, forces=base.integrator.forces,
+                                                   methods=[pd.Langevin(gamma=50.0, kT=1.0)], scheme=pd.BAOA),
+                        seed=77)
+    st = sim.state
+    assert st.langevin_scheme == "baoa"
+    pd.evaluate_forces_into_f(sim)
+    p0, v0, f0 = st.positions(), st.velocities(), st.forces()
+    st.step(1, use_graph=False)
+    p1, v1 = st.positions(), st.velocities()
+    vh = (v0 + np.float32(0.5 * 2e-4) * f0).astype(np.float32)
+    pr, vr = ora.baoab_drift(p0, vh, f0, 1.0, st.box, dt=2e-4, gamma=50.0, kT=1.0, seed=77, step=0)
+    assert np.max(np.abs(p1 - pr)) < 1e-5
+    assert np.max(np.abs(v1 - vr)) < 1e-4 * max(1.0, np.max(np.abs(vr)))
