@@ -41,8 +41,9 @@ def _bf16_input(n, seed, cuda):
     return X.to(cuda), X.float().numpy()
 
 
-@pytest.mark.parametrize("n", [1, 127, 1000, 5 * 128])
+@pytest.mark.parametrize("n", [1, 127, 1000, 5 * 128, 100_000])
 def test_mlp_forward_matches_oracle(pd, lo, cuda, n):
+    # 100 000 rows: 782 tiles, more than the 4 x 148 warpgroup slots, so warpgroups take several tiles
     import torch
     net = pd.learned.MLPNetwork(_params(pd, 3))
     X, Xh = _bf16_input(n, 11 + n, cuda)
