@@ -661,8 +661,8 @@ def main():
     # end to end through the C ABI with pinned host buffers: every step copies the state (x, v) in from
     # pinned host memory and copies the stepped state back (the step's result)
     n = st.n
-    hx = torch.empty(3 * n, dtype=torch.float32, pin_memory=True).numpy()
-    hv = torch.empty(3 * n, dtype=torch.float32, pin_memory=True).numpy()
+    hxv = torch.empty(6 * n, dtype=torch.float32, pin_memory=True).numpy()   # positions then velocities
+    hx, hv = hxv[:3 * n], hxv[3 * n:]
     hx[:] = torch.cat([st.x, st.y, st.z]).cpu().numpy()
     hv[:] = torch.cat([st.vx, st.vy, st.vz]).cpu().numpy()
     e2e_steps = max(20, args.steps // 4)

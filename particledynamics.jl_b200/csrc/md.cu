@@ -467,13 +467,21 @@ int pd_md_step_host(pd_md *md, float *host_xyz, float *host_v, int nsteps, float
     pd_md_state &st = md->st;
     const size_t nb = sizeof(float) * (size_t)st.n;
     float *dx[3] = {st.x, st.y, st.z}, *dv[3] = {st.vx, st.vy, st.vz};
-    // one copy per array triple when the caller keeps its components in one block
+    // one copy per array triple when the caller keeps its components in one block, one copy for the
+    // whole state when positions and velocities are adjacent blocks on both sides
     const bool xblock = st.y == st.x + st.n && st.z == st.y + st.n;
     const bool vblock = st.vy == st.vx + st.n && st.vz == st.vy + st.n;
-    for (int d = 0; d < (xblock ? 1 : 3); ++d)
-        PD_CUDA(cudaMemcpyAsync(dx[d], host_xyz + (size_t)d * st.n, xblock ? 3 * nb : nb, cudaMemcpyHostToDevice, s));
-    for (int d = 0; d < (vblock ? 1 : 3); ++d)
-        PD_CUDA(cudaMemcpyAsync(dv[d], host_v + (size_t)d * st.n, vblock ? 3 * nb : nb, cudaMemcpyHostToDevice, s));
+    const bool whole = xblock && vblock && st.vx == st.x + 3 * (size_t)st.n && host_v == host_xyz + 3 * (size_t)st.n;
+    if (whole) {
+        PD_CUDA(cudaMemcpyAsync(st.x, host_xyz, 6 * nb, cudaMemcpyHostToDevice, s));
+    } else {
+        for (int d = 0; d < (xblock ? 1 : 3); ++d)
+            PD_CUDA(cudaMemcpyAsync(dx[d], host_xyz + (size_t)d * st.n, xblock ? 3 * nb : nb, cudaMemcpyHostToDevice,
+                                    s));
+        for (int d = 0; d < (vblock ? 1 : 3); ++d)
+            PD_CUDA(cudaMemcpyAsync(dv[d], host_v + (size_t)d * st.n, vblock ? 3 * nb : nb, cudaMemcpyHostToDevice,
+                                    s));
+    }
     int rc = pd_md_step(md, nsteps, dt, epot_sum ? 1 : 0, 1, sp);
     if (rc) return rc;
     if (epot_sum) {
@@ -482,10 +490,16 @@ int pd_md_step_host(pd_md *md, float *host_xyz, float *host_v, int nsteps, float
         PD_LAUNCHED();
         PD_CUDA(cudaMemcpyAsync(epot_sum, md->esum, sizeof(double), cudaMemcpyDeviceToHost, s));
     }
-    for (int d = 0; d < (xblock ? 1 : 3); ++d)
-        PD_CUDA(cudaMemcpyAsync(host_xyz + (size_t)d * st.n, dx[d], xblock ? 3 * nb : nb, cudaMemcpyDeviceToHost, s));
-    for (int d = 0; d < (vblock ? 1 : 3); ++d)
-        PD_CUDA(cudaMemcpyAsync(host_v + (size_t)d * st.n, dv[d], vblock ? 3 * nb : nb, cudaMemcpyDeviceToHost, s));
+    if (whole) {
+        PD_CUDA(cudaMemcpyAsync(host_xyz, st.x, 6 * nb, cudaMemcpyDeviceToHost, s));
+    } else {
+        for (int d = 0; d < (xblock ? 1 : 3); ++d)
+            PD_CUDA(cudaMemcpyAsync(host_xyz + (size_t)d * st.n, dx[d], xblock ? 3 * nb : nb, cudaMemcpyDeviceToHost,
+                                    s));
+        for (int d = 0; d < (vblock ? 1 : 3); ++d)
+            PD_CUDA(cudaMemcpyAsync(host_v + (size_t)d * st.n, dv[d], vblock ? 3 * nb : nb, cudaMemcpyDeviceToHost,
+                                    s));
+    }
     PD_CUDA(cudaStreamSynchronize(s));
     return PD_OK;
 }

@@ -234,13 +234,13 @@ class SimulationState:
         L = np.array(self.box)
         D = self.dim
         pos = system.positions - L * np.floor(system.positions / L + 0.5)   # centred image
-        # components of one (D, n) block each, so that host transfers of a whole state are single copies
-        self._pos = torch.tensor(np.ascontiguousarray(pos.T), **f32)
-        comp = [self._pos[d] for d in range(D)] + [None] * (3 - D)
-        self.x, self.y, self.z = comp
+        # positions and velocities as the rows of one (2D, n) block, so that host transfers of a whole
+        # state are single copies
         v = system.velocities if system.velocities is not None else np.zeros((n, D))
-        self._vel = torch.tensor(np.ascontiguousarray(np.asarray(v, float).T), **f32)
-        comp = [self._vel[d] for d in range(D)] + [None] * (3 - D)
+        self._xv = torch.tensor(np.ascontiguousarray(np.concatenate([pos.T, np.asarray(v, float).T])), **f32)
+        comp = [self._xv[d] for d in range(D)] + [None] * (3 - D)
+        self.x, self.y, self.z = comp
+        comp = [self._xv[D + d] for d in range(D)] + [None] * (3 - D)
         self.vx, self.vy, self.vz = comp
         comp = [torch.zeros(n, **f32) for _ in range(D)] + [None] * (3 - D)
         self.fx, self.fy, self.fz = comp
