@@ -509,6 +509,79 @@ def run_batch_workload(pd, args, world, rank):
                           "clocks": clk.summary()}))
 
 
+def run_melts_workload(pd, args, world, rank):
+    """64 independent charged melts (N log-uniform in [2 000, 32 000] at 0.0375 ions per cubic Angstrom, the
+    64 000-ion melt's LJ and SPME settings with its 1 A mesh, order 5): each system's captured step replayed
+    on one of 16 streams, so that the systems' latency-bound steps overlap, against the same replays one after
+    another on one stream.  The mesh path is not batched into one launch per stage (one cuFFT plan per mesh
+    size); this measures the concurrent replay of the per-system graphs."""
+    import torch
+    rng = np.random.default_rng(SEED + 64 + rank)
+    ns = [int(round(math.exp(rng.uniform(math.log(2000), math.log(32000))))) for _ in range(args.melts)]
+    ns = [n + (n % 2) for n in ns]   # neutral: half +1, half -1
+    dt = DT_FS / pd.synthetic.TIME_UNIT_FS
+    states = []
+    for k, n in enumerate(ns):
+        L = (n / RHO) ** (1.0 / 3.0)
+        pos, q, box = pd.synthetic.ionic_melt(n, L, 2.2, seed=SEED + 1000 + k)
+        m = pd.synthetic.melt_masses(q)
+        v = pd.synthetic.maxwell_boltzmann(m, T_INIT, seed=SEED + 2000 + k, kB=pd.synthetic.KB_EV)
+        system = pd.ParticleSystem(pos, box, types=["Na", "Cl"], typeids=np.where(q > 0, 1, 2), masses=m,
+                                   charges=q, velocities=v)
+        st = pd.Simulation(system, pd.Integrator(dt=dt, forces=forces(pd, args.buffer, args.prune))).state
+        st.evaluate_forces_into_f(False)
+        states.append(st)
+    total = sum(ns)
+    nstream = 16
+    streams = [torch.cuda.Stream() for _ in range(nstream)]
+
+    def replay(steps, concurrent):
+        # system k always replays on stream k % 16 (its captured graph is bound to that stream); the
+        # sequential replay chains the systems with events, the concurrent one lets them overlap
+        prev = None
+        for _ in range(steps):
+            for k, st in enumerate(states):
+                s = streams[k % nstream]
+                if not concurrent and prev is not None:
+                    s.wait_event(prev)
+                st.engine.step(1, dt, energy_last=False, use_graph=True, stream=s)
+                if not concurrent:
+                    prev = torch.cuda.Event()
+                    prev.record(s)
+
+    replay(args.warmup, True)
+    torch.cuda.synchronize()
+    out = {}
+    for conc in (False, True):
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        t0.record(streams[0])
+        for s in streams[1:]:
+            s.wait_event(t0)
+        replay(args.steps, conc)
+        for s in streams[1:]:
+            ev = torch.cuda.Event()
+            ev.record(s)
+            streams[0].wait_event(ev)
+        t1.record(streams[0])
+        torch.cuda.synchronize()
+        ms = max_over_ranks(world, t0.elapsed_time(t1) / args.steps)
+        out["concurrent" if conc else "sequential"] = {"ms_per_step": ms, "value": world * total * 1000.0 / ms}
+    for st in states:
+        if st.cluster.statistics()["error"]:
+            raise RuntimeError("cluster list error during the melts run")
+    if rank == 0:
+        print(json.dumps({"metric": "atom-steps/s", "value": out["concurrent"]["value"], "unit": "atom-steps/s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": out["concurrent"]["ms_per_step"], "higher_is_better": True,
+                          "scaling": "weak", "dtype": "f32", "data": "synthetic",
+                          "config": {"workload": f"{args.melts} charged melts, N log-uniform [2000, 32000] "
+                                                 f"(total {total}), 0.0375 A^-3, LJ + SPME 1 A order 5, NVE 1 fs",
+                                     "parallelism": f"replicas x{world}", "streams": nstream},
+                          "sequential_replay": out["sequential"]}))
+
+
 def run_reference(args, world, rank):
     """--impl reference: the CPU restatement on the host cores (rank 0 only)."""
     if rank != 0:
@@ -556,8 +629,9 @@ def main():
     ap.add_argument("--buffer", type=float, default=BUFFER, help="cluster list buffer (Angstrom)")
     ap.add_argument("--prune", type=float, default=PRUNE, help="prune buffer (Angstrom)")
     ap.add_argument("--replicas", type=int, default=512, help="replicas of the batch512 workload")
+    ap.add_argument("--melts", type=int, default=64, help="charged melts of the melts64 workload")
     ap.add_argument("--workload", default="melt64k",
-                    choices=["melt64k", "melt512k", "lj1m", "wca2d1m", "lj4k", "batch512"],
+                    choices=["melt64k", "melt512k", "lj1m", "wca2d1m", "lj4k", "batch512", "melts64"],
                     help="melt64k: the headline run; melt512k: the same forms at 512 000 ions (L = 239 A); lj4k / "
                          "lj1m (3D LJ fluid, ELL route, NVE) and wca2d1m (2D WCA disks, ELL route, Langevin) and "
                          "batch512 (batched replicas) time the other configurations (not the headline metric)")
@@ -589,6 +663,9 @@ def main():
     L = pd._native.lib()
     if args.workload == "batch512":
         run_batch_workload(pd, args, world, rank)
+        return
+    if args.workload == "melts64":
+        run_melts_workload(pd, args, world, rank)
         return
     if args.workload not in ("melt64k", "melt512k"):
         run_ell_workload(pd, args, world, rank)
