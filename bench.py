@@ -695,6 +695,11 @@ def main():
             print(json.dumps({"profile": "melt64k eager steps", "steps": args.steps, "warmup": args.warmup,
                               "list": st.cluster.statistics()}))
         return
+    # the pair kernel's CTA shape (parts per super-cluster x warps per part) by the autotuner; the timed
+    # passes accumulated into the slot forces, two evaluations restore the forces
+    tune = st.cluster.autotune_pairs(stream=s)
+    st.evaluate_forces_into_f(False)
+    st.evaluate_forces_into_f(False)
     # kernels of one eager step: the always-run part (the prune kernel included: it is launched every
     # step and returns at once unless the device decision asks for a prune) plus the build kernels, which
     # the captured graph launches only inside its conditional node on steps that rebuild the list
@@ -803,6 +808,8 @@ def main():
                                       f"{'x'.join(str(k) for k in st.solver.mesh)} order 5, NVE dt=1 fs",
                           "form": form, "parallelism": f"replicas x{world}",
                           "list_buffer_A": args.buffer, "prune_buffer_A": args.prune,
+                          "pair_shape": {"nsplit": tune["nsplit"], "warps": tune["warps"],
+                                         "autotune_ms": tune["ms"]},
                           "l2": "flushed (256 MiB write) before every timed step" if not args.no_flush else "warm",
                           "timed_builds": timed_builds, "timed_prunes": timed_prunes},
                "roofline": roofline, "cpu_baseline": cpu,

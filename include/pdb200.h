@@ -125,6 +125,11 @@ int pd_cluster_destroy(pd_cluster *c);
 /* setup!(list, box, rlist, npmax) (List.jl:874-937): size every buffer for this box and
  * request a build.  Host boundary: may reallocate (captured graphs must be recaptured). */
 int pd_cluster_setup(pd_cluster *c, const double box[3]);
+/* Shape of the pair kernel (no reference counterpart; the autotuner's choice): nsplit CTAs per
+ * super-cluster, each splitting the super-cluster's entries, and 1, 2 or 4 warps per CTA taking
+ * entries in turn.  Captured steps re-capture after a change. */
+int pd_cluster_set_pair_shape(pd_cluster *c, int nsplit, int warps);
+int pd_cluster_pair_shape(pd_cluster *c, int *nsplit, int *warps);
 /* ensure_capacity!(list) (List.jl:959-969): after PD_ECAPACITY grow the outer-entry storage to
  * 1.5x (first growth) or 1.25x the required entries plus 1024, and request a build. */
 int pd_cluster_grow(pd_cluster *c);

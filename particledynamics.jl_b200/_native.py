@@ -118,6 +118,8 @@ _SIGS = {
     "pd_cluster_destroy": (C.c_int, [_p]),
     "pd_cluster_setup": (C.c_int, [_p, C.POINTER(C.c_double)]),
     "pd_cluster_grow": (C.c_int, [_p]),
+    "pd_cluster_set_pair_shape": (C.c_int, [_p, C.c_int, C.c_int]),
+    "pd_cluster_pair_shape": (C.c_int, [_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "pd_cluster_request_build": (C.c_int, [_p, _p]),
     "pd_cluster_decide": (C.c_int, [_p, _fp, _fp, _fp, C.c_int, _p]),
     "pd_cluster_build": (C.c_int, [_p, _fp, _fp, _fp, _fp, _fp, C.c_int, _p]),

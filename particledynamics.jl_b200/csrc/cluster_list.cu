@@ -1147,6 +1147,25 @@ int pd_cluster_setup(pd_cluster *c, const double box[3]) {
     return PD_OK;
 }
 
+int pd_cluster_set_pair_shape(pd_cluster *c, int nsplit, int warps) {
+    PD_CHECK(c, PD_EINVAL, "pd_cluster_set_pair_shape: null handle");
+    PD_CHECK(nsplit >= 1 && nsplit <= 64, PD_EINVAL, "pd_cluster_set_pair_shape: parts per super-cluster 1..64");
+    PD_CHECK(warps == 1 || warps == 2 || warps == 4, PD_EINVAL, "pd_cluster_set_pair_shape: warps 1, 2 or 4");
+    if (c->nsplit != nsplit || c->pair_warps != warps) {
+        c->nsplit = nsplit;
+        c->pair_warps = warps;
+        c->shape_epoch += 1;
+    }
+    return PD_OK;
+}
+
+int pd_cluster_pair_shape(pd_cluster *c, int *nsplit, int *warps) {
+    PD_CHECK(c && nsplit && warps, PD_EINVAL, "pd_cluster_pair_shape: null argument");
+    *nsplit = c->nsplit;
+    *warps = c->pair_warps;
+    return PD_OK;
+}
+
 int pd_cluster_grow(pd_cluster *c) {
     PD_CHECK(c, PD_EINVAL, "pd_cluster_grow: null handle");
     int h[W_LEN];

@@ -3,7 +3,7 @@
 // Semantics: _cluster_pair_kernel! and _scatter_kernel! of
 // src/clusterpairs/Kernels.jl (ParticleDynamics.jl) with the pair physics of
 // pair_force (src/clusterpairs/PairFunctor.jl:127-156).  Layout of this
-// library: one 64-thread CTA (two warps) per super-cluster part; thread
+// library: one CTA of 1, 2 or 4 warps (two by default; the tuned shape) per super-cluster part; thread
 // (ti, tj) = (tid & 7, tid >> 3) pairs i-atom ti of each of the 8 i-clusters
 // with j-atom tj of the current j-cluster.  The 64 i-atoms live in shared
 // memory as packed float4 (x, y, z, C q); j-atoms are read as one float4 each,
@@ -57,26 +57,27 @@ __device__ __forceinline__ float horner(const float (&c)[NP], float x) {
 }
 
 template <int LJK, bool COUL, bool ENERGY, int NP>
-__global__ void __launch_bounds__(64) k_pairs(const float4 *__restrict__ xq, const int *__restrict__ ts,
+__global__ void __launch_bounds__(128) k_pairs(const float4 *__restrict__ xq, const int *__restrict__ ts,
                                               const uint2 *__restrict__ cjw, const int *__restrict__ scio,
                                               const int *__restrict__ nw, const int *__restrict__ counts,
                                               const float *__restrict__ lj_table, float4 *__restrict__ fc,
                                               float *__restrict__ vc, int nslot, int nsplit, const PairParams pp) {
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int nwarp = blockDim.x >> 5;   // warps per super-cluster part (1, 2 or 4: the tuned shape)
     const int ti = lane & 7, q = lane >> 3;
     const int S = blockIdx.x / nsplit, part = blockIdx.x % nsplit;
     if (S >= counts[W_NS] || counts[W_ERR] != 0) return;
     __shared__ float4 sxq[SUPER];
     __shared__ int sty[SUPER];
     __shared__ float4 stab[LJK == PD_LJ_TABLE ? PD_MAX_TYPES * PD_MAX_TYPES : 1];
-    {
-        float4 v = xq[S * SUPER + tid];
+    for (int k = tid; k < SUPER; k += blockDim.x) {
+        float4 v = xq[S * SUPER + k];
         if (COUL) v.w *= pp.C;
-        sxq[tid] = v;
+        sxq[k] = v;
+        if (LJK == PD_LJ_TABLE) sty[k] = (ts[S * SUPER + k] - 1) * pp.ntypes;
     }
     if (LJK == PD_LJ_TABLE) {
-        sty[tid] = (ts[S * SUPER + tid] - 1) * pp.ntypes;
-        for (int k = tid; k < pp.ntypes * pp.ntypes; k += SUPER)
+        for (int k = tid; k < pp.ntypes * pp.ntypes; k += blockDim.x)
             stab[k] = reinterpret_cast<const float4 *>(lj_table)[k];
     }
     __syncthreads();
@@ -195,7 +196,7 @@ __global__ void __launch_bounds__(64) k_pairs(const float4 *__restrict__ xq, con
     const int e0 = scio[S], ne = nw[S];
     const int ea = e0 + (int)(((long long)ne * part) / nsplit);
     const int eb = e0 + (int)(((long long)ne * (part + 1)) / nsplit);
-    // The two warps take alternate entries.  Lane (ti, q) pairs i-atom ti of every
+    // The warps take entries in turn.  Lane (ti, q) pairs i-atom ti of every
     // i-cluster in the mask with j-atoms q (j half 0) and q + 4 (j half 1); the next
     // entry's word and j-atoms are loaded while the current one is evaluated.
     const bool gtA = q > ti, gtB = q + 4 > ti;
@@ -208,12 +209,12 @@ __global__ void __launch_bounds__(64) k_pairs(const float4 *__restrict__ xq, con
         ta = ts[(int)ent.x * 8 + q];
         tb = ts[(int)ent.x * 8 + q + 4];
     }
-    for (; e < eb; e += 2) {
+    for (; e < eb; e += nwarp) {
         const uint2 cur = ent;
         const float4 ja = pa, jb = pb;
         const int cta = ta, ctb = tb;
-        if (e + 2 < eb) {
-            ent = cjw[e + 2];
+        if (e + nwarp < eb) {
+            ent = cjw[e + nwarp];
             pa = xq[(int)ent.x * 8 + q];
             pb = xq[(int)ent.x * 8 + q + 4];
             if (LJK == PD_LJ_TABLE) {
@@ -322,9 +323,8 @@ __global__ void k_scatter(const int *__restrict__ perm, int nslot, const int *__
 
 template <int LJK, bool COUL, bool EN, int NP>
 static void launch_pairs(pd_cluster *c, cudaStream_t s) {
-    k_pairs<LJK, COUL, EN, NP><<<c->nsmax * c->nsplit, 64, 0, s>>>(c->xq, c->ts, c->cjw, c->scio, c->nw, c->counts,
-                                                                   c->lj_table, c->fc, c->vc, c->nslot, c->nsplit,
-                                                                   c->pp);
+    k_pairs<LJK, COUL, EN, NP><<<c->nsmax * c->nsplit, 32 * c->pair_warps, 0, s>>>(
+        c->xq, c->ts, c->cjw, c->scio, c->nw, c->counts, c->lj_table, c->fc, c->vc, c->nslot, c->nsplit, c->pp);
 }
 
 template <int LJK, bool EN>

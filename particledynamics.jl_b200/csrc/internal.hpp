@@ -88,6 +88,8 @@ struct pd_cluster {
     bool grown = false;
     bool have_build = false;
     int nsplit = 1;
+    int pair_warps = 2;        // warps per super-cluster part of the pair kernel
+    int shape_epoch = 0;       // incremented when the pair-kernel shape changes (captured steps re-capture)
     int num_sms = 148;
     // device buffers
     int *counts = nullptr;     // W_LEN words

@@ -140,6 +140,40 @@ class ClusterPairEngine:
         N.call("pd_cluster_scatter", self.handle, _ptr(fx), _ptr(fy), _ptr(fz), _ptr(epot), _ptr(vir6), _ptr(q),
                int(bool(energy)), int(bool(add)), _stream(stream))
 
+    def pair_shape(self) -> tuple[int, int]:
+        a, b = C.c_int(), C.c_int()
+        N.call("pd_cluster_pair_shape", self.handle, C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def set_pair_shape(self, nsplit: int, warps: int):
+        N.call("pd_cluster_set_pair_shape", self.handle, int(nsplit), int(warps))
+
+    def autotune_pairs(self, stream=None, reps: int = 20, warps=(1, 2, 4)) -> dict:
+        """Time the pair pass (force only) over CTA shapes -- parts per super-cluster (the default and
+        half / twice it) x warps per part -- and keep the fastest.  The pair pass accumulates into the slot
+        forces, so the caller re-evaluates the forces afterwards."""
+        n0, w0 = self.pair_shape()
+        splits = sorted({max(1, n0 // 2), n0, min(64, 2 * n0)})
+        s = stream if stream is not None else torch.cuda.current_stream()
+        times = {}
+        for ns in splits:
+            for w in warps:
+                self.set_pair_shape(ns, w)
+                with torch.cuda.stream(s):
+                    for _ in range(3):
+                        self.pairs(energy=False, stream=s)
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(s)
+                    for _ in range(reps):
+                        self.pairs(energy=False, stream=s)
+                    b.record(s)
+                b.synchronize()
+                times[(ns, w)] = a.elapsed_time(b) / reps
+        best = min(times, key=times.get)
+        self.set_pair_shape(*best)
+        return {"nsplit": best[0], "warps": best[1], "default": [n0, w0],
+                "ms": {f"{k[0]}x{k[1]}": v for k, v in times.items()}}
+
     def grow(self):
         N.call("pd_cluster_grow", self.handle)
 

@@ -152,3 +152,31 @@ def test_rejects_small_box(pd, cuda):
     with pytest.raises(pd._native.NativeError) as ei:
         _lj_engine(pd, 10, (4.0, 4.0, 4.0), 1.0, 1.0, 2.5)
     assert ei.value.code == pd._native.PD_EINVAL
+
+
+@pytest.mark.parametrize("nsplit,warps", [(1, 1), (3, 4), (7, 2), (2, 1)])
+def test_pair_shapes_agree(pd, cuda, nsplit, warps):
+    # every CTA shape of the pair kernel (parts per super-cluster x warps per part) gives the same forces,
+    # energies and virials (up to the order of the float reductions)
+    n, Lb = 3000, 39.6
+    pos, q, box = pd.synthetic.ionic_melt(n, Lb, 2.2, seed=6)
+    C, rc = pd.synthetic.COULOMB_EV_A, 9.0
+    alpha = pd.splits.alpha_from_tolerance(rc, 1e-5)
+    cp = pd.splits.coulomb_polynomial(alpha, C, rc)
+    table = pd.splits.lj_type_table(2.8, 0.01, rc)
+
+    def run(shape):
+        eng = pd.ClusterPairEngine(n, box, rmax=rc, skin=1.0, prune_buffer=0.3, lj=dict(table=table), coulomb=cp,
+                                   selfc=pd.splits.self_coefficient(alpha))
+        if shape is not None:
+            eng.set_pair_shape(*shape)
+            assert eng.pair_shape() == shape
+        out = _compute(pd, eng, pos, q=q)
+        eng.close()
+        return out
+
+    F0, E0, W0 = run(None)
+    F1, E1, W1 = run((nsplit, warps))
+    assert np.linalg.norm(F1 - F0) <= 1e-6 * np.linalg.norm(F0)
+    assert np.linalg.norm(E1 - E0) <= 1e-6 * np.linalg.norm(E0)
+    assert np.linalg.norm(W1 - W0) <= 1e-6 * np.linalg.norm(W0)
