@@ -427,7 +427,7 @@ def profile_learned(pd, args, system, box, dt):
 
 def run_batch_workload(pd, args, world, rank):
     """512 independent 3D LJ / WCA replicas (N log-uniform in [500, 20 000], density 0.70-0.90, T 0.6-1.2,
-    r_c 2.5 (LJ) or 2^(1/6) (WCA), skin 0.3, NVE dt 0.005) as one batch: one launch per stage over all
+    r_c 2.5 (LJ) or 2^(1/6) (WCA), NVE dt 0.005) as one batch: one launch per stage over all
     replicas, the step captured into one CUDA graph, lanes per row chosen by the autotuner.  Reported:
     aggregate atom-steps/s of the batch and of the loop of single-system ELL engines (one captured step per
     replica, launched one after another on one stream)."""
@@ -439,16 +439,38 @@ def run_batch_workload(pd, args, world, rank):
     systems = pd.batch.make_systems(specs)
     ntot = sum(s["n"] for s in systems)
     dt = 0.005
-    b = pd.batch.BatchedReplicas(systems, skin=0.3)
-    b.evaluate()
     if args.profile:
+        b = pd.batch.BatchedReplicas(systems, skin=0.3)
+        b.evaluate()
         b.step(args.warmup, dt, use_graph=False)
         b.step(args.steps, dt, use_graph=False)
         b.synchronize()
         if rank == 0:
             print(json.dumps({"profile": "batch512 eager steps", "steps": args.steps, "rows": b.status()}))
         return
-    tune = b.autotune_lanes()
+    # autotuner: list skin (rows longer vs rebuilt less often) and lanes per row, each candidate timed on
+    # a short run of this batch
+    trials = {}
+    for skin in (0.3, 0.45, 0.6):
+        bt = pd.batch.BatchedReplicas(systems, skin=skin)
+        bt.evaluate()
+        lanes = bt.autotune_lanes()
+        bt.step(5, dt)
+        bt.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(bt.stream)
+        bt.step(30, dt)
+        a1.record(bt.stream)
+        a1.synchronize()
+        trials[skin] = (a0.elapsed_time(a1) / 30, lanes["lanes"])
+        bt.close()
+        del bt
+        torch.cuda.empty_cache()
+    best_skin = min(trials, key=lambda k: trials[k][0])
+    b = pd.batch.BatchedReplicas(systems, skin=best_skin, lanes=trials[best_skin][1])
+    b.evaluate()
+    tune = {"skin": best_skin, "lanes": b.lanes,
+            "trials_ms": {f"skin {k}, lanes {v[1]}": v[0] for k, v in trials.items()}}
     b.step(args.warmup, dt)
     b.synchronize()
     pre = b.status()
@@ -471,7 +493,8 @@ def run_batch_workload(pd, args, world, rank):
     s = torch.cuda.Stream()
     for sy in systems:
         kw = dict(model="lj", cutoff=2.5) if sy["kind"] == "lj" else dict(model="wca")
-        eng = pd.ELLEngine(sy["n"], sy["box"], skin=0.3, capacity=int(b.cap), interval=100, lanes=b.lanes, **kw)
+        eng = pd.ELLEngine(sy["n"], sy["box"], skin=best_skin, capacity=int(b.cap), interval=100, lanes=b.lanes,
+                           **kw)
         f32 = dict(dtype=torch.float32, device="cuda")
         state = {k: torch.tensor(sy["positions"][:, d], **f32) for d, k in enumerate("xyz")}
         state.update({k: torch.tensor(sy["velocities"][:, d], **f32) for d, k in enumerate(("vx", "vy", "vz"))})
@@ -499,7 +522,8 @@ def run_batch_workload(pd, args, world, rank):
                           "higher_is_better": True, "scaling": "strong", "dtype": "f32", "data": "synthetic",
                           "config": {"workload": f"{args.replicas} LJ/WCA 3D replicas, N log-uniform [500, 20000] "
                                                  f"(total {job_atoms}), rho 0.70-0.90, T 0.6-1.2, r_c 2.5 / 2^(1/6), "
-                                                 "skin 0.3, NVE dt 0.005, one launch per stage over all replicas",
+                                                 f"skin {best_skin} (tuned), NVE dt 0.005, one launch per stage over "
+                                                 "all replicas",
                                      "parallelism": f"replicas split by cost over {world} GPUs",
                                      "rank0_replicas": len(specs), "rank0_atoms": ntot,
                                      "l2": "warm (batch working set per rank)"},
