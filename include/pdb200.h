@@ -350,6 +350,11 @@ int pd_ell_md_step(pd_ell_md *md, int nsteps, float dt, int energy_last, int use
  * noise from Philox4x32-10 keyed on (particle id, device step) and seed (src/engine/Philox.jl). */
 int pd_ell_md_langevin(pd_ell_md *md, int nsteps, float dt, float gamma, float kT, unsigned long long seed,
                        int energy_last, int use_graph, pd_stream_t s);
+/* Langevin bookkeeping (LangevinData.dq / dU / Ekin, Langevin.jl:25-35): n-float device arrays the
+ * Langevin steps accumulate into -- heat exchanged with the bath (dq), work of the forces (dU, the
+ * power v.f of every kick) -- and the per-particle kinetic energy after the step (ekin); all three or
+ * none (NULL detaches). */
+int pd_ell_md_bookkeeping(pd_ell_md *md, float *dq, float *dU, float *ekin);
 /* nsteps Langevin BAOA steps (_baoa_kernel!, Langevin.jl:51-80 with kick = 2 dt): B1 with the full
  * dt, A O A, the forces, no trailing half kick. */
 int pd_ell_md_baoa(pd_ell_md *md, int nsteps, float dt, float gamma, float kT, unsigned long long seed,

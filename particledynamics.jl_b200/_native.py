@@ -163,6 +163,7 @@ _SIGS = {
     "pd_ell_md_langevin": (C.c_int, [_p, C.c_int, C.c_float, C.c_float, C.c_float, C.c_ulonglong, C.c_int,
                                      C.c_int, _p]),
     "pd_ell_md_gjf": (C.c_int, [_p, C.c_int, C.c_float, C.c_float, C.c_float, C.c_ulonglong, C.c_int, C.c_int, _p]),
+    "pd_ell_md_bookkeeping": (C.c_int, [_p, _fp, _fp, _fp]),
     "pd_ell_md_baoa": (C.c_int, [_p, C.c_int, C.c_float, C.c_float, C.c_float, C.c_ulonglong, C.c_int, C.c_int, _p]),
     "pd_mlp_param_count": (C.c_int, []),
     "pd_mlp_create": (C.c_int, [C.POINTER(_p)]),

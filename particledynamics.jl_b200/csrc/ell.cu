@@ -400,6 +400,7 @@ struct EllKick {     // closing half kick fused into the pair kernel (step engin
     const float *inv_mass;
     float inv_mass_uniform, half_dt;
     int advance;     // advance the device step counter (last kernel of a step)
+    float *dU, *ekin;   // Langevin bookkeeping of the closing kick (B2), or null
 };
 
 // Row pair kernel (_pair_cooperative_kernel!, PairTraversal.jl:66-125, with the UniformLJ /
@@ -490,10 +491,17 @@ __global__ void __launch_bounds__(ELL_THREADS) k_ell_pairs(const float4 *__restr
             for (int k = 0; k < NV; ++k) vir[(size_t)i * NV + k] = w[k];
         }
         if (KICK) {
-            const float c = kick.half_dt * (kick.inv_mass ? kick.inv_mass[i] : kick.inv_mass_uniform);
-            kick.vx[i] = fmaf(c, a[0], kick.vx[i]);
-            kick.vy[i] = fmaf(c, a[1], kick.vy[i]);
-            if (D == 3) kick.vz[i] = fmaf(c, a[2], kick.vz[i]);
+            const float im = kick.inv_mass ? kick.inv_mass[i] : kick.inv_mass_uniform;
+            const float c = kick.half_dt * im;
+            const float v0 = fmaf(c, a[0], kick.vx[i]), v1 = fmaf(c, a[1], kick.vy[i]);
+            const float v2 = D == 3 ? fmaf(c, a[2], kick.vz[i]) : 0.f;
+            kick.vx[i] = v0;
+            kick.vy[i] = v1;
+            if (D == 3) kick.vz[i] = v2;
+            if (kick.dU) {   // _b2_kernel! (Langevin.jl:141-160): power v.f and kinetic energy after B2
+                kick.dU[i] += v0 * a[0] + v1 * a[1] + v2 * a[2];
+                kick.ekin[i] = 0.5f * (v0 * v0 + v1 * v1 + v2 * v2) / im;
+            }
         }
     }
     if (KICK && kick.advance && blockIdx.x == 0 && threadIdx.x == 0) st[E_STEP] += 1;
@@ -910,6 +918,7 @@ struct EllStepArgs {
     unsigned long long seed;
     float *f0x, *f0y, *f0z;   // GJF: the previous step's force
     float kick;               // BAOAB / BAOA: the B1 kick length, dt (BAOAB) or 2 dt (BAOA, no B2)
+    float *dq, *dU, *ekin;    // Langevin bookkeeping (heat, work of the forces, kinetic energy), or null
     float4 *xq;
     const float4 *ref;
     float threshold;
@@ -966,22 +975,31 @@ __global__ void __launch_bounds__(ELL_THREADS) k_ell_drift(EllStepArgs a, long l
         } else {
             const double dt = a.dt, imA = im, g = a.gamma;
             const double hk = (double)a.kick * imA / 2.0;   // kick = dt (BAOAB) or 2 dt (BAOA)
-            double v1[3], x1[3];
+            double v1[3], x1[3], pw = 0.0;
 #pragma unroll
             for (int d = 0; d < D; ++d) {
                 v1[d] = (double)v[d] + hk * (double)f[d];        // B1
                 x1[d] = (double)p[d] + 0.5 * dt * v1[d];         // A1
+                pw += v1[d] * (double)f[d];
             }
             const double c = exp(-g * dt * imA);
             const double rr = sqrt((1.0 - c * c) * imA / (2.0 * g * dt));
             float xi[4];
             philox_normals4(a.seed, (unsigned long long)st[E_STEP], (unsigned)(i + 1), 0u, xi);
+            double vb2 = 0.0, vbb = 0.0;
 #pragma unroll
             for (int d = 0; d < D; ++d) {
                 const double beta = (double)(a.noise * xi[d]);
                 const double v2 = c * v1[d] + rr * beta;         // O
+                const double vbar = 0.5 * (v1[d] + v2);
+                vb2 += vbar * vbar;
+                vbb += vbar * beta;
                 v[d] = (float)v2;
                 p[d] = wrap_half((float)(x1[d] + 0.5 * dt * v2), a.L[d]);   // A2
+            }
+            if (a.dq) {   // _baoa_kernel! (Langevin.jl:58-78): dU += v1.f after B1, dq += -g |vbar|^2 + vbar.beta / dt
+                a.dU[i] += (float)pw;
+                a.dq[i] += (float)(-g * vb2 + vbb / dt);
             }
         }
         a.x[i] = p[0];
@@ -1020,11 +1038,22 @@ __global__ void __launch_bounds__(ELL_THREADS) k_ell_gjf_vel(EllStepArgs a, long
         float *v[3] = {a.vx, a.vy, a.vz};
         const float *f[3] = {a.fx, a.fy, a.fz};
         const float *f0[3] = {a.f0x, a.f0y, a.f0z};
+        double v2 = 0.0, psto = 0.0, pcons = 0.0;
 #pragma unroll
         for (int d = 0; d < D; ++d) {
             const double beta = (double)(a.noise * xi[d]);
-            const double vn = aA * (double)v[d][i] + kf * (aA * (double)f0[d][i] + (double)f[d][i]) + nf * beta;
+            const double vp = (double)v[d][i];
+            const double vn = aA * vp + kf * (aA * (double)f0[d][i] + (double)f[d][i]) + nf * beta;
+            v2 += vn * vn;
+            psto += 0.5 * (vp + vn) * (beta / bA);
+            pcons += vn * (double)f[d][i];
             v[d][i] = (float)vn;
+        }
+        if (a.dq) {   // P_diss = -g |v|^2, P_sto = vbar.(beta / b) / dt, P_cons = v.f (Langevin.jl:199-206)
+            const double g = a.gamma;
+            a.ekin[i] = (float)(0.5 * v2 / (double)im);
+            a.dq[i] -= (float)(-g * v2 + psto / (double)a.dt);
+            a.dU[i] += (float)pcons;
         }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) st[E_STEP] += 1;
@@ -1042,6 +1071,7 @@ struct pd_ell_md {
     EllStepArgs key[3][2];
     cudaStream_t exec_stream[3][2] = {{nullptr, nullptr}, {nullptr, nullptr}, {nullptr, nullptr}};
     float *f0 = nullptr;   // GJF old forces, 3 n
+    float *dq = nullptr, *dU = nullptr, *ekin = nullptr;   // caller-owned Langevin bookkeeping, or null
 };
 
 namespace pdb {
@@ -1069,6 +1099,11 @@ static EllStepArgs ell_step_args(pd_ell_md *md, float dt, float gamma, float kT,
     a.noise = gamma > 0.f ? (float)std::sqrt(2.0 * (double)gamma * (double)kT * (double)dt) : 0.f;
     a.seed = seed;
     a.kick = kick;
+    if (gamma > 0.f) {
+        a.dq = md->dq;
+        a.dU = md->dU;
+        a.ekin = md->ekin;
+    }
     a.xq = e->xq;
     a.ref = e->ref;
     a.threshold = e->threshold;
@@ -1130,6 +1165,10 @@ static int ell_enqueue_step(pd_ell_md *md, const EllStepArgs &a, int mode, int e
     kick.vz = md->st.vz;
     kick.inv_mass = md->st.inv_mass;
     kick.inv_mass_uniform = md->st.inv_mass_uniform;
+    if (mode == 1) {
+        kick.dU = a.dU;
+        kick.ekin = a.ekin;
+    }
     // the closing half kick: dt / 2 (NVE, BAOAB), none for BAOA (its B1 kicked the full 2 dt / 2)
     kick.half_dt = mode == 1 ? 0.5f * (2.f * a.dt - a.kick) : 0.5f * a.dt;
     kick.advance = 1;
@@ -1244,6 +1283,16 @@ int pd_ell_md_langevin(pd_ell_md *md, int nsteps, float dt, float gamma, float k
     PD_CHECK(!energy_last || (md->st.epot && md->st.vir6), PD_EINVAL,
              "pd_ell_md_langevin: energy needs epot and vir6");
     return ell_run(md, 1, nsteps, dt, gamma, kT, seed, energy_last, use_graph, (cudaStream_t)s);
+}
+
+int pd_ell_md_bookkeeping(pd_ell_md *md, float *dq, float *dU, float *ekin) {
+    PD_CHECK(md, PD_EINVAL, "pd_ell_md_bookkeeping: null handle");
+    PD_CHECK((dq && dU && ekin) || (!dq && !dU && !ekin), PD_EINVAL,
+             "pd_ell_md_bookkeeping: give all three arrays or none");
+    md->dq = dq;
+    md->dU = dU;
+    md->ekin = ekin;
+    return PD_OK;
 }
 
 int pd_ell_md_baoa(pd_ell_md *md, int nsteps, float dt, float gamma, float kT, unsigned long long seed,

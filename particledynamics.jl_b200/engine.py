@@ -584,6 +584,12 @@ class ELLDeviceEngine:
         N.call("pd_ell_md_step", self.handle, int(nsteps), float(dt), int(bool(energy_last)), int(bool(use_graph)),
                _stream(stream))
 
+    def bookkeeping(self, dq=None, dU=None, ekin=None):
+        """Attach (or detach) the Langevin bookkeeping arrays: heat dq, force work dU (accumulated) and the
+        kinetic energy after each step, n floats each."""
+        N.call("pd_ell_md_bookkeeping", self.handle, _ptr(dq), _ptr(dU), _ptr(ekin))
+        self._bookkeeping = (dq, dU, ekin)
+
     def langevin(self, nsteps: int, dt: float, gamma: float, kT: float, seed: int, energy_last=False,
                  use_graph=True, stream=None, scheme: str = "baoab"):
         """Langevin steps: ``scheme`` "baoab" (BAOAB splitting), "baoa" (BAOA) or "gjf" (Grønbech-Jensen-Farago)."""

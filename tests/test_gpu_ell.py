@@ -375,3 +375,44 @@ def test_baoa_step_matches_oracle(pd, ora, cuda):
     pr, vr = ora.baoab_drift(p0, vh, f0, 1.0, st.box, dt=2e-4, gamma=50.0, kT=1.0, seed=77, step=0)
     assert np.max(np.abs(p1 - pr)) < 1e-5
     assert np.max(np.abs(v1 - vr)) < 1e-4 * max(1.0, np.max(np.abs(vr)))
+
+
+def test_langevin_bookkeeping(pd, ora, cuda):
+    # dq, dU, Ekin of one BAOAB step (_baoa_kernel! and _b2_kernel!, Langevin.jl:58-78, 141-160)
+    import torch
+    sim = _system(pd, 2, [pd.Langevin(gamma=50.0, kT=1.0)], 2e-4, seed=5)
+    st = sim.state
+    pd.evaluate_forces_into_f(sim)
+    n = st.n
+    dq, dU, ek = (torch.zeros(n, device="cuda") for _ in range(3))
+    st.engine.bookkeeping(dq, dU, ek)
+    p0, v0, f0 = st.positions(), st.velocities().astype(np.float64), st.forces().astype(np.float64)
+    st.step(1, use_graph=False)
+    v1f, f1 = st.velocities().astype(np.float64), st.forces().astype(np.float64)
+    dt, g, kT = 2e-4, 50.0, 1.0
+    noise = np.float32(np.sqrt(2.0 * g * kT * float(np.float32(dt))))
+    xi = np.stack([ora.philox_normals4(5, 0, i + 1, 0)[0][:2] for i in range(n)])
+    beta = (noise * xi.astype(np.float32)).astype(np.float64)
+    dt64 = float(np.float32(dt))
+    vb1 = v0 + 0.5 * dt64 * f0
+    c = np.exp(-g * dt64)
+    rr = np.sqrt((1.0 - c * c) / (2.0 * g * dt64))
+    v2 = c * vb1 + rr * beta
+    vbar = 0.5 * (vb1 + v2)
+    dq_ref = -g * (vbar * vbar).sum(1) + (vbar * beta).sum(1) / dt64
+    dU_ref = (vb1 * f0).sum(1) + (v1f * f1).sum(1)
+    ek_ref = 0.5 * (v1f * v1f).sum(1)
+    rel = lambda a, b: np.linalg.norm(a - b) / np.linalg.norm(b)   # noqa: E731
+    assert rel(dq.double().cpu().numpy(), dq_ref) < 1e-4
+    assert rel(dU.double().cpu().numpy(), dU_ref) < 1e-4
+    assert rel(ek.double().cpu().numpy(), ek_ref) < 1e-5
+    # GJF: the kinetic energy after the velocity update
+    sim2 = _gjf(pd, 9)
+    st2 = sim2.state
+    pd.evaluate_forces_into_f(sim2)
+    q2, u2, k2 = (torch.zeros(st2.n, device="cuda") for _ in range(3))
+    st2.engine.bookkeeping(q2, u2, k2)
+    st2.step(3, use_graph=False)
+    v = st2.velocities().astype(np.float64)
+    assert rel(k2.double().cpu().numpy(), 0.5 * (v * v).sum(1)) < 1e-5
+    assert np.all(np.isfinite(q2.cpu().numpy())) and np.abs(u2.cpu().numpy()).sum() > 0
