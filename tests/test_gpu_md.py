@@ -41,7 +41,7 @@ def test_melt_forces_energy_virial(pd, ora, cuda, kind):
     ref = _oracle_forces(pd, ora, sim, q, box, kind="spme" if kind == "PME" else "p3m_ad")
     F = st.forces()
     rel = np.linalg.norm(F - ref["F"]) / np.linalg.norm(ref["F"])
-    assert rel < 1e-5, rel                              # the north-star parity bound (relative RMS)
+    assert rel < 1e-5, rel                              # the parity bound: 1e-5 relative RMS force
     E = st.potential_energy()
     assert abs(E - ref["Etot"]) / abs(ref["Etot"]) < 1e-5
     W = st.virial_tensor()
