@@ -366,7 +366,7 @@ int pd_ell_md_gjf(pd_ell_md *md, int nsteps, float dt, float gamma, float kT, un
                   int energy_last, int use_graph, pd_stream_t s);
 
 /* ------------------------------------------------------------------------------------------
- * Learned coarse-mesh correction (no reference counterpart: an added form judged against the
+ * Learned coarse-mesh correction (no reference counterpart: an added form compared with the
  * plain fine-mesh PME above).  PME runs on a 2x coarser mesh; a 32-128-128-1 SiLU network
  * (BF16 tensor cores, FP32 accumulation) maps each particle's local charge descriptors to a
  * scalar s_i, and the force residual is F_i = s_i V_i with

@@ -1,7 +1,7 @@
 """CPU oracle of the learned coarse-mesh correction -- TEST INFRASTRUCTURE ONLY.
 
-The learned form has no counterpart in ParticleDynamics.jl (it is an added force term judged
-against the plain fine-mesh PME), so there is no reference code or golden vector to restate:
+The learned form has no counterpart in ParticleDynamics.jl (it is an added force term compared
+with the plain fine-mesh PME), so there is no reference code or golden vector to restate:
 parity unpinned against the reference.  The restatement below is pinned instead by
 
 * central finite differences of the exact-arithmetic network (``mlp_grads`` with

@@ -1,6 +1,6 @@
 """Learned coarse-mesh correction: host side of ``mlp.cu``, ``learned.cu`` and ``ewald.cu``.
 
-The reference has no learned form; this is an added force term judged against the plain
+The reference has no learned form; this is an added force term compared with the plain
 fine-mesh PME of the same system.  PME runs on a mesh twice as coarse (2.0 A, order 4 instead of
 1.0 A, order 5) and the force residual of the coarse mesh is predicted per particle:
 
