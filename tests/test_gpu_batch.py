@@ -109,3 +109,29 @@ def test_batch_autotuner_picks_a_candidate(pd, cuda):
     res = b.autotune_lanes()
     assert res["lanes"] in (1, 2, 4, 8) and set(res["ms"]) == {1, 2, 4, 8}
     assert b.lanes == res["lanes"]
+
+
+def test_batch_sparse_and_small_replicas(pd, ora, cuda):
+    # a dilute replica (a few particles per cell) and the smallest box the list radius allows (three
+    # cells per dimension, the stencil spans the whole box) next to a dense one
+    import torch
+    rng = np.random.default_rng(3)
+    systems = []
+    for n, L, kind in ((40, 12.0, "lj"), (60, 5.7, "wca"), (700, 9.5, "lj")):
+        pos = rng.uniform(-L / 2, L / 2, (n, 3))
+        if n == 700:
+            pos, box = pd.synthetic.fcc_fill(n, 0.8, seed=4)
+            L = box[0]
+        systems.append(dict(n=n, box=(L, L, L), kind=kind, positions=pos, velocities=np.zeros((n, 3)), masses=1.0))
+    b = pd.batch.BatchedReplicas(systems, skin=0.3, cap=160)
+    b.evaluate(energy=True)
+    st = b.status()
+    assert st["error"] == 0 and st["valid"] == 1
+    for k, s in enumerate(systems):
+        pos = np.stack([b.replica(k, t).cpu().numpy() for t in (b.x, b.y, b.z)], 1).astype(np.float64)
+        kw = dict(kind=1, sigma=1.0, eps=1.0, rc_lj=2.5) if s["kind"] == "lj" else \
+            dict(kind=2, sigma=1.0, eps=1.0, rc_lj=float(np.sqrt(np.float32(1.2599211))))
+        ref = ora.pairs_direct(pos, s["box"], **kw)
+        F = torch.stack([b.replica(k, t) for t in (b.fx, b.fy, b.fz)], 1).double().cpu().numpy()
+        scale = max(np.linalg.norm(ref["F"]), 1e-12)
+        assert np.linalg.norm(F - ref["F"]) <= 2e-5 * scale + 1e-6, (k, s["kind"])

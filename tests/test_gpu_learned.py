@@ -256,3 +256,29 @@ def test_trained_network_beats_the_coarse_mesh(pd, cuda):
     assert e["fine"] < e["coarse"]
     assert e["learned"] < 0.95 * e["coarse"]
     assert e["learned"] <= 1.02 * e["radial"]
+
+
+def test_descriptors_of_isolated_and_sparse_ions(pd, lo, cuda):
+    # an ion with no neighbour inside the cutoff has zero features and a zero residual direction; a
+    # sparse system (few ions per row) still matches the direct pair loop
+    import torch
+    L = 40.0
+    pos = np.array([[0.0, 0.0, 0.0], [15.0, 15.0, 15.0], [17.5, 15.0, 15.0], [-15.0, 12.0, 3.0],
+                    [-13.0, 13.0, 4.0], [5.0, -18.0, 9.0]])
+    q = np.array([1.0, -1.0, 1.0, -1.0, 1.0, -1.0])
+    typ = np.where(q > 0, 1, 2).astype(np.int32)
+    box = (L, L, L)
+    n = len(pos)
+    lc = pd.learned.LearnedCorrection(n, box, cap=8)
+    lc.set_radial(np.linspace(0.5, -0.5, lc.nb))
+    t = [torch.tensor(pos[:, d], dtype=torch.float32, device=cuda) for d in range(3)]
+    X, V = lc.descriptors(*t, torch.tensor(q, dtype=torch.float32, device=cuda), torch.tensor(typ, device=cuda))
+    cfg = lc.cfg
+    Xr, Vr, _ = lo.descriptors(pos.astype(np.float32), q, typ, box, rcut=cfg["rcut"], mu0=cfg["mu0"],
+                               dmu=cfg["dmu"], sigma=cfg["sigma"], nb=cfg["nb"], nu0=cfg["nu0"], dnu=cfg["dnu"],
+                               tau=cfg["tau"], coef=lc.coef)
+    Xg, Vg = X.float().cpu().numpy(), V.cpu().numpy()[:, :3]
+    for i in (0, 5):   # no neighbour within 6 A
+        assert not Xg[i].any() and not Vg[i].any()
+    assert np.all(np.abs(Xg - Xr) <= 2.0 ** -7 * np.abs(Xr) + 1e-4)
+    assert np.allclose(Vg, Vr, rtol=2e-5, atol=1e-6)
