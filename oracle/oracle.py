@@ -242,6 +242,34 @@ def mesh(pos, q, box, K, P, kind="spme", alpha=1.0, C=1.0, nmax=2, background=Fa
     return dict(F=F.reshape(n, 3), E=E, Emesh=Emesh, W=Wm, phi=phi, ubg=ubg)
 
 
+def mesh_source_forces(pos, q, box, K, P, tables, sources, workers=1):
+    """Mesh force (AD gather) on every particle from each source charge alone: (len(sources), n, 3).
+
+    The mesh part is linear in the charges, so summing over all sources gives ``mesh(...)["F"]``; the
+    source's own row entry is its self force through the mesh (zero for the exact reciprocal sum).
+    """
+    L = _load()
+    K = np.ascontiguousarray(K, np.int32)
+    x, y, z = _xyz(pos)
+    n = len(x)
+    qq = np.ascontiguousarray(q, np.float64)
+    b = _box(box)
+    G = tables[0]
+    out = np.zeros((len(sources), n, 3))
+    for s, j in enumerate(sources):
+        grid = np.zeros(int(K[0]) * int(K[1]) * int(K[2]))
+        xs, ys, zs = (np.ascontiguousarray(a[j:j + 1]) for a in (x, y, z))
+        L.ora_spread(1, _p(xs), _p(ys), _p(zs), _p(np.ascontiguousarray(qq[j:j + 1])), _p(b), _p(K, _i), int(P),
+                     _p(grid))
+        spec = _rfft(grid, K, workers)
+        pot = _irfft(spec * G.reshape(spec.shape), K, workers)
+        F = np.zeros(3 * n)
+        phi = np.zeros(n)
+        L.ora_gather_ad(n, _p(x), _p(y), _p(z), _p(qq), _p(b), _p(K, _i), int(P), _p(pot), _p(F), _p(phi))
+        out[s] = F.reshape(n, 3)
+    return out
+
+
 def pme_total(pos, q, box, *, C, alpha, rc, K, P, kind="spme", nmax=2, lj=None, workers=1):
     """Total (real space + mesh + self) forces, energy and virial of a charged system in FP64.
 
