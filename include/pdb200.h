@@ -241,6 +241,16 @@ int pd_mesh_energy(pd_mesh *m, double out7[7], pd_stream_t s);
 int pd_mesh_influence(pd_mesh *m, float *G, float *Vc);
 /* Mesh dimensions and mode count. */
 int pd_mesh_dims(pd_mesh *m, int mesh[3], int *nmodes);
+/* Self-force removal (no counterpart in the reference; off by default, so the mesh forces stay the
+ * reference's): the AD gather subtracts q_i^2 S(u_i), the force that particle i receives through the
+ * mesh from its own charge, interpolated trilinearly from a table of S at table_size^3 fractional
+ * grid positions.  The table comes from the mesh's own influence function and is recomputed by
+ * pd_mesh_set_box.  table_size 0 turns it off; 4..64 otherwise.  Energies are unchanged.
+ * PD_ENOTSUP for ik differentiation. */
+int pd_mesh_set_self_force_removal(pd_mesh *m, int table_size);
+/* Host copy of the table (4 floats per entry, x fastest: entry (t1 + T (t2 + T t3)) is S at grid
+ * coordinates (t1, t2, t3) / T per unit charge squared) and its size T (0 when off); out4 may be NULL. */
+int pd_mesh_self_force_table(pd_mesh *m, float *out4, int *table_size);
 
 /* ======================================================================
  * Device step engine: the captured per-step graph of the reference's device engine

@@ -143,6 +143,8 @@ _SIGS = {
     "pd_mesh_energy": (C.c_int, [_p, C.POINTER(C.c_double), _p]),
     "pd_mesh_influence": (C.c_int, [_p, _p, _p]),
     "pd_mesh_dims": (C.c_int, [_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "pd_mesh_set_self_force_removal": (C.c_int, [_p, C.c_int]),
+    "pd_mesh_self_force_table": (C.c_int, [_p, _p, C.POINTER(C.c_int)]),
     "pd_md_create": (C.c_int, [C.POINTER(_p), _p, _p, C.POINTER(MDState), C.POINTER(C.c_double)]),
     "pd_md_destroy": (C.c_int, [_p]),
     "pd_md_evaluate": (C.c_int, [_p, C.c_int, _p]),

@@ -142,6 +142,9 @@ struct pd_mesh {
     void *work = nullptr;
     size_t work_size = 0;
     cudaStream_t plan_stream = nullptr;
+    float4 *self_tab = nullptr; // self-force table (T^3 samples of the fractional position), or null
+    int self_T = 0;
+    int epoch = 0;              // bumped when a change needs captured steps to be captured again
 };
 
 namespace pdb {

@@ -36,6 +36,7 @@ struct pd_md {
     float exec_dt[2] = {0.f, 0.f};
     cudaStream_t exec_stream[2] = {nullptr, nullptr};
     int exec_epoch[2] = {-1, -1};   // pair-kernel shape the graphs were captured with
+    int exec_mepoch[2] = {-1, -1};  // mesh epoch the graphs were captured with
     double *esum = nullptr;   // device FP64 energy sum
     float half_c_self = 0.f;
     // learned coarse-mesh correction: descriptors + network on a third stream
@@ -431,7 +432,7 @@ int pd_md_step(pd_md *md, int nsteps, float dt, int energy_last, int use_graph, 
             continue;
         }
         if (!md->exec[energy] || md->exec_dt[energy] != dt || md->exec_stream[energy] != s ||
-            md->exec_epoch[energy] != md->c->shape_epoch) {
+            md->exec_epoch[energy] != md->c->shape_epoch || (md->m && md->exec_mepoch[energy] != md->m->epoch)) {
             if (md->exec[energy]) {
                 cudaGraphExecDestroy(md->exec[energy]);
                 md->exec[energy] = nullptr;
@@ -458,6 +459,7 @@ int pd_md_step(pd_md *md, int nsteps, float dt, int energy_last, int use_graph, 
             md->exec_dt[energy] = dt;
             md->exec_stream[energy] = s;
             md->exec_epoch[energy] = md->c->shape_epoch;
+            if (md->m) md->exec_mepoch[energy] = md->m->epoch;
         }
         PD_CUDA(cudaGraphLaunch(md->exec[energy], s));
     }

@@ -382,7 +382,38 @@ struct GatherOut {
     float half_c_self;       // JOIN energy: 0.5 C selfc
     float bg;                // background potential per unit charge
     const float4 *extra;     // JOIN: per-particle force added before the kick (learned correction), or null
+    const float4 *self_tab;  // self-force table of the mesh (T^3), or null: no self-force removal
+    int self_T;
 };
+
+// Spurious self force of a unit charge at grid coordinates (u1, u2, u3): trilinear interpolation of
+// the table sampled at the fractional positions t / T (t = 0 .. T-1) on each axis; the self force is
+// periodic with period one node on every axis.
+__device__ __forceinline__ float4 self_force(const float4 *__restrict__ tab, int T, float u1, float u2, float u3) {
+    int i[3], j[3];
+    float t[3];
+    const float u[3] = {u1, u2, u3};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const float f = (u[d] - floorf(u[d])) * (float)T;
+        int a = (int)f;
+        a = a < 0 ? 0 : (a >= T ? T - 1 : a);
+        i[d] = a;
+        j[d] = a + 1 == T ? 0 : a + 1;
+        t[d] = f - (float)a;
+    }
+    float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const int a1 = (c & 1) ? j[0] : i[0], a2 = (c & 2) ? j[1] : i[1], a3 = (c & 4) ? j[2] : i[2];
+        const float w = ((c & 1) ? t[0] : 1.f - t[0]) * ((c & 2) ? t[1] : 1.f - t[1]) * ((c & 4) ? t[2] : 1.f - t[2]);
+        const float4 v = __ldg(tab + ((size_t)a3 * T + a2) * T + a1);
+        r.x = fmaf(w, v.x, r.x);
+        r.y = fmaf(w, v.y, r.y);
+        r.z = fmaf(w, v.z, r.z);
+    }
+    return r;
+}
 
 template <int P, int MODE, bool ENERGY>   // MODE 0: add, 1: set, 2: join (+ kick)
 __global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_gather(const float4 *__restrict__ xq, int nchunks,
@@ -416,10 +447,14 @@ __global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_gather(const
     }
     float w1[P], w2[P], w3[P], g1[P], g2[P], g3[P];
     int k1 = 0, k2 = 0, k3 = 0;
+    float u1 = 0.f, u2 = 0.f, u3 = 0.f;
     if (charged) {
-        k1 = bspline<P>(grid_coordinate(v.x, Lx, K1), w1, g1);
-        k2 = bspline<P>(grid_coordinate(v.y, Ly, K2), w2, g2);
-        k3 = bspline<P>(grid_coordinate(v.z, Lz, K3), w3, g3);
+        u1 = grid_coordinate(v.x, Lx, K1);
+        u2 = grid_coordinate(v.y, Ly, K2);
+        u3 = grid_coordinate(v.z, Lz, K3);
+        k1 = bspline<P>(u1, w1, g1);
+        k2 = bspline<P>(u2, w2, g2);
+        k3 = bspline<P>(u3, w3, g3);
     }
     int d1 = 0, d2 = 0, d3 = 0;
     Brick b;
@@ -508,6 +543,13 @@ __global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_gather(const
         Fy = -(qi * gy * ((float)K2 / Ly));
         Fz = -(qi * gz * ((float)K3 / Lz));
         if (ENERGY) Ei = 0.5f * qi * phi + o.bg * qi;
+        if (o.self_tab) {   // remove the charge's own force through the mesh: F -= q^2 S(u)
+            const float4 sf = self_force(o.self_tab, o.self_T, u1, u2, u3);
+            const float q2 = qi * qi;
+            Fx = fmaf(-q2, sf.x, Fx);
+            Fy = fmaf(-q2, sf.y, Fy);
+            Fz = fmaf(-q2, sf.z, Fz);
+        }
     }
     if (MODE == 2) {
         if (id < 0) return;
@@ -603,6 +645,43 @@ __global__ void k_gather_ik(const float4 *__restrict__ xq, int n, const int *__r
 }
 
 // Particles of `order` packed as (x, y, z, q) in chunks of 64 (zero-charge padding).
+// Self-force table: a unit charge at grid coordinate t / T (t = 0 .. T-1 per axis) spreads the
+// weights W_b (b in the P^3 stencil) and gathers -grad W_a . phi_a with phi_a = sum_b Ghat(a - b) W_b,
+// where Ghat is the potential grid that the solve and the inverse transform make from a unit grid
+// charge at node 0 (the mesh's own discrete kernel, translation invariant).  The result is the force
+// that the AD gather gives a particle from its own charge (zero for the exact reciprocal sum);
+// Ballenegger, Cerda and Holm, Comput. Phys. Commun. 182 (2011) 1919, remove it the same way.
+template <int P>
+__global__ void k_self_table(const float *__restrict__ ghat, int K1, int K2, int K3, float s1, float s2, float s3,
+                             int T, float4 *__restrict__ tab) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= T * T * T) return;
+    const int t1 = idx % T, t2 = (idx / T) % T, t3 = idx / (T * T);
+    float w1[P], w2[P], w3[P], g1[P], g2[P], g3[P];
+    bspline<P>((float)t1 / (float)T, w1, g1);
+    bspline<P>((float)t2 / (float)T, w2, g2);
+    bspline<P>((float)t3 / (float)T, w3, g3);
+    double fx = 0, fy = 0, fz = 0;
+    for (int a3 = 0; a3 < P; ++a3)
+        for (int a2 = 0; a2 < P; ++a2)
+            for (int a1 = 0; a1 < P; ++a1) {
+                double phi = 0;
+                for (int b3 = 0; b3 < P; ++b3)
+                    for (int b2 = 0; b2 < P; ++b2) {
+                        const size_t row = ((size_t)wrap_node(a3 - b3, K3) * K2 + wrap_node(a2 - b2, K2)) * K1;
+                        const double wb = (double)w3[b3] * w2[b2];
+                        for (int b1 = 0; b1 < P; ++b1)
+                            phi += wb * w1[b1] * (double)ghat[row + wrap_node(a1 - b1, K1)];
+                    }
+                fx += (double)g1[a1] * w2[a2] * w3[a3] * phi;
+                fy += (double)w1[a1] * g2[a2] * w3[a3] * phi;
+                fz += (double)w1[a1] * w2[a2] * g3[a3] * phi;
+            }
+    tab[idx] = make_float4((float)(-fx * s1), (float)(-fy * s2), (float)(-fz * s3), 0.f);
+}
+
+__global__ void k_unit_node(float *grid) { grid[0] = 1.f; }
+
 __global__ void k_pack_order(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
                              const float *__restrict__ q, const int *__restrict__ order, int n, int ntot,
                              float4 *__restrict__ out) {
@@ -881,6 +960,37 @@ static void refresh_background(pd_mesh *m) {
         k_spread<PP><<<nchunks, MESH_THREADS, 0, s>>>(xq, nchunks, ns_dev, m->gridA, m->K1, m->K2, m->K3, Lx, Ly, Lz); \
         break;
 
+// Fill m->self_tab (T = m->self_T) for the current box and influence function (host boundary: runs on
+// the legacy stream and waits for it).  Leaves the charge grid zero, as every transform does.
+static int compute_self_table(pd_mesh *m) {
+    if (!m->self_tab || m->self_T <= 0) return PD_OK;
+    cudaStream_t s = 0;
+    k_unit_node<<<1, 1, 0, s>>>(m->gridA);
+    PD_LAUNCHED();
+    PD_CUFFT(cufftSetStream(m->fwd, s));
+    PD_CUFFT(cufftExecR2C(m->fwd, m->gridA, m->spec));
+    k_solve<false><<<(m->nmodes + 255) / 256, 256, 0, s>>>((float2 *)m->spec, m->G, m->Vc, m->acc, m->K1, m->K1h,
+                                                            m->nmodes, m->gridA, m->nnodes);
+    PD_LAUNCHED();
+    PD_CUFFT(cufftSetStream(m->bwd, s));
+    PD_CUFFT(cufftExecC2R(m->bwd, m->spec, m->gridB));
+    const int T = m->self_T, cells = T * T * T;
+    const float s1 = (float)(m->K1 / m->box[0]), s2 = (float)(m->K2 / m->box[1]), s3 = (float)(m->K3 / m->box[2]);
+#define PD_ST(PP)                                                                                             \
+    case PP:                                                                                                  \
+        k_self_table<PP><<<(cells + 127) / 128, 128, 0, s>>>(m->gridB, m->K1, m->K2, m->K3, s1, s2, s3, T,     \
+                                                             m->self_tab);                                    \
+        break;
+    switch (m->p.order) {
+        PD_ST(3) PD_ST(4) PD_ST(5) PD_ST(6) PD_ST(7) PD_ST(8) PD_ST(9) PD_ST(10) PD_ST(11) PD_ST(12)
+        default: break;
+    }
+#undef PD_ST
+    PD_LAUNCHED();
+    PD_CUDA(cudaStreamSynchronize(s));
+    return PD_OK;
+}
+
 int mesh_transform_packed(pd_mesh *m, const float4 *xq, int nchunks, const int *ns_dev, int energy, cudaStream_t s) {
     const float Lx = (float)m->box[0], Ly = (float)m->box[1], Lz = (float)m->box[2];
     switch (m->p.order) {
@@ -975,6 +1085,8 @@ int mesh_gather_join(pd_mesh *m, pd_cluster *c, const float4 *xq, const int *per
     o.half_c_self = half_c_self;
     o.bg = m->bg;
     o.extra = extra;
+    o.self_tab = m->self_tab;
+    o.self_T = m->self_T;
     if (energy)
         launch_gather<2, true>(m, xq, nchunks, ns_dev, o, s);
     else
@@ -994,6 +1106,8 @@ static void free_mesh(pd_mesh *m) {
     dfree(m->Vc);
     dfree(m->acc);
     dfree(m->packed);
+    dfree(m->self_tab);
+    m->self_T = 0;
     if (m->plans) {
         cufftDestroy(m->fwd);
         cufftDestroy(m->bwd);
@@ -1103,6 +1217,31 @@ int pd_mesh_set_box(pd_mesh *m, const double box[3]) {
     int rc = compute_influence(m);
     if (rc) return rc;
     refresh_background(m);
+    return compute_self_table(m);
+}
+
+int pd_mesh_set_self_force_removal(pd_mesh *m, int table_size) {
+    PD_CHECK(m, PD_EINVAL, "pd_mesh_set_self_force_removal: null handle");
+    PD_CHECK(table_size == 0 || (table_size >= 4 && table_size <= 64), PD_EINVAL,
+             "self-force table size must be 0 (off) or 4..64; got %d", table_size);
+    PD_CHECK(table_size == 0 || m->p.kind != PD_MESH_P3M_IK, PD_ENOTSUP,
+             "self-force removal needs analytic differentiation (SPME or P3M-AD)");
+    dfree(m->self_tab);
+    m->self_T = 0;
+    ++m->epoch;   // captured steps hold the old table pointer
+    if (table_size == 0) return PD_OK;
+    int rc = dalloc(&m->self_tab, (size_t)table_size * table_size * table_size);
+    if (rc) return rc;
+    m->self_T = table_size;
+    return compute_self_table(m);
+}
+
+int pd_mesh_self_force_table(pd_mesh *m, float *out4, int *table_size) {
+    PD_CHECK(m, PD_EINVAL, "pd_mesh_self_force_table: null handle");
+    if (table_size) *table_size = m->self_T;
+    if (out4 && m->self_tab)
+        PD_CUDA(cudaMemcpy(out4, m->self_tab, sizeof(float4) * (size_t)m->self_T * m->self_T * m->self_T,
+                           cudaMemcpyDeviceToHost));
     return PD_OK;
 }
 
@@ -1166,6 +1305,8 @@ int pd_mesh_gather(pd_mesh *m, const float *x, const float *y, const float *z, c
         o.ids = order;
         o.n_entries = n;
         o.bg = m->bg;
+        o.self_tab = m->self_tab;
+        o.self_T = m->self_T;
         if (set) {
             if (energy) launch_gather<1, true>(m, m->packed, nchunks, nullptr, o, st);
             else launch_gather<1, false>(m, m->packed, nchunks, nullptr, o, st);

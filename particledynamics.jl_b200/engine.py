@@ -394,6 +394,23 @@ class ElectrostaticsSolver:
     def coulomb_polynomial(self) -> splits.CoulombPolynomial:
         return splits.coulomb_polynomial(self.spec.alpha, self.C, self.spec.real_cutoff, eshift=self.eshift)
 
+    def set_self_force_removal(self, table_size: int = 16):
+        """Subtract each charge's own force through the mesh (AD gathers; 0 turns it off).
+
+        Not part of the reference's solver, whose mesh forces keep the spurious self force; the
+        learned coarse-mesh form uses it on its coarse mesh."""
+        N.call("pd_mesh_set_self_force_removal", self.handle, int(table_size))
+        self.self_force_T = int(table_size)
+
+    def self_force_table(self) -> np.ndarray:
+        """(T, T, T, 3) array S[t3, t2, t1] of the self force per unit charge squared (empty when off)."""
+        T = C.c_int()
+        N.call("pd_mesh_self_force_table", self.handle, None, C.byref(T))
+        out = np.empty((T.value, T.value, T.value, 4), np.float32)
+        if T.value:
+            N.call("pd_mesh_self_force_table", self.handle, out.ctypes.data_as(C.c_void_p), C.byref(T))
+        return out[..., :3]
+
 
 # ----------------------------------------------------------------------------- step engine
 

@@ -12,6 +12,10 @@ fine-mesh PME of the same system.  PME runs on a mesh twice as coarse (2.0 A, or
   scalar times a per-neighbour radial weight multiplies each displacement vector, so the residual
   rotates with the configuration.
 
+Before anything is learned, the coarse mesh's spurious self force (the force each ion receives
+through the mesh from its own charge, a known function of its position relative to the nodes) is
+removed exactly (``ElectrostaticsSolver.set_self_force_removal``).
+
 Training (``CoarseMeshTrainer``): snapshots from a fine-mesh run give the target
 ``R_i = F_fine_mesh - F_coarse_mesh`` (the real-space part is identical for both meshes), the radial
 function ``b`` is fitted by linear least squares, then the network is trained by Adam on the mean
@@ -244,7 +248,8 @@ class CoarseMeshTrainer:
     """
 
     def __init__(self, n, box, q, typ, spec: ElectrostaticsSpec, *, coarse_spacing=2.0, coarse_order=4, seed=0,
-                 correction: LearnedCorrection | None = None, net: MLPNetwork | None = None, **desc):
+                 self_force_table: int = 16, correction: LearnedCorrection | None = None,
+                 net: MLPNetwork | None = None, **desc):
         self.n = int(n)
         self.box = tuple(float(b) for b in box)
         self.q, self.typ = q, typ
@@ -258,6 +263,11 @@ class CoarseMeshTrainer:
                                    real_space_modifier=spec.real_space_modifier)
         self.coarse_spec = cspec
         self.coarse = ElectrostaticsSolver(cspec, self.box, qh, nmax=self.n)
+        # the coarse mesh's spurious self force is known exactly (a function of each ion's position
+        # relative to the nodes): it is removed before anything is learned
+        self.self_force_table = int(self_force_table)
+        if self.self_force_table:
+            self.coarse.set_self_force_removal(self.self_force_table)
         self.corr = correction if correction is not None else LearnedCorrection(self.n, self.box, **desc)
         self.net = net if net is not None else MLPNetwork(seed=seed)
         self.snap_pos = []      # centred coordinates (3, n) float32 per snapshot

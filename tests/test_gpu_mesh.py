@@ -124,3 +124,66 @@ def test_zero_charges_and_validation(pd, cuda):
         _solver(pd, "spme", 0.9, (24, 25, 27), 5, 1.0, 7.0, L, q)           # r_c >= L/2
     with pytest.raises(ValueError):
         pd.ElectrostaticsSpec(coulomb_prefactor=1.0, real_cutoff=3.0, alpha=1.0, order=2, mesh=(16, 16, 16))
+
+
+def _melt(pd, L, seed):
+    n = int(0.0375 * L ** 3) // 2 * 2
+    pos, q, _ = pd.synthetic.ionic_melt(n, L, seed=seed)
+    return np.asarray(pos, np.float32).astype(np.float64), np.asarray(q, np.float64)
+
+
+@pytest.mark.parametrize("influence", ["spme", "p3m_ad"])
+def test_self_force_table_and_removal(pd, ora, cuda, influence):
+    # the table equals the self force of a lone unit charge through the FP64 oracle mesh; the gather
+    # subtracts q^2 times its trilinear interpolation; removing it lowers the coarse mesh's error
+    # against a fine mesh; 0 turns it off again
+    C, alpha, L, K, P = 14.399645, 0.34705, 30.0, 15, 4
+    box = (L, L, L)
+    R, q = _melt(pd, L, 21)
+    s = _solver(pd, influence, alpha, (K, K, K), P, C, 9.0, box, q)
+    F_off, _, _, _ = _mesh_gpu(pd, s, R, q, energy=False)
+    s.set_self_force_removal(16)
+    tab = s.self_force_table().astype(np.float64)
+    assert tab.shape == (16, 16, 16, 3)
+    tables = ora.influence(influence, P, (K, K, K), box, C, alpha)
+    rng = np.random.default_rng(0)
+    for t in rng.integers(0, 16, (24, 3)):
+        pos = (t[::-1] / 16.0 * L / K)[None, :]          # table index (t3, t2, t1) -> grid coordinate (t1, t2, t3)/T
+        ex = ora.mesh_source_forces(pos, np.array([1.0]), box, (K, K, K), P, tables, [0])[0, 0]
+        assert np.abs(tab[t[0], t[1], t[2]] - ex).max() <= 1e-3 * np.abs(tab).max() + 1e-9, (t, ex)
+    F_on, _, _, _ = _mesh_gpu(pd, s, R, q, energy=False)
+    u = (R / L - np.floor(R / L)) * K
+    f = (u - np.floor(u)) * 16
+    i0 = np.minimum(f.astype(int), 15)
+    w = f - i0
+    S = np.zeros_like(R)
+    for c in range(8):
+        b = [(c >> d) & 1 for d in range(3)]
+        idx = [(i0[:, d] + b[d]) % 16 for d in range(3)]
+        wt = np.prod([w[:, d] if b[d] else 1 - w[:, d] for d in range(3)], axis=0)
+        S += wt[:, None] * tab[idx[2], idx[1], idx[0]]
+    expect = F_off - (q * q)[:, None] * S
+    assert np.linalg.norm(F_on - expect) <= 2e-5 * np.linalg.norm(F_off)
+    fine = ora.mesh(R, q, box, (30, 30, 30), 5, kind=influence, alpha=alpha, C=C)["F"]
+    e_off, e_on = np.linalg.norm(F_off - fine), np.linalg.norm(F_on - fine)
+    assert e_on < 0.95 * e_off, (e_on, e_off)
+    # a new box recomputes the table; 0 turns the removal off
+    s.set_box((L + 1.0,) * 3)
+    tab2 = s.self_force_table()
+    assert np.abs(tab2 - tab).max() > 1e-3 * np.abs(tab).max()
+    s.set_box(box)
+    s.set_self_force_removal(0)
+    assert s.self_force_table().size == 0
+    F_again, _, _, _ = _mesh_gpu(pd, s, R, q, energy=False)
+    assert np.linalg.norm(F_again - F_off) <= 1e-6 * np.linalg.norm(F_off)   # spread atomics: order varies
+    with pytest.raises(Exception):
+        s.set_self_force_removal(3)
+    s.close()
+
+
+def test_self_force_removal_refused_for_ik(pd, cuda):
+    R, q = _cloud(64, (14.0, 15.0, 16.0), 5)
+    s = _solver(pd, "p3m_ik", 0.9, (24, 25, 27), 5, 1.7, 4.0, (14.0, 15.0, 16.0), q)
+    with pytest.raises(Exception):
+        s.set_self_force_removal(16)
+    s.close()
