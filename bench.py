@@ -43,6 +43,7 @@ T_INIT = 1200.0
 BUFFER, PRUNE = 2.5, 0.7
 E5_SPACING, E5_ORDER = 0.75, 6   # plain form at <= 1e-5 relative RMS force error against the Ewald sum
 SEED = 2026
+SELF_FORCE_TABLE = 16            # learned form: coarse-mesh self-force table size per axis
 
 
 def ns_per_day(ms_per_step: float, dt_fs: float = DT_FS) -> float:
@@ -66,9 +67,10 @@ def forces(pd, buffer=BUFFER, prune=PRUNE):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms; the summary keeps the samples taken
+    inside the timed region (the ``with`` block), which starts only once the sampler writes rows."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -76,6 +78,7 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         try:
@@ -83,14 +86,20 @@ class ClockSampler:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            deadline = time.time() + 15.0   # the first row shows that the sampler is running
+            while time.time() < deadline and os.path.getsize(self.path) == 0 and self.proc.poll() is None:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
+        self.t0 = time.time()
         return self
 
     def __exit__(self, *a):
+        self.t1 = time.time()
         if self.proc is not None:
+            time.sleep(0.15)   # let the samples of the region's last moments be written
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -98,24 +107,33 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        import datetime
         if not self.path or not os.path.exists(self.path):
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         rows = []
         for line in open(self.path):
             p = [s.strip() for s in line.split(",")]
-            if len(p) < 9:
+            if len(p) < 10:
                 continue
             try:
-                rows.append((float(p[1]), float(p[2]), float(p[3]) if p[3] not in ("[N/A]", "") else 0.0, p[5:9]))
+                ts = datetime.datetime.strptime(p[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(p[2]), float(p[3]), float(p[4]) if p[4] not in ("[N/A]", "") else 0.0,
+                             p[6:10]))
             except ValueError:
                 continue
         os.unlink(self.path)
-        if not rows:
+        inside = [r for r in rows if self.t0 is not None and self.t0 - 0.025 <= r[0] <= self.t1 + 0.025]
+        window = "timed region"
+        if not inside:   # a region shorter than the sampling period: the samples nearest to it
+            inside = sorted(rows, key=lambda r: abs(r[0] - 0.5 * (self.t0 + self.t1)))[:2]
+            window = "nearest to the timed region"
+        if not inside:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[3][k].lower() == "active"})
-        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
-                "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": reasons}
+        reasons = sorted({names[k] for r in inside for k in range(4) if r[4][k].lower() == "active"})
+        return {"sm_mhz": statistics.median(r[1] for r in inside), "sm_max_mhz": max(r[2] for r in inside),
+                "power_w_max": max(r[3] for r in inside), "samples": len(inside), "window": window,
+                "region_s": round(self.t1 - self.t0, 3), "reasons": reasons}
 
 
 def dist_setup():
@@ -323,7 +341,8 @@ def run_learned_form(pd, args, st, system, dt, flush):
     spec = st.solver.spec
     st.evaluate_forces_into_f(False)
     t0 = time.perf_counter()
-    tr = pd.learned.CoarseMeshTrainer(n, box, st.q, st.typ, spec, coarse_spacing=2.0, coarse_order=4, seed=SEED)
+    tr = pd.learned.CoarseMeshTrainer(n, box, st.q, st.typ, spec, coarse_spacing=2.0, coarse_order=4, seed=SEED,
+                                      self_force_table=SELF_FORCE_TABLE)
     for _ in range(args.snapshots):
         st.step(args.snapshot_stride, use_graph=True)
         st.synchronize()
@@ -346,7 +365,8 @@ def run_learned_form(pd, args, st, system, dt, flush):
     spec_e5 = pd.ElectrostaticsSpec(coulomb_prefactor=spec.coulomb_prefactor, real_cutoff=spec.real_cutoff,
                                     alpha=spec.alpha, order=E5_ORDER, mesh_spacing=E5_SPACING)
     solver_e5 = pd.ElectrostaticsSolver(spec_e5, box, st.q.double().cpu().numpy(), nmax=n)
-    errs = {"plain_fine": [], "plain_e5": [], "coarse": [], "coarse_radial": [], "learned": []}
+    raw = pd.ElectrostaticsSolver(tr.coarse_spec, box, st.q.double().cpu().numpy(), nmax=n)   # self force kept
+    errs = {"plain_fine": [], "plain_e5": [], "coarse": [], "coarse_self": [], "coarse_radial": [], "learned": []}
     for _ in range(args.heldout):
         st.step(100, use_graph=True)
         st.synchronize()
@@ -357,7 +377,8 @@ def run_learned_form(pd, args, st, system, dt, flush):
         den = torch.sqrt((Ft ** 2).sum())
         fine = tr.mesh_forces(tr.fine, x, y, z).double()
         coarse = tr.mesh_forces(tr.coarse, x, y, z).double()
-        forms = {"plain_fine": fine, "plain_e5": tr.mesh_forces(solver_e5, x, y, z).double(), "coarse": coarse,
+        forms = {"plain_fine": fine, "plain_e5": tr.mesh_forces(solver_e5, x, y, z).double(),
+                 "coarse": tr.mesh_forces(raw, x, y, z).double(), "coarse_self": coarse,
                  "coarse_radial": coarse + tr.corr.correction(ones, x, y, z, tr.q, tr.typ)[:, :3].double(),
                  "learned": coarse + tr.corr.correction(tr.net, x, y, z, tr.q, tr.typ)[:, :3].double()}
         for k, f in forms.items():
@@ -372,6 +393,7 @@ def run_learned_form(pd, args, st, system, dt, flush):
     st2 = pd.Simulation(sys2, pd.Integrator(dt=dt, forces=forces2)).state
     st2.evaluate_forces_into_f(False)
     ms_coarse = time_md_steps(st2, dt, args.steps, args.warmup, flush, args.no_flush)
+    st2.solver.set_self_force_removal(SELF_FORCE_TABLE)
     st2.engine.set_learned(tr.corr, tr.net)
     st2.evaluate_forces_into_f(False)
     ms_learned = time_md_steps(st2, dt, args.steps, args.warmup, flush, args.no_flush)
@@ -392,6 +414,9 @@ def run_learned_form(pd, args, st, system, dt, flush):
                           "reciprocal Ewald sum, over the RMS of the full Ewald force; the real-space part is "
                           "common to all forms)",
             "mesh": "coarse PME 2.0 A (60^3), order 4; fine 1.0 A (120^3), order 5",
+            "forms_note": "coarse: the coarse mesh alone (also the timed coarse_only step); coarse_self: its "
+                          "self force removed (table %d^3); coarse_radial: plus the fitted radial term (s = 1); "
+                          "learned: plus the trained network (the timed learned step)" % SELF_FORCE_TABLE,
             "training": {"snapshots": args.snapshots, "stride_steps": args.snapshot_stride, "epochs": args.epochs,
                          "mse_per_epoch": losses, "radial_coef": [float(c) for c in coef],
                          "seconds": {"snapshots": t_gen, "dataset": t_data, "adam": t_train},
@@ -407,6 +432,7 @@ def profile_learned(pd, args, system, box, dt):
     el = pd.PME(coulomb_prefactor=pd.synthetic.COULOMB_EV_A, real_cutoff=RC, real_space_tolerance=1e-5,
                 mesh_spacing=2.0, order=4)
     st = pd.Simulation(system, pd.Integrator(dt=dt, forces=forces(pd, args.buffer, args.prune)[:1] + [el])).state
+    st.solver.set_self_force_removal(SELF_FORCE_TABLE)
     lc = pd.learned.LearnedCorrection(st.n, box)
     lc.set_radial(np.linspace(0.01, -0.02, lc.nb))
     net = pd.learned.MLPNetwork(pd.learned.init_params(SEED, s0=1.0, out_scale=0.1))
