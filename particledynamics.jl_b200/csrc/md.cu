@@ -445,7 +445,10 @@ int pd_md_step(pd_md *md, int nsteps, float dt, int energy_last, int use_graph, 
                 PD_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
                 rc = enqueue_step(md, dt, energy, s, cond);
                 cudaError_t e = cudaStreamEndCapture(s, &g);
-                if (rc == PD_OK && e == cudaSuccess) e = cudaGraphInstantiate(&md->exec[energy], g, 0);
+                // per-node priorities: the mesh branch, captured from the high-priority side stream,
+                // keeps its priority inside the graph (the default instantiation drops it)
+                if (rc == PD_OK && e == cudaSuccess)
+                    e = cudaGraphInstantiateWithFlags(&md->exec[energy], g, cudaGraphInstantiateFlagUseNodePriority);
                 if (g) cudaGraphDestroy(g);
                 if (rc == PD_OK && e == cudaSuccess) break;
                 md->exec[energy] = nullptr;
