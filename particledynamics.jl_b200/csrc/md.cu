@@ -44,6 +44,10 @@ struct pd_md {
     const pd_mlp *net = nullptr;
     cudaStream_t side2 = nullptr;
     cudaEvent_t ev_fork2 = nullptr, ev_join2 = nullptr;
+    // host-buffer steps: the positions are final after the drift, so their copy back runs on its
+    // own stream beside the force pass (ev_pos is recorded in every captured step)
+    cudaStream_t copy = nullptr;
+    cudaEvent_t ev_pos = nullptr, ev_copied = nullptr;
 };
 
 namespace pdb {
@@ -268,6 +272,18 @@ static int enqueue_forces(pd_md *md, int energy, float half_dt, cudaStream_t s) 
 // One full step, device-decided.  cond = 1 (inside a stream capture): the build and
 // prune bodies become IF nodes of the captured graph; otherwise their kernels are
 // launched and return at once when the device flags are clear.
+// Marks the end of the drift (positions final for this step): an external event node inside a
+// capture, so that work outside the graph can wait for it; a plain record otherwise.
+static int record_positions(pd_md *md, cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    PD_CUDA(cudaStreamIsCapturing(s, &cs));
+    if (cs == cudaStreamCaptureStatusActive)
+        PD_CUDA(cudaEventRecordWithFlags(md->ev_pos, s, cudaEventRecordExternal));
+    else
+        PD_CUDA(cudaEventRecord(md->ev_pos, s));
+    return PD_OK;
+}
+
 static int enqueue_step(pd_md *md, float dt, int energy, cudaStream_t s, int cond) {
     pd_cluster *c = md->c;
     pd_md_state &st = md->st;
@@ -286,6 +302,7 @@ static int enqueue_step(pd_md *md, float dt, int energy, cudaStream_t s, int con
                                               c->slot_of, c->xq, c->ref_build, c->ref_prune, hb * hb, hp * hp,
                                               c->counts, c->p.nstlist, c->p.nstprune, hbuild);
         PD_LAUNCHED();
+        if ((rc = record_positions(md, s))) return rc;
         if ((rc = capture_if_body(s, md->body, hbuild, [&](cudaStream_t cs) {
                  return cluster_build_launch(c, st.x, st.y, st.z, q, st.type, 1, cs);
              })))
@@ -296,6 +313,7 @@ static int enqueue_step(pd_md *md, float dt, int energy, cudaStream_t s, int con
                                                c->slot_of, c->xq, c->ref_build, c->ref_prune, hb * hb, hp * hp,
                                                c->counts, c->p.nstlist, c->p.nstprune, 0);
         PD_LAUNCHED();
+        if ((rc = record_positions(md, s))) return rc;
         if ((rc = cluster_build_launch(c, st.x, st.y, st.z, q, st.type, 1, s))) return rc;
     }
     // the mesh transform forks before the prune, which runs as a flag-gated kernel
@@ -331,6 +349,9 @@ int pd_md_create(pd_md **out, pd_cluster *c, pd_mesh *m, const pd_md_state *st, 
         cudaStreamCreateWithFlags(&md->body, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&md->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&md->ev_join, cudaEventDisableTiming) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&md->copy, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&md->ev_pos, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&md->ev_copied, cudaEventDisableTiming) != cudaSuccess ||
         dalloc(&md->esum, 1) != PD_OK) {
         set_error("pd_md_create: stream/event allocation failed");
         pd_md_destroy(md);
@@ -346,6 +367,9 @@ int pd_md_destroy(pd_md *md) {
         if (md->exec[k]) cudaGraphExecDestroy(md->exec[k]);
     if (md->ev_fork) cudaEventDestroy(md->ev_fork);
     if (md->ev_join) cudaEventDestroy(md->ev_join);
+    if (md->ev_pos) cudaEventDestroy(md->ev_pos);
+    if (md->ev_copied) cudaEventDestroy(md->ev_copied);
+    if (md->copy) cudaStreamDestroy(md->copy);
     if (md->side) cudaStreamDestroy(md->side);
     if (md->body) cudaStreamDestroy(md->body);
     if (md->side2) cudaStreamDestroy(md->side2);
@@ -475,7 +499,7 @@ int pd_md_step_host(pd_md *md, float *host_xyz, float *host_v, int nsteps, float
     pd_md_state &st = md->st;
     const size_t nb = sizeof(float) * (size_t)st.n;
     float *dx[3] = {st.x, st.y, st.z}, *dv[3] = {st.vx, st.vy, st.vz};
-    // one copy per array triple when the caller keeps its components in one block, one copy for the
+    // copies in: one per array triple when the caller keeps its components in one block, one for the
     // whole state when positions and velocities are adjacent blocks on both sides
     const bool xblock = st.y == st.x + st.n && st.z == st.y + st.n;
     const bool vblock = st.vy == st.vx + st.n && st.vz == st.vy + st.n;
@@ -498,16 +522,16 @@ int pd_md_step_host(pd_md *md, float *host_xyz, float *host_v, int nsteps, float
         PD_LAUNCHED();
         PD_CUDA(cudaMemcpyAsync(epot_sum, md->esum, sizeof(double), cudaMemcpyDeviceToHost, s));
     }
-    if (whole) {
-        PD_CUDA(cudaMemcpyAsync(host_xyz, st.x, 6 * nb, cudaMemcpyDeviceToHost, s));
-    } else {
-        for (int d = 0; d < (xblock ? 1 : 3); ++d)
-            PD_CUDA(cudaMemcpyAsync(host_xyz + (size_t)d * st.n, dx[d], xblock ? 3 * nb : nb, cudaMemcpyDeviceToHost,
-                                    s));
-        for (int d = 0; d < (vblock ? 1 : 3); ++d)
-            PD_CUDA(cudaMemcpyAsync(host_v + (size_t)d * st.n, dv[d], vblock ? 3 * nb : nb, cudaMemcpyDeviceToHost,
-                                    s));
-    }
+    // positions: final after the last step's drift (ev_pos), copied back while its forces are computed;
+    // velocities after the closing kick
+    PD_CUDA(cudaStreamWaitEvent(md->copy, md->ev_pos, 0));
+    for (int d = 0; d < (xblock ? 1 : 3); ++d)
+        PD_CUDA(cudaMemcpyAsync(host_xyz + (size_t)d * st.n, dx[d], xblock ? 3 * nb : nb, cudaMemcpyDeviceToHost,
+                                md->copy));
+    PD_CUDA(cudaEventRecord(md->ev_copied, md->copy));
+    for (int d = 0; d < (vblock ? 1 : 3); ++d)
+        PD_CUDA(cudaMemcpyAsync(host_v + (size_t)d * st.n, dv[d], vblock ? 3 * nb : nb, cudaMemcpyDeviceToHost, s));
+    PD_CUDA(cudaStreamWaitEvent(s, md->ev_copied, 0));
     PD_CUDA(cudaStreamSynchronize(s));
     return PD_OK;
 }
