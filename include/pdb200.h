@@ -286,7 +286,9 @@ int pd_md_evaluate(pd_md *md, int energy, pd_stream_t s);
 int pd_md_step(pd_md *md, int nsteps, float dt, int energy_last, int use_graph, pd_stream_t s);
 /* Steps through the C ABI with host buffers: copies x, v (pinned host, 3n floats each,
  * [x..., y..., z...]) to the device, runs nsteps, copies them back with the potential energy
- * sum (double) of the last step.  Used for end-to-end timing. */
+ * sum (double) of the last step.  The positions are copied back on an internal stream as soon as
+ * the last step's drift has written them (beside the force pass); the call returns when both
+ * copies are done.  Used for end-to-end timing. */
 int pd_md_step_host(pd_md *md, float *host_xyz, float *host_v, int nsteps, float dt,
                     double *epot_sum, pd_stream_t s);
 
