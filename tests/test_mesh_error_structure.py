@@ -9,7 +9,9 @@ The test states three facts about E_ij on a small melt at the melt's density and
 * the self term E_ii (the mesh's spurious self force, a function of the ion's position relative to
   the nodes) carries a fifth of |R|^2 or more;
 * the best radial pair model E_ij ~ q_i q_j b(r_ij) r_ij (b averaged over all pairs at each
-  distance, the most a rotation-invariant pair term can reach) leaves more than half of |R|^2.
+  distance, the most a rotation-invariant pair term can reach) leaves more than half of |R|^2;
+* radial terms modulated by the first harmonics of either ion's fractional grid position do no
+  better on held-out ions than the plain radial terms.
 
 So what a local model must learn depends on where both ions sit relative to the mesh nodes, which
 rotation-invariant charge descriptors cannot see.
@@ -38,7 +40,8 @@ def decomposition(pd, ora):
     d = pos[:, None, :] - pos[None, :, :]
     d -= L * np.round(d / L)
     r = np.sqrt((d * d).sum(-1))
-    return dict(n=n, q=q, R=Ff - Fc, E=np.transpose(E, (1, 0, 2)), d=d, r=r, Ff=Ff)
+    u = (pos / L - np.floor(pos / L)) * 15
+    return dict(n=n, q=q, R=Ff - Fc, E=np.transpose(E, (1, 0, 2)), d=d, r=r, Ff=Ff, u=u - np.floor(u))
 
 
 def test_source_terms_sum_to_the_residual(decomposition):
@@ -78,3 +81,37 @@ def test_self_term_and_radial_model_shares(decomposition):
     radial = ((qq * b_r)[..., None] * d).sum(1)
     left = ((D["R"] - radial) ** 2).sum() / tot
     assert left > 0.5, left
+
+
+def test_grid_modulated_radial_terms_add_nothing(decomposition):
+    """Linear pair models whose radial terms are modulated by the first harmonics of either ion's
+    fractional grid position, fitted on half of the ions (self term removed first), leave about
+    what the plain radial terms leave on the other half: the grid-dependent part of the error is
+    not a low-harmonic modulation of the radial pair term."""
+    D = decomposition
+    n, E, d, r, q, u = D["n"], D["E"], D["d"], D["r"], D["q"], D["u"]
+    R = D["R"]
+    R1 = R - E[np.arange(n), np.arange(n)]
+    qq = q[:, None] * q[None, :]
+    near = (r > 0) & (r < 8.0)
+    nu = 2.0 + 0.7 * np.arange(10)
+    fc = np.where(near, (1 - (r / 8.0) ** 2) ** 2, 0.0)
+    G = np.exp(-((r[..., None] - nu) ** 2) / (2 * 0.45 ** 2)) * fc[..., None]
+    F0 = np.einsum("ij,ijm,ijc->icm", qq, G, d)
+    cols = [np.ones(n)]
+    for a in range(3):
+        cols += [np.cos(2 * np.pi * u[:, a]), np.sin(2 * np.pi * u[:, a])]
+    phi = np.stack(cols, 1)
+    Fi = np.einsum("icm,ik->ickm", F0, phi).reshape(n, 3, -1)
+    Fj = np.einsum("ij,ijm,ijc,jk->ickm", qq, G, d, phi).reshape(n, 3, -1)
+    train = np.arange(n) < n // 2
+    tot = (R[~train] ** 2).sum()
+
+    def left(feats):
+        th, *_ = np.linalg.lstsq(feats[train].reshape(-1, feats.shape[-1]), R1[train].reshape(-1), rcond=None)
+        return ((R1[~train] - feats[~train] @ th) ** 2).sum() / tot
+
+    base, mod = left(F0), left(np.concatenate([Fi, Fj], -1))
+    assert base < 0.8, base
+    assert mod > 0.9 * base, (mod, base)
+
