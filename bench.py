@@ -868,6 +868,8 @@ def main():
                "config": {"workload": f"ionic melt N={n} (L={box[0]:.1f} A) LJ+SPME r_c=9 A, "
                                       f"{'x'.join(str(k) for k in st.solver.mesh)} order 5, NVE dt=1 fs",
                           "form": form, "parallelism": f"replicas x{world}",
+                          "aggregate": ("value = ns/day summed over the independent replicas, one per GPU"
+                                        if world > 1 else "one system"),
                           "list_buffer_A": args.buffer, "prune_buffer_A": args.prune,
                           "pair_shape": {"nsplit": tune["nsplit"], "warps": tune["warps"],
                                          "pair_pass_ms": tune["ms"], "step_ms": tune["step_ms"]},

@@ -168,9 +168,10 @@ int pd_cluster_compute(pd_cluster *c, const float *x, const float *y, const floa
                        float *epot, float *vir6, int energy, pd_stream_t s);
 /* Allocation-free force evaluation.  This entry point has no counterpart in the reference.
  *
- * It serves callers that cannot call cudaMalloc: a host that has sized its device memory to the
- * byte and forbids further allocation, code running while a CUDA graph region is being built,
- * or a real-time loop that must stay out of the allocator.  It does the work of
+ * It serves callers that cannot call cudaMalloc: a plugin inside a host program whose own memory
+ * pool has claimed the device memory (CUDA.jl, PyTorch's caching allocator), a host that has
+ * sized its device memory to the byte and forbids further allocation, or a real-time loop that
+ * must stay out of the allocator (cudaMalloc may synchronise the device).  It does the work of
  * pd_cluster_compute (build, prune, pair pass, scatter) for one small system without a handle,
  * taking every scratch buffer from one static device array of PD_STATIC_SCRATCH_BYTES that each
  * GPU loading the library holds until the process exits.  The caller passes the inputs and the
@@ -181,7 +182,8 @@ int pd_cluster_compute(pd_cluster *c, const float *x, const float *y, const floa
  * array's device address (cudaGetSymbolAddress) with that device current, so make that first
  * call before any stream capture.  All calls share the array and it keeps the last call's
  * contents (the call clears what must start at zero); calls that overlap on the GPU race.
- * The call reads a device status word back at its end, so it synchronises s. */
+ * The call reads a device status word back at its end, so it synchronises s.  On PD_ECAPACITY or
+ * PD_ENONFINITE the outputs have already been overwritten (they hold no pair forces). */
 #define PD_STATIC_SCRATCH_BYTES (4u << 20)
 #define PD_STATIC_MAX_N 4096
 int pd_cluster_compute_static(const pd_cluster_params *p, const double box[3], const float *x, const float *y,

@@ -964,6 +964,72 @@ int cluster_decide_launch(pd_cluster *c, const float *x, const float *y, const f
     return PD_OK;
 }
 
+int cluster_check_params(const pd_cluster_params *p) {
+    PD_CHECK(p->n >= 1, PD_EINVAL, "cluster-pair engine needs at least one particle");
+    PD_CHECK(p->skin >= 0 && p->prune_buffer >= 0 && p->prune_buffer <= p->skin, PD_EINVAL,
+             "cluster pairs need 0 <= prune_buffer <= skin.");
+    PD_CHECK(p->rmax > 0, PD_EINVAL, "The cluster-pair backend needs a vdW term or an electrostatics solver.");
+    PD_CHECK(p->lj_kind >= PD_LJ_NONE && p->lj_kind <= PD_LJ_TABLE, PD_EINVAL, "unknown LJ kind %d", p->lj_kind);
+    PD_CHECK(p->lj_kind != PD_LJ_TABLE || (p->ntypes >= 1 && p->ntypes <= PD_MAX_TYPES), PD_EINVAL,
+             "LJ type table needs 1 <= ntypes <= %d", PD_MAX_TYPES);
+    PD_CHECK(!p->coulomb || (p->coul_ne >= 1 && p->coul_ne <= PD_MAX_POLY && p->coul_nf >= 1 &&
+                             p->coul_nf <= PD_MAX_POLY),
+             PD_EINVAL, "Coulomb polynomial needs 1..%d coefficients", PD_MAX_POLY);
+    return PD_OK;
+}
+
+// setup! (List.jl:874-937): super-cluster edge b = cbrt(64 / rho), z-bins of about 4 particles,
+// NSmax = ceil(N / 64) + ncol, search span with a 2 % shrink allowance.
+int cluster_geometry(int N, double rlist, const double box[3], ClusterGeom *g) {
+    const double Lx = (float)box[0], Ly = (float)box[1], Lz = (float)box[2];
+    PD_CHECK(std::isfinite(Lx) && std::isfinite(Ly) && std::isfinite(Lz) && Lx > 0 && Ly > 0 && Lz > 0, PD_EINVAL,
+             "box lengths must be finite and positive");
+    PD_CHECK(std::min(Lx, std::min(Ly, Lz)) > 2 * rlist, PD_EINVAL,
+             "cluster-pair list radius %g needs every box length above %g.", rlist, 2 * rlist);
+    g->rlist = rlist;
+    g->rho = N / (Lx * Ly * Lz);
+    const double b = std::cbrt(SUPER / g->rho);
+    g->ncx = std::max(1, (int)std::floor(Lx / b));
+    g->ncy = std::max(1, (int)std::floor(Ly / b));
+    g->ncol = g->ncx * g->ncy;
+    g->nzb = std::max(1, (int)std::nearbyint(Lz * g->rho * (Lx / g->ncx) * (Ly / g->ncy) / 4));
+    g->nbin = (long long)g->ncol * g->nzb;
+    PD_CHECK(g->nbin < (1LL << 30), PD_EINVAL, "cluster-pair binning exceeds int range.");
+    g->nsmax = (N + SUPER - 1) / SUPER + g->ncol;
+    g->nslot = SUPER * g->nsmax;
+    const double shrink = 0.98;
+    g->mx = (int)std::floor(rlist / (shrink * Lx / g->ncx)) + 1;
+    g->my = (int)std::floor(rlist / (shrink * Ly / g->ncy)) + 1;
+    g->ncs = std::min(2 * g->mx + 1, g->ncx) * std::min(2 * g->my + 1, g->ncy);
+    PD_CHECK(g->ncs <= SEARCH_MAX_COLS, PD_EINVAL,
+             "cluster-pair search needs %d columns per super-cluster (limit %d).", g->ncs, SEARCH_MAX_COLS);
+    return PD_OK;
+}
+
+void cluster_pair_params(const pd_cluster_params *p, const double box[3], PairParams *pp) {
+    memset(pp, 0, sizeof *pp);
+    pp->Lx = (float)box[0];
+    pp->Ly = (float)box[1];
+    pp->Lz = (float)box[2];
+    pp->lj_kind = p->lj_kind;
+    pp->c6 = p->lj_c6;
+    pp->c12 = p->lj_c12;
+    pp->lrc2 = p->lj_rc2;
+    pp->esh = p->lj_esh;
+    pp->ntypes = p->lj_kind == PD_LJ_TABLE ? p->ntypes : 1;
+    pp->coulomb = p->coulomb;
+    pp->C = p->coul_C;
+    pp->rc2 = p->coul_rc2;
+    pp->sx = p->coul_sx;
+    pp->eshift = p->coul_eshift;
+    pp->ne = p->coulomb ? p->coul_ne : 1;
+    pp->nf = p->coulomb ? p->coul_nf : 1;
+    for (int k = 0; k < PD_MAX_POLY; ++k) {   // coefficients past the fitted length are zero (exact padding)
+        pp->pe[k] = k < pp->ne ? p->coul_pe[k] : 0.f;
+        pp->pf[k] = k < pp->nf ? p->coul_pf[k] : 0.f;
+    }
+}
+
 }  // namespace pdb
 
 // ------------------------------------------------------------------ C ABI
@@ -994,20 +1060,11 @@ uint64_t pd_launch_count(void) { return __atomic_load_n(&pdb::g_launches, __ATOM
 int pd_cluster_create(pd_cluster **out, const pd_cluster_params *p, const double box[3]) {
     PD_CHECK(out && p && box, PD_EINVAL, "pd_cluster_create: null argument");
     *out = nullptr;
-    PD_CHECK(p->n >= 1, PD_EINVAL, "cluster-pair engine needs at least one particle");
-    PD_CHECK(p->skin >= 0 && p->prune_buffer >= 0 && p->prune_buffer <= p->skin, PD_EINVAL,
-             "cluster pairs need 0 <= prune_buffer <= skin.");
-    PD_CHECK(p->rmax > 0, PD_EINVAL, "The cluster-pair backend needs a vdW term or an electrostatics solver.");
-    PD_CHECK(p->lj_kind >= PD_LJ_NONE && p->lj_kind <= PD_LJ_TABLE, PD_EINVAL, "unknown LJ kind %d", p->lj_kind);
-    PD_CHECK(p->lj_kind != PD_LJ_TABLE || (p->ntypes >= 1 && p->ntypes <= PD_MAX_TYPES), PD_EINVAL,
-             "LJ type table needs 1 <= ntypes <= %d", PD_MAX_TYPES);
-    PD_CHECK(!p->coulomb || (p->coul_ne >= 1 && p->coul_ne <= PD_MAX_POLY && p->coul_nf >= 1 &&
-                             p->coul_nf <= PD_MAX_POLY),
-             PD_EINVAL, "Coulomb polynomial needs 1..%d coefficients", PD_MAX_POLY);
+    int rc = cluster_check_params(p);
+    if (rc) return rc;
     pd_cluster *c = new pd_cluster();
     c->p = *p;
     c->n = p->n;
-    int rc;
     if ((rc = dalloc(&c->counts, W_LEN)) || (rc = dalloc(&c->slot_of, (size_t)c->n)) ||
         (rc = dalloc(&c->order, (size_t)c->n)) || (rc = dalloc(&c->ref_build, (size_t)c->n)) ||
         (rc = dalloc(&c->ref_prune, (size_t)c->n)) || (rc = dalloc(&c->lj_table, PD_MAX_TYPES * PD_MAX_TYPES * 4))) {
@@ -1019,26 +1076,7 @@ int pd_cluster_create(pd_cluster **out, const pd_cluster_params *p, const double
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev);
-    // kernel parameters of the pair pass
-    PairParams &pp = c->pp;
-    memset(&pp, 0, sizeof pp);
-    pp.lj_kind = p->lj_kind;
-    pp.c6 = p->lj_c6;
-    pp.c12 = p->lj_c12;
-    pp.lrc2 = p->lj_rc2;
-    pp.esh = p->lj_esh;
-    pp.ntypes = p->lj_kind == PD_LJ_TABLE ? p->ntypes : 1;
-    pp.coulomb = p->coulomb;
-    pp.C = p->coul_C;
-    pp.rc2 = p->coul_rc2;
-    pp.sx = p->coul_sx;
-    pp.eshift = p->coul_eshift;
-    pp.ne = p->coulomb ? p->coul_ne : 1;
-    pp.nf = p->coulomb ? p->coul_nf : 1;
-    for (int k = 0; k < PD_MAX_POLY; ++k) {   // coefficients past the fitted length are zero (exact padding)
-        pp.pe[k] = k < pp.ne ? p->coul_pe[k] : 0.f;
-        pp.pf[k] = k < pp.nf ? p->coul_pf[k] : 0.f;
-    }
+    cluster_pair_params(p, box, &c->pp);   // kernel parameters of the pair pass
     if ((rc = pd_cluster_setup(c, box))) {
         pd_cluster_destroy(c);
         return rc;
@@ -1064,27 +1102,13 @@ int pd_cluster_destroy(pd_cluster *c) {
 int pd_cluster_setup(pd_cluster *c, const double box[3]) {
     PD_CHECK(c && box, PD_EINVAL, "pd_cluster_setup: null argument");
     const int N = c->n;
-    const double rlist = c->p.rmax + c->p.skin;
-    const double Lx = (float)box[0], Ly = (float)box[1], Lz = (float)box[2];
-    PD_CHECK(std::isfinite(Lx) && std::isfinite(Ly) && std::isfinite(Lz) && Lx > 0 && Ly > 0 && Lz > 0, PD_EINVAL,
-             "box lengths must be finite and positive");
-    PD_CHECK(std::min(Lx, std::min(Ly, Lz)) > 2 * rlist, PD_EINVAL,
-             "cluster-pair list radius %g needs every box length above %g.", rlist, 2 * rlist);
-    const double rho = N / (Lx * Ly * Lz);
-    const double b = std::cbrt(SUPER / rho);
-    int ncx = std::max(1, (int)std::floor(Lx / b)), ncy = std::max(1, (int)std::floor(Ly / b));
-    int ncol = ncx * ncy;
-    int nzb = std::max(1, (int)std::nearbyint(Lz * rho * (Lx / ncx) * (Ly / ncy) / 4));
-    long long nbin = (long long)ncol * nzb;
-    PD_CHECK(nbin < (1LL << 30), PD_EINVAL, "cluster-pair binning exceeds int range.");
-    int nsmax = (N + SUPER - 1) / SUPER + ncol;
-    int nslot = SUPER * nsmax;
-    const double shrink = 0.98;
-    int mx = (int)std::floor(rlist / (shrink * Lx / ncx)) + 1;
-    int my = (int)std::floor(rlist / (shrink * Ly / ncy)) + 1;
-    const int ncs = std::min(2 * mx + 1, ncx) * std::min(2 * my + 1, ncy);
-    PD_CHECK(ncs <= SEARCH_MAX_COLS, PD_EINVAL, "cluster-pair search needs %d columns per super-cluster (limit %d).",
-             ncs, SEARCH_MAX_COLS);
+    ClusterGeom g;
+    int grc = cluster_geometry(N, c->p.rmax + c->p.skin, box, &g);
+    if (grc) return grc;
+    const double rlist = g.rlist, rho = g.rho;
+    const int ncx = g.ncx, ncy = g.ncy, ncol = g.ncol, nzb = g.nzb, nsmax = g.nsmax, nslot = g.nslot;
+    const int mx = g.mx, my = g.my, ncs = g.ncs;
+    const long long nbin = g.nbin;
     bool same_geom = c->nslot > 0 && ncx == c->ncx && ncy == c->ncy && nzb == c->nzb && nsmax == c->nsmax &&
                      ncs == c->ncs;
     for (int d = 0; d < 3; ++d) {

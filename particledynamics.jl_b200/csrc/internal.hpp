@@ -74,6 +74,19 @@ struct PairParams {
     float pf[PD_MAX_POLY];
 };
 
+// Geometry of the cluster list for n particles in a box (the setup! rules, List.jl:874-937).
+struct ClusterGeom {
+    int ncx, ncy, ncol, nzb, nsmax, nslot, mx, my, ncs;
+    long long nbin;
+    double rho, rlist;
+};
+// Argument checks of an engine's parameters (shared by every cluster entry point that takes them).
+int cluster_check_params(const pd_cluster_params *p);
+// The box checks and geometry rules for n particles and list radius rlist; PD_EINVAL on a bad box.
+int cluster_geometry(int n, double rlist, const double box[3], ClusterGeom *g);
+// Pair-kernel parameters of an engine (box lengths from box, the rest from p).
+void cluster_pair_params(const pd_cluster_params *p, const double box[3], PairParams *pp);
+
 }  // namespace pdb
 
 struct pd_cluster {

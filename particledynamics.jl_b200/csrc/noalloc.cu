@@ -1,11 +1,15 @@
 // Allocation-free cluster-pair force evaluation (pd_cluster_compute_static).
 //
-// Some callers cannot call cudaMalloc: a host that has already sized its
-// device memory pool to the byte and forbids further allocation, a caller in
-// the middle of building a CUDA graph region, or a real-time loop that must
-// not enter the allocator.  For them this file keeps one file-scope device
-// arena and runs the ordinary build -> prune -> pair -> scatter sequence of
-// the cluster-pair engine with every scratch buffer carved out of it.
+// Some callers cannot call cudaMalloc: a plugin inside a host program whose
+// own memory pool has already claimed the device memory (a Julia CUDA.jl
+// session, a PyTorch process with its caching allocator), so that a direct
+// cudaMalloc fails or escapes the pool's accounting; a host that has sized
+// its device memory to the byte and forbids further allocation; or a
+// real-time loop that must not enter the allocator, because cudaMalloc can
+// synchronise the device and take unbounded time.  For them this file keeps
+// one file-scope device arena and runs the ordinary build -> prune -> pair ->
+// scatter sequence of the cluster-pair engine with every scratch buffer carved
+// out of it.
 //
 // Properties of the arena (PD_STATIC_SCRATCH_BYTES, 4 MiB): it exists on every
 // GPU that loads libpdb200 until the process exits; all calls share it and it
@@ -14,7 +18,11 @@
 // (different streams, or different host threads) race on it.  The host needs
 // the arena's device address, which it obtains once per device with
 // cudaGetSymbolAddress on the first call made while that device is current;
-// make that first call before any stream capture begins.
+// make that first call before any stream capture begins.  The call reads the
+// list's status word back at its end, so it synchronises its stream.  On a list
+// failure (PD_ECAPACITY, PD_ENONFINITE) the outputs have already been
+// overwritten with the empty pair pass's result (no pair forces) when the error
+// is returned.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -76,82 +84,45 @@ extern "C" int pd_cluster_compute_static(const pd_cluster_params *p, const doubl
                                          float *fy, float *fz, float *epot, float *vir6, int energy, pd_stream_t sp) {
     PD_CHECK(p && box && x && y && z && fx && fy && fz, PD_EINVAL, "pd_cluster_compute_static: null argument");
     PD_CHECK(!energy || epot, PD_EINVAL, "pd_cluster_compute_static: energy needs epot");
-    PD_CHECK(p->n >= 1 && p->n <= PD_STATIC_MAX_N, PD_EINVAL,
+    int rc = cluster_check_params(p);
+    if (rc) return rc;
+    PD_CHECK(p->n <= PD_STATIC_MAX_N, PD_EINVAL,
              "pd_cluster_compute_static: %d particles; the static scratch serves 1..%d", p->n, PD_STATIC_MAX_N);
-    PD_CHECK(p->skin >= 0 && p->prune_buffer >= 0 && p->prune_buffer <= p->skin && p->rmax > 0, PD_EINVAL,
-             "pd_cluster_compute_static: need rmax > 0 and 0 <= prune_buffer <= skin");
-    PD_CHECK(p->lj_kind >= PD_LJ_NONE && p->lj_kind <= PD_LJ_TABLE, PD_EINVAL, "unknown LJ kind %d", p->lj_kind);
-    PD_CHECK(p->lj_kind != PD_LJ_TABLE || (p->ntypes >= 1 && p->ntypes <= PD_MAX_TYPES), PD_EINVAL,
-             "LJ type table needs 1 <= ntypes <= %d", PD_MAX_TYPES);
-    PD_CHECK(!p->coulomb || (p->coul_ne >= 1 && p->coul_ne <= PD_MAX_POLY && p->coul_nf >= 1 &&
-                             p->coul_nf <= PD_MAX_POLY),
-             PD_EINVAL, "Coulomb polynomial needs 1..%d coefficients", PD_MAX_POLY);
     cudaStream_t s = (cudaStream_t)sp;
 
-    // geometry of this box (the setup! rules, without allocation)
+    // geometry of this box: the rules pd_cluster_setup applies, without its allocations
     pd_cluster c;
     c.p = *p;
     c.n = p->n;
     const int N = p->n;
-    const double rlist = p->rmax + p->skin;
-    const double Lx = (float)box[0], Ly = (float)box[1], Lz = (float)box[2];
-    PD_CHECK(std::isfinite(Lx) && std::isfinite(Ly) && std::isfinite(Lz) && Lx > 0 && Ly > 0 && Lz > 0, PD_EINVAL,
-             "box lengths must be finite and positive");
-    PD_CHECK(std::min(Lx, std::min(Ly, Lz)) > 2 * rlist, PD_EINVAL,
-             "cluster-pair list radius %g needs every box length above %g.", rlist, 2 * rlist);
-    const double rho = N / (Lx * Ly * Lz);
-    const double b = std::cbrt(SUPER / rho);
-    c.ncx = std::max(1, (int)std::floor(Lx / b));
-    c.ncy = std::max(1, (int)std::floor(Ly / b));
-    c.ncol = c.ncx * c.ncy;
-    c.nzb = std::max(1, (int)std::nearbyint(Lz * rho * (Lx / c.ncx) * (Ly / c.ncy) / 4));
-    const long long nbin = (long long)c.ncol * c.nzb;
-    PD_CHECK(nbin <= 4LL * PD_STATIC_MAX_N, PD_EINVAL, "pd_cluster_compute_static: %lld z-bins exceed the static "
-             "scratch", nbin);
-    c.nbin = (int)nbin;
-    c.nsmax = (N + SUPER - 1) / SUPER + c.ncol;
-    c.nslot = SUPER * c.nsmax;
-    c.mx = (int)std::floor(rlist / (0.98 * Lx / c.ncx)) + 1;
-    c.my = (int)std::floor(rlist / (0.98 * Ly / c.ncy)) + 1;
-    c.ncs = std::min(2 * c.mx + 1, c.ncx) * std::min(2 * c.my + 1, c.ncy);
-    PD_CHECK(c.ncs <= SEARCH_MAX_COLS, PD_EINVAL, "pd_cluster_compute_static: %d search columns exceed %d", c.ncs,
-             SEARCH_MAX_COLS);
+    ClusterGeom g;
+    if ((rc = cluster_geometry(N, p->rmax + p->skin, box, &g))) return rc;
+    PD_CHECK(g.nbin <= 4LL * PD_STATIC_MAX_N, PD_EINVAL, "pd_cluster_compute_static: %lld z-bins exceed the static "
+             "scratch", g.nbin);
+    c.ncx = g.ncx;
+    c.ncy = g.ncy;
+    c.ncol = g.ncol;
+    c.nzb = g.nzb;
+    c.nbin = (int)g.nbin;
+    c.nsmax = g.nsmax;
+    c.nslot = g.nslot;
+    c.mx = g.mx;
+    c.my = g.my;
+    c.ncs = g.ncs;
+    c.rlist = g.rlist;
     for (int d = 0; d < 3; ++d) {
         c.box[d] = box[d];
         c.L[d] = (float)box[d];
     }
-    c.rlist = rlist;
     int dev = 0;
     PD_CUDA(cudaGetDevice(&dev));
     PD_CUDA(cudaDeviceGetAttribute(&c.num_sms, cudaDevAttrMultiProcessorCount, dev));
     c.nsplit = std::max(1, std::min(32, (32 * c.num_sms + c.nsmax - 1) / std::max(c.nsmax, 1)));
-    PairParams &pp = c.pp;
-    memset(&pp, 0, sizeof pp);
-    pp.Lx = c.L[0];
-    pp.Ly = c.L[1];
-    pp.Lz = c.L[2];
-    pp.lj_kind = p->lj_kind;
-    pp.c6 = p->lj_c6;
-    pp.c12 = p->lj_c12;
-    pp.lrc2 = p->lj_rc2;
-    pp.esh = p->lj_esh;
-    pp.ntypes = p->lj_kind == PD_LJ_TABLE ? p->ntypes : 1;
-    pp.coulomb = p->coulomb;
-    pp.C = p->coul_C;
-    pp.rc2 = p->coul_rc2;
-    pp.sx = p->coul_sx;
-    pp.eshift = p->coul_eshift;
-    pp.ne = p->coulomb ? p->coul_ne : 1;
-    pp.nf = p->coulomb ? p->coul_nf : 1;
-    for (int k = 0; k < PD_MAX_POLY; ++k) {   // coefficients past the fitted length are zero (exact padding)
-        pp.pe[k] = k < pp.ne ? p->coul_pe[k] : 0.f;
-        pp.pf[k] = k < pp.nf ? p->coul_pf[k] : 0.f;
-    }
+    cluster_pair_params(p, box, &c.pp);
 
     // carve every buffer of the list out of the arena
     void *base = nullptr;
-    int rc = arena_address(&base);
-    if (rc) return rc;
+    if ((rc = arena_address(&base))) return rc;
     Carver cv{reinterpret_cast<unsigned char *>(base)};
     c.counts = cv.take<int>(W_LEN);
     c.bin = cv.take<int>(N);

@@ -11,7 +11,8 @@ taken from the text of its own test files:
 * test/test_electrostatics.jl:299-309 -- the solver cases (box, C, r_c, alpha,
   mesh, order) and their force / energy tolerances against the Ewald oracle.
 
-Run with the reference checked out at REFERENCE_ROOT (default /root/reference).
+Run with REFERENCE_ROOT set to a checkout of the reference (ParticleDynamics.jl v0.7.0):
+``REFERENCE_ROOT=<checkout> python tests/golden/make_fixtures.py``.
 """
 from __future__ import annotations
 
@@ -21,7 +22,9 @@ import re
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REF = Path(os.environ.get("REFERENCE_ROOT", "/root/reference"))
+if "REFERENCE_ROOT" not in os.environ:
+    raise SystemExit("set REFERENCE_ROOT to a checkout of ParticleDynamics.jl v0.7.0")
+REF = Path(os.environ["REFERENCE_ROOT"])
 
 
 def _lines(rel: str) -> list[str]:
