@@ -276,7 +276,9 @@ typedef struct {
     float *vglobal6;           /* mesh virial (energy steps), 6 floats */
 } pd_md_state;
 
-/* The engine borrows c, m (may be NULL) and the state arrays for its lifetime. */
+/* The engine borrows c, m (may be NULL) and the state arrays for its lifetime.  The mesh may use
+ * any influence kind: SPME and P3M-AD gather with analytic derivatives, P3M-ik from its three
+ * field grids. */
 int pd_md_create(pd_md **out, pd_cluster *c, pd_mesh *m, const pd_md_state *st, double box[3]);
 int pd_md_destroy(pd_md *md);
 /* evaluate_forces_into_f!(st, energy) (src/simulation/ForceEvaluation.jl:40-44): forces (and

@@ -112,6 +112,28 @@ def pairs_cells(pos, box, *, q=None, kind=1, sigma=1.0, eps=1.0, rc_lj=2.5, eshi
     return dict(F=np.stack([fx, fy, fz], 1), E=e, W=w)
 
 
+def pair_force_abs_sums(pos, box, *, kind=1, sigma=1.0, eps=1.0, rc_lj=2.5):
+    """S_i = sum_j |f_ij| over the LJ (kind 1) or WCA (kind 2) pairs inside r_c, in FP64: the scale of
+    the rounding error of an FP32 sum of pair forces (each pair force is computed to a few ulps of its
+    own magnitude, so |F_i(FP32) - F_i| stays within a small multiple of eps_32 S_i however much the
+    pair forces cancel in F_i)."""
+    from scipy.spatial import cKDTree
+    L = np.asarray(box, float)
+    p = np.asarray(pos, float) % L
+    tree = cKDTree(p, boxsize=L)
+    ij = tree.query_pairs(rc_lj, output_type="ndarray")
+    d = p[ij[:, 0]] - p[ij[:, 1]]
+    d -= L * np.round(d / L)
+    r2 = (d * d).sum(1)
+    ir2 = sigma * sigma / r2
+    ir6 = ir2 * ir2 * ir2
+    f = np.abs(24.0 * eps * (2.0 * ir6 - 1.0) * ir6 / np.sqrt(r2))
+    S = np.zeros(len(p))
+    np.add.at(S, ij[:, 0], f)
+    np.add.at(S, ij[:, 1], f)
+    return S
+
+
 def neighbor_rows(pos, box, radius, cap=512):
     """reference_neighbor_rows (test/neighbor_reference.jl:6-16): sorted rows of j within radius."""
     L = _load()
@@ -291,6 +313,42 @@ def pme_total(pos, q, box, *, C, alpha, rc, K, P, kind="spme", nmax=2, lj=None, 
 
 
 # ------------------------------------------------------------------ cluster list
+
+def displacement_ratios(pos, ref_build, ref_prune, box, skin, prune_buffer):
+    """Largest minimum-image |r - r_build|^2 / (skin/2)^2 and the larger of that and
+    |r - r_prune|^2 / (prune_buffer/2)^2 over the particles (_displacement_kernel!,
+    src/clusterpairs/List.jl:799-825; a zero threshold gives inf for any motion)."""
+    L = np.asarray(box, float)
+
+    def ratio(ref, half):
+        d = np.asarray(pos, float) - np.asarray(ref, float)
+        d -= L * np.round(d / L)
+        d2 = (d * d).sum(1)
+        if half == 0.0:
+            return np.where(d2 > 0, np.inf, 0.0)
+        r = d2 / (half * half)
+        return np.where(np.isfinite(r), r, np.inf)
+
+    rb = ratio(ref_build, 0.5 * skin)
+    rp = ratio(ref_prune, 0.5 * prune_buffer)
+    return float(rb.max()), float(np.maximum(rb, rp).max())
+
+
+def list_decision(build_ratio, any_ratio, *, request=False, nstlist=0, nstprune=0, k=0):
+    """(build, prune) of the device decision (_decide_kernel!, src/clusterpairs/Engine.jl:301-324).
+
+    Triggers (nstlist = 0): rebuild when a particle moved more than skin/2 since the build or on
+    request, prune after a rebuild or when one moved more than prune_buffer/2 since the prune.
+    Fixed intervals: rebuild at decision k % nstlist == 0, on request or on non-finite motion; prune
+    after a rebuild or at k % nstprune == 0."""
+    if nstlist > 0:
+        build = (k % nstlist == 0) or request or not math.isfinite(build_ratio)
+        prune = build or (nstprune > 0 and k % nstprune == 0)
+    else:
+        build = build_ratio > 1.0 or request
+        prune = build or any_ratio > 1.0
+    return bool(build), bool(prune)
+
 
 def force_coordinate(x, L):
     """force_coordinate (PeriodicDisplacement.jl:21-25) in Float32."""

@@ -332,8 +332,6 @@ int pd_md_create(pd_md **out, pd_cluster *c, pd_mesh *m, const pd_md_state *st, 
     PD_CHECK(st->x && st->y && st->z && st->vx && st->vy && st->vz && st->fx && st->fy && st->fz, PD_EINVAL,
              "pd_md_create: state arrays missing");
     PD_CHECK(!m || st->q, PD_EINVAL, "pd_md_create: a mesh needs charges");
-    PD_CHECK(!m || m->p.kind != PD_MESH_P3M_IK, PD_ENOTSUP,
-             "pd_md_create: the fused step supports analytic differentiation (SPME, P3M-AD)");
     PD_CHECK(!m || m->p.nmax >= 0, PD_EINVAL, "bad mesh");
     pd_md *md = new pd_md();
     md->c = c;

@@ -415,11 +415,19 @@ __device__ __forceinline__ float4 self_force(const float4 *__restrict__ tab, int
     return r;
 }
 
-template <int P, int MODE, bool ENERGY>   // MODE 0: add, 1: set, 2: join (+ kick)
+// Grids a gather reads: AD the potential (g[0]); ik the three field components (g[0..2]) and, with
+// energy, the potential (g[3]).
+struct GatherGrids {
+    const float *g[4];
+};
+
+// IK: the ik gather (_gather_ik_kernel!, MeshKernels.jl:105-147), F_i = q_i sum W E, with the three
+// field grids staged through the same brick one after another.
+template <int P, int MODE, bool ENERGY, bool IK>   // MODE 0: add, 1: set, 2: join (+ kick)
 __global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_gather(const float4 *__restrict__ xq, int nchunks,
-                                                         const int *__restrict__ nchunk_dev,
-                                                         const float *__restrict__ grid, int K1, int K2, int K3,
-                                                         float Lx, float Ly, float Lz, GatherOut o) {
+                                                         const int *__restrict__ nchunk_dev, GatherGrids grids,
+                                                         int K1, int K2, int K3, float Lx, float Ly, float Lz,
+                                                         GatherOut o) {
     const int c = blockIdx.x;
     if (nchunk_dev && c >= *nchunk_dev) return;
     if (c >= nchunks) return;
@@ -452,17 +460,81 @@ __global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_gather(const
         u1 = grid_coordinate(v.x, Lx, K1);
         u2 = grid_coordinate(v.y, Ly, K2);
         u3 = grid_coordinate(v.z, Lz, K3);
-        k1 = bspline<P>(u1, w1, g1);
-        k2 = bspline<P>(u2, w2, g2);
-        k3 = bspline<P>(u3, w3, g3);
+        k1 = bspline<P>(u1, w1, IK ? nullptr : g1);
+        k2 = bspline<P>(u2, w2, IK ? nullptr : g2);
+        k3 = bspline<P>(u3, w3, IK ? nullptr : g3);
     }
     int d1 = 0, d2 = 0, d3 = 0;
     Brick b;
     chunk_brick<P>(charged, k1, k2, k3, K1, K2, K3, d1, d2, d3, b, sm, rowbase);
     constexpr int PH = (P + 1) / 2;
+    constexpr int NG = IK ? (ENERGY ? 4 : 3) : 1;   // grids read one after another
 
     float phi = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-    if (b.fits) {
+    if (IK && b.fits) {
+#pragma unroll 1
+        for (int gi = 0; gi < NG; ++gi) {
+            const float *grid = grids.g[gi];
+            if (gi > 0) __syncthreads();   // every thread is done with the previous grid's brick
+            if (b.vec) {
+                float4 *tile4 = reinterpret_cast<float4 *>(tile);
+                for_brick(b, rowbase, K1, [&](int kt, size_t kg) {
+                    tile4[kt] = __ldg(reinterpret_cast<const float4 *>(grid + kg));
+                });
+            } else {
+                for_brick(b, rowbase, K1, [&](int kt, size_t kg) { tile[kt] = __ldg(grid + kg); });
+            }
+            __syncthreads();
+            if (charged) {
+                float acc = 0.f;
+#pragma unroll
+                for (int j3 = 0; j3 < P; ++j3) {   // this half's z nodes only (warp-uniform test)
+                    if ((j3 < PH) != (h == 0)) continue;
+                    float s0 = 0.f;
+#pragma unroll
+                    for (int j2 = 0; j2 < P; ++j2) {
+                        const float *row = tile + ((d3 + j3) * b.e2 + (d2 + j2)) * b.e1 + d1;
+                        float a0 = 0.f;
+#pragma unroll
+                        for (int j1 = 0; j1 < P; ++j1) a0 = fmaf(w1[j1], row[j1], a0);
+                        s0 = fmaf(w2[j2], a0, s0);
+                    }
+                    acc = fmaf(w3[j3], s0, acc);
+                }
+                if (gi == 0) gx = acc;
+                else if (gi == 1) gy = acc;
+                else if (gi == 2) gz = acc;
+                else phi = acc;
+            }
+        }
+    } else if (IK && charged) {
+#pragma unroll 1
+        for (int gi = 0; gi < NG; ++gi) {
+            const float *grid = grids.g[gi];
+            float acc = 0.f;
+#pragma unroll
+            for (int j3 = 0; j3 < P; ++j3) {   // this half's z nodes only (warp-uniform test)
+                if ((j3 < PH) != (h == 0)) continue;
+                const int n3 = wrap_node(k3 + j3, K3);
+                float s0 = 0.f;
+#pragma unroll
+                for (int j2 = 0; j2 < P; ++j2) {
+                    const int n2 = wrap_node(k2 + j2, K2);
+                    float a0 = 0.f;
+#pragma unroll
+                    for (int j1 = 0; j1 < P; ++j1)
+                        a0 = fmaf(w1[j1], grid[((size_t)n3 * K2 + n2) * K1 + wrap_node(k1 + j1, K1)], a0);
+                    s0 = fmaf(w2[j2], a0, s0);
+                }
+                acc = fmaf(w3[j3], s0, acc);
+            }
+            if (gi == 0) gx = acc;
+            else if (gi == 1) gy = acc;
+            else if (gi == 2) gz = acc;
+            else phi = acc;
+        }
+    } else if (b.fits) {
+        const float *grid = grids.g[0];
         if (b.vec) {
             float4 *tile4 = reinterpret_cast<float4 *>(tile);
             for_brick(b, rowbase, K1, [&](int kt, size_t kg) {
@@ -498,6 +570,7 @@ __global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_gather(const
             }
         }
     } else if (charged) {
+        const float *grid = grids.g[0];
 #pragma unroll
         for (int j3 = 0; j3 < P; ++j3) {   // this half's z nodes only (warp-uniform test)
             if ((j3 < PH) != (h == 0)) continue;
@@ -539,11 +612,17 @@ __global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_gather(const
     const float qi = v.w;
     float Fx = 0.f, Fy = 0.f, Fz = 0.f, Ei = 0.f;
     if (charged) {
-        Fx = -(qi * gx * ((float)K1 / Lx));
-        Fy = -(qi * gy * ((float)K2 / Ly));
-        Fz = -(qi * gz * ((float)K3 / Lz));
+        if (IK) {
+            Fx = qi * gx;
+            Fy = qi * gy;
+            Fz = qi * gz;
+        } else {
+            Fx = -(qi * gx * ((float)K1 / Lx));
+            Fy = -(qi * gy * ((float)K2 / Ly));
+            Fz = -(qi * gz * ((float)K3 / Lz));
+        }
         if (ENERGY) Ei = 0.5f * qi * phi + o.bg * qi;
-        if (o.self_tab) {   // remove the charge's own force through the mesh: F -= q^2 S(u)
+        if (!IK && o.self_tab) {   // remove the charge's own force through the mesh: F -= q^2 S(u)
             const float4 sf = self_force(o.self_tab, o.self_T, u1, u2, u3);
             const float q2 = qi * qi;
             Fx = fmaf(-q2, sf.x, Fx);
@@ -586,61 +665,6 @@ __global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_gather(const
             o.fz[id] += Fz;
             if (ENERGY) o.epot[id] += Ei;
         }
-    }
-}
-
-// ik gather (_gather_ik_kernel!, MeshKernels.jl:105-147): one thread per entry.
-template <int P, bool ENERGY>
-__global__ void k_gather_ik(const float4 *__restrict__ xq, int n, const int *__restrict__ ids,
-                            const float *__restrict__ ex, const float *__restrict__ ey, const float *__restrict__ ez,
-                            const float *__restrict__ pot, int K1, int K2, int K3, float Lx, float Ly, float Lz,
-                            float bg, int set, float *__restrict__ fx, float *__restrict__ fy, float *__restrict__ fz,
-                            float *__restrict__ epot) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const int i = ids ? ids[t] : t;
-    const float4 v = xq[t];
-    const float qi = v.w;
-    if (qi == 0.f) {
-        if (set) {
-            fx[i] = 0.f;
-            fy[i] = 0.f;
-            fz[i] = 0.f;
-            if (ENERGY) epot[i] = 0.f;
-        }
-        return;
-    }
-    float w1[P], w2[P], w3[P];
-    const int k1 = bspline<P>(grid_coordinate(v.x, Lx, K1), w1, nullptr);
-    const int k2 = bspline<P>(grid_coordinate(v.y, Ly, K2), w2, nullptr);
-    const int k3 = bspline<P>(grid_coordinate(v.z, Lz, K3), w3, nullptr);
-    float sx = 0.f, sy = 0.f, sz = 0.f, phi = 0.f;
-    for (int j3 = 0; j3 < P; ++j3) {
-        const int n3 = wrap_node(k3 + j3, K3);
-        for (int j2 = 0; j2 < P; ++j2) {
-            const int n2 = wrap_node(k2 + j2, K2);
-            const float w23 = w2[j2] * w3[j3];
-            const size_t base = ((size_t)n3 * K2 + n2) * K1;
-            for (int j1 = 0; j1 < P; ++j1) {
-                const size_t l = base + wrap_node(k1 + j1, K1);
-                const float ww = w23 * w1[j1];
-                sx += ww * ex[l];
-                sy += ww * ey[l];
-                sz += ww * ez[l];
-                if (ENERGY) phi += ww * pot[l];
-            }
-        }
-    }
-    if (set) {
-        fx[i] = qi * sx;
-        fy[i] = qi * sy;
-        fz[i] = qi * sz;
-        if (ENERGY) epot[i] = 0.5f * qi * phi + bg * qi;
-    } else {
-        fx[i] += qi * sx;
-        fy[i] += qi * sy;
-        fz[i] += qi * sz;
-        if (ENERGY) epot[i] += 0.5f * qi * phi + bg * qi;
     }
 }
 
@@ -1048,9 +1072,18 @@ static void launch_gather(pd_mesh *m, const float4 *xq, int nchunks, const int *
                           cudaStream_t s) {
     const float Lx = (float)m->box[0], Ly = (float)m->box[1], Lz = (float)m->box[2];
     const int K1 = m->K1, K2 = m->K2, K3 = m->K3;
-    const float *g = m->gridB;
-#define PD_G(PP) \
-    case PP: k_gather<PP, MODE, ENERGY><<<nchunks, MESH_THREADS, 0, s>>>(xq, nchunks, ns_dev, g, K1, K2, K3, Lx, Ly, Lz, o); break;
+    const bool ik = m->p.kind == PD_MESH_P3M_IK;
+    GatherGrids g = {{m->gridB, nullptr, nullptr, nullptr}};
+    if (ik) g = GatherGrids{{m->field[0], m->field[1], m->field[2], m->gridB}};
+#define PD_G(PP)                                                                                                       \
+    case PP:                                                                                                           \
+        if (ik)                                                                                                        \
+            k_gather<PP, MODE, ENERGY, true><<<nchunks, MESH_THREADS, 0, s>>>(xq, nchunks, ns_dev, g, K1, K2, K3, Lx,  \
+                                                                              Ly, Lz, o);                              \
+        else                                                                                                           \
+            k_gather<PP, MODE, ENERGY, false><<<nchunks, MESH_THREADS, 0, s>>>(xq, nchunks, ns_dev, g, K1, K2, K3, Lx, \
+                                                                               Ly, Lz, o);                             \
+        break;
     switch (m->p.order) {
         PD_G(3) PD_G(4) PD_G(5) PD_G(6) PD_G(7) PD_G(8) PD_G(9) PD_G(10) PD_G(11) PD_G(12)
         default: break;
@@ -1063,7 +1096,6 @@ int mesh_gather_join(pd_mesh *m, pd_cluster *c, const float4 *xq, const int *per
                      float inv_mass_uniform, float half_dt, float *epot, float *vir6, float *vglobal6, const float *q,
                      float half_c_self, const float4 *extra, int energy, cudaStream_t s) {
     (void)q;
-    PD_CHECK(m->p.kind != PD_MESH_P3M_IK, PD_ENOTSUP, "the fused gather step supports analytic differentiation only");
     GatherOut o;
     memset(&o, 0, sizeof o);
     o.fx = fx;
@@ -1274,28 +1306,7 @@ int pd_mesh_gather(pd_mesh *m, const float *x, const float *y, const float *z, c
                                                                          m->packed);
         PD_LAUNCHED();
     }
-    const float Lx = (float)m->box[0], Ly = (float)m->box[1], Lz = (float)m->box[2];
-    if (m->p.kind == PD_MESH_P3M_IK) {
-#define PD_GIK(PP)                                                                                               \
-    case PP:                                                                                                     \
-        if (energy)                                                                                              \
-            k_gather_ik<PP, true><<<(n + 127) / 128, 128, 0, st>>>(m->packed, n, order, m->field[0], m->field[1], \
-                                                                   m->field[2], m->gridB, m->K1, m->K2, m->K3, Lx, \
-                                                                   Ly, Lz, m->bg, set, fx, fy, fz, epot);          \
-        else                                                                                                     \
-            k_gather_ik<PP, false><<<(n + 127) / 128, 128, 0, st>>>(m->packed, n, order, m->field[0], m->field[1], \
-                                                                    m->field[2], m->gridB, m->K1, m->K2, m->K3, Lx, \
-                                                                    Ly, Lz, m->bg, set, fx, fy, fz, epot);          \
-        break;
-        if (n > 0) {
-            switch (m->p.order) {
-                PD_GIK(3) PD_GIK(4) PD_GIK(5) PD_GIK(6) PD_GIK(7) PD_GIK(8) PD_GIK(9) PD_GIK(10) PD_GIK(11) PD_GIK(12)
-                default: break;
-            }
-            PD_LAUNCHED();
-        }
-#undef PD_GIK
-    } else if (n > 0) {
+    if (n > 0) {
         GatherOut o;
         memset(&o, 0, sizeof o);
         o.fx = fx;
