@@ -201,19 +201,24 @@ int pd_cluster_buffers(pd_cluster *c, const int **perm, const float **xq, const 
 
 /* ======================================================================
  * Mesh engine: ElectrostaticsSolver / MeshWorkspace (src/electrostatics/Solver.jl:17-158)
- * for SPME (B-spline window, exact deconvolution) and P3M with the optimal influence
- * function for analytic (AD) or ik differentiation.  cuFFT does the transforms.
+ * for SPME (B-spline window, exact deconvolution), P3M with the optimal influence
+ * function for analytic (AD) or ik differentiation, and ESP (prolate split and window,
+ * optimal AD influence or plain deconvolution).  cuFFT does the transforms.
  * ====================================================================== */
 typedef struct pd_mesh pd_mesh;
 
-enum pd_mesh_kind { PD_MESH_SPME = 1, PD_MESH_P3M_AD = 2, PD_MESH_P3M_IK = 3 };
+/* influence kinds :spme, :p3m_ad, :p3m_ik, :esp, :esp_deconvolution (Spec.jl:5) */
+enum pd_mesh_kind {
+    PD_MESH_SPME = 1, PD_MESH_P3M_AD = 2, PD_MESH_P3M_IK = 3, PD_MESH_ESP = 4, PD_MESH_ESP_DECONV = 5
+};
 
 typedef struct {
-    int kind;               /* pd_mesh_kind (influence :spme, :p3m_ad, :p3m_ik, Spec.jl:5) */
-    int order;              /* B-spline order P, 3..12 (BSplineWindow, Windows.jl:18-24) */
+    int kind;               /* pd_mesh_kind */
+    int order;              /* window width P, 3..12: the B-spline order (BSplineWindow, Windows.jl:18-24)
+                             * or the prolate window's grid points (ProlateWindow, Windows.jl:38-54) */
     int alias_order;        /* P3M alias sums |n| <= alias_order, 0..6 */
     int mesh[3];            /* K1, K2, K3 (resolve_mesh, Spec.jl:141-146) */
-    double alpha;           /* Gaussian split parameter */
+    double alpha;           /* Gaussian split parameter (SPME, P3M; unused by ESP) */
     double C;               /* coulomb_prefactor / relative_permittivity */
     int background;         /* net_charge = :background (Solver.jl:179-185) */
     double qtotal;          /* total charge (background term) */
@@ -221,6 +226,31 @@ typedef struct {
 } pd_mesh_params;
 
 int pd_mesh_create(pd_mesh **out, const pd_mesh_params *p, const double box[3]);
+
+/* Prolate split and window of an ESP mesh: what the reference's host setup computes in FP64
+ * (ProlateSplit, Splits.jl:37-60; ProlateWindow and its device stencil, Windows.jl:38-135;
+ * window_deconvolution / window_alias_table, Windows.jl:367-411).  The influence function is then
+ * computed on the device with the exact quadrature of the split's transform
+ * (compute_influence!, Influence.jl:190-227). */
+#define PD_PROLATE_MAX_QUAD 256
+#define PD_PROLATE_MAX_DEG 24
+#define PD_PROLATE_MAX_NODES 8
+typedef struct {
+    double cutoff;          /* r_c of the split: g(k) = 4 pi c_hat(k r_c) / k^2 */
+    int nquad;              /* quadrature of c_hat(u) = sum_q wchi[q] cos(u xq[q]), 1..PD_PROLATE_MAX_QUAD */
+    double xq[PD_PROLATE_MAX_QUAD];    /* nodes on [0, 1] */
+    double wchi[PD_PROLATE_MAX_QUAD];  /* quadrature weights times chi(xq) */
+    double background_coefficient;     /* pi r_c^2 m_2 (background energy -C coef Q^2 / V) */
+    int deg;                /* degree of the node polynomials, 1..PD_PROLATE_MAX_DEG */
+    double poly[PD_PROLATE_MAX_DEG + 1][PD_PROLATE_MAX_NODES];  /* [k][h]: coefficient of tau^k of
+                             * node h < ceil(P/2) (ProlatePolyStencil, Windows.jl:63-72) */
+    const double *table[3]; /* per axis d: PD_MESH_ESP_DECONV the deconvolution 1/phi_hat^2 (K_d values);
+                             * PD_MESH_ESP the alias table phi_hat(theta_m + 2 pi n), (2 alias_order + 1)
+                             * values per mode m, m-major (entry m (2 alias_order + 1) + n + alias_order) */
+} pd_prolate;
+/* ElectrostaticsSolver(spec) for an ESP spec (p->kind PD_MESH_ESP or PD_MESH_ESP_DECONV).  Copies the
+ * tables.  The gather is the AD gather with the prolate window; self-force removal is not offered. */
+int pd_mesh_create_prolate(pd_mesh **out, const pd_mesh_params *p, const pd_prolate *w, const double box[3]);
 int pd_mesh_destroy(pd_mesh *m);
 /* refresh_geometry!(solver, box) (Solver.jl:193-209): FP64 influence function and virial
  * coefficients on the device for a new box (compute_influence!, Influence.jl:190-227). */

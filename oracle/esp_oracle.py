@@ -57,11 +57,10 @@ class Psi:
         t = np.asarray(t, float)
         return (-(np.sin(self.c * np.multiply.outer(t, self.x)) * (self.c * self.x)) @ (self.w * self.v)) / self.lam
 
-    def integral(self, t, n=64):
-        """int_0^t psi."""
+    def integral(self, t):
+        """int_0^t psi, in closed form from the Nystrom representation (the integral of each cosine)."""
         t = np.atleast_1d(np.asarray(t, float))
-        u, wu = gl(n, 0.0, 1.0)
-        return (self(np.multiply.outer(t, u)) @ wu) * t
+        return (np.sin(self.c * np.multiply.outer(t, self.x)) / (self.c * self.x)) @ (self.w * self.v) / self.lam
 
     def l2_norm(self):
         return math.sqrt(float((self.w * self(self.x) ** 2).sum()))
@@ -87,7 +86,7 @@ class Split:
         self.psi = Psi(shape)
         self.norm = float(self.psi.integral(1.0)[0])
         self.chi0 = 1.0 / self.norm
-        xq, wq = gl(256, 0.0, 1.0)
+        xq, wq = gl(128, 0.0, 1.0)
         chi = self.psi(xq) / self.norm
         self.m2 = float((wq * xq ** 2 * chi).sum())
         self.xq, self.wchi = xq, wq * chi
@@ -254,7 +253,7 @@ def mesh(pos, q, box, K, window, split, kind="esp", C=1.0, nmax=2, background=Fa
     a2 = wgt * np.abs(spec) ** 2
     Emesh = float((a2 * G3).sum())
     Wm = np.array([float((a2 * Vc[c].reshape(spec.shape)).sum()) for c in range(6)])
-    pot = np.fft.irfftn(spec * G3, s=(K[2], K[1], K[0])) * (K[0] * K[1] * K[2])
+    pot = np.fft.irfftn(spec * G3, s=(K[2], K[1], K[0]), axes=(0, 1, 2)) * (K[0] * K[1] * K[2])
     d1, d2, d3 = st[0][2], st[1][2], st[2][2]
     phi = np.zeros(n)
     gx = np.zeros(n)
@@ -290,16 +289,15 @@ def pairs(pos, q, box, split, C=1.0):
         d = pos[a:a + 256, None, :] - pos[None, :, :]
         d -= L * np.round(d / L)
         r2 = (d * d).sum(-1)
-        mask = (r2 > 0) & (r2 < split.rc ** 2)
-        r = np.sqrt(np.where(mask, r2, 1.0))
-        e, f = split.pair(r)
-        qq = C * q[a:a + 256, None] * q[None, :]
-        e = np.where(mask, e * qq, 0.0)
-        f = np.where(mask, f * qq, 0.0)
-        F[a:a + 256] += (f[..., None] * d).sum(1)
-        E[a:a + 256] += 0.5 * e.sum(1)
+        ii, jj = np.nonzero((r2 > 0) & (r2 < split.rc ** 2))
+        dij = d[ii, jj]
+        e, f = split.pair(np.sqrt(r2[ii, jj]))
+        qq = C * q[a + ii] * q[jj]
+        e, f = e * qq, f * qq
+        np.add.at(F, a + ii, f[:, None] * dij)
+        np.add.at(E, a + ii, 0.5 * e)
         for j, (p1, p2) in enumerate(((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))):
-            W[j] += 0.5 * (f * d[..., p1] * d[..., p2]).sum()
+            W[j] += 0.5 * (f * dij[:, p1] * dij[:, p2]).sum()
     return dict(F=F, E=E, W=W)
 
 

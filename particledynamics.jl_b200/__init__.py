@@ -5,11 +5,11 @@ package holds the host side above its C ABI: ctypes bindings, the FP64 setup
 math, the engine objects and the workflow API.  Importing the package does
 not require a GPU; creating an engine does, and there is no CPU fallback.
 """
-from . import _native, batch, learned, splits, synthetic  # noqa: F401
+from . import _native, batch, learned, prolates, splits, synthetic  # noqa: F401
 from .engine import (ClusterPairEngine, DeviceEngine, ELLDeviceEngine, ELLEngine, ElectrostaticsSolver,  # noqa: F401
                      ElectrostaticsSpec)
 from .workflow import (  # noqa: F401
-    BAOA, BAOAB, PME, PPPM, WCA, CellList, ClusterPairList, ConstantVolume, Integrator, Langevin, LennardJones,
+    BAOA, BAOAB, ESP, PME, PPPM, WCA, CellList, ClusterPairList, ConstantVolume, Integrator, Langevin, LennardJones,
     ParticleSystem, Simulation, SimulationState, Stage, VelocityVerlet, electrostatics_spec, evaluate_forces_into_f,
     run, state, step,
 )

@@ -61,6 +61,21 @@ class MeshParams(C.Structure):
     ]
 
 
+PD_MESH_ESP, PD_MESH_ESP_DECONV = 4, 5
+PD_PROLATE_MAX_QUAD, PD_PROLATE_MAX_DEG, PD_PROLATE_MAX_NODES = 256, 24, 8
+
+
+class Prolate(C.Structure):
+    """pd_prolate: the prolate split and window of an ESP mesh (include/pdb200.h)."""
+    _fields_ = [
+        ("cutoff", C.c_double), ("nquad", C.c_int),
+        ("xq", C.c_double * PD_PROLATE_MAX_QUAD), ("wchi", C.c_double * PD_PROLATE_MAX_QUAD),
+        ("background_coefficient", C.c_double), ("deg", C.c_int),
+        ("poly", (C.c_double * PD_PROLATE_MAX_NODES) * (PD_PROLATE_MAX_DEG + 1)),
+        ("table", C.c_void_p * 3),
+    ]
+
+
 class MDState(C.Structure):
     _fields_ = [
         ("n", C.c_int),
@@ -135,6 +150,8 @@ _SIGS = {
     "pd_cluster_buffers": (C.c_int, [_p, C.POINTER(_p), C.POINTER(_p), C.POINTER(_p), C.POINTER(_p),
                                      C.POINTER(_p), C.POINTER(_p)]),
     "pd_mesh_create": (C.c_int, [C.POINTER(_p), C.POINTER(MeshParams), C.POINTER(C.c_double)]),
+    "pd_mesh_create_prolate": (C.c_int, [C.POINTER(_p), C.POINTER(MeshParams), C.POINTER(Prolate),
+                                         C.POINTER(C.c_double)]),
     "pd_mesh_destroy": (C.c_int, [_p]),
     "pd_mesh_set_box": (C.c_int, [_p, C.POINTER(C.c_double)]),
     "pd_mesh_transform": (C.c_int, [_p, _fp, _fp, _fp, _fp, _fp, C.c_int, C.c_int, _p]),

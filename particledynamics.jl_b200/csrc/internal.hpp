@@ -155,6 +155,15 @@ struct pd_mesh {
     void *work = nullptr;
     size_t work_size = 0;
     cudaStream_t plan_stream = nullptr;
+    // ESP (prolate split and window): quadrature of the split's transform, window node polynomials
+    // ((deg + 1) x H floats) and the per-axis deconvolution or alias tables, all on the device
+    bool prolate = false;
+    double split_rc = 0.0, bg_coef = 0.0;
+    int nquad = 0;
+    double *xq = nullptr, *wchi = nullptr;
+    float *wpoly = nullptr;
+    int wdeg = 0;
+    double *wtab[3] = {nullptr, nullptr, nullptr};
     float4 *self_tab = nullptr; // self-force table (T^3 samples of the fractional position), or null
     int self_T = 0;
     int epoch = 0;              // bumped when a change needs captured steps to be captured again

@@ -1,21 +1,14 @@
-// PME / P3M mesh engine of libpdb200.
+// PME / P3M / ESP mesh engine of libpdb200: host setup, influence functions,
+// solve and transforms.
 //
-// Semantics follow src/electrostatics of ParticleDynamics.jl: B-spline windows
-// (Windows.jl:187-308), influence functions and virial coefficients in FP64
+// Semantics follow src/electrostatics of ParticleDynamics.jl: B-spline and
+// prolate windows (Windows.jl:18-308), Gaussian and prolate splits
+// (Splits.jl:21-240), influence functions and virial coefficients in FP64
 // (Influence.jl:24-227), the solve with the FP64 energy/virial reduction
 // (MeshKernels.jl:34-81), the ik field (MeshKernels.jl:84-102) and the AD / ik
 // gathers (MeshKernels.jl:105-147, 281-333); cuFFT does the transforms
-// (Solver.jl:34-65, 305-347).
-//
-// Layout of this library: particles are processed in chunks of 64 consecutive
-// entries of a spatially sorted sequence (a super-cluster of the cluster list).
-// A chunk's stencils cover a small brick of the mesh; the spread accumulates
-// the chunk into that brick in shared memory and adds the brick to the global
-// grid once (one coalesced reduction per brick node instead of P^3 scattered
-// atomics per particle), and the gather stages the brick of the potential in
-// shared memory before every particle reads its P^3 nodes.  A chunk whose
-// brick exceeds the shared-memory budget falls back to direct global
-// accumulation.  The charge grid is kept zero between transforms: the solve
+// (Solver.jl:34-65, 305-347).  The spread and gather kernels are in
+// mesh_kernels.cuh.  The charge grid is kept zero between transforms: the solve
 // clears it after the forward transform has consumed it, and the inverse
 // transform writes the potential into a second grid.
 #include <cufft.h>
@@ -27,6 +20,7 @@
 
 #include "common.cuh"
 #include "internal.hpp"
+#include "mesh_kernels.cuh"
 
 using namespace pdb;
 
@@ -40,262 +34,6 @@ using namespace pdb;
     } while (0)
 
 namespace pdb {
-
-constexpr int MESH_CHUNK = 64;        // particles per CTA
-constexpr int MESH_THREADS = 128;     // two threads per particle (halves of the z stencil)
-constexpr int TILE_MAX = 6144;        // floats of the shared brick (24 KiB)
-constexpr int MESH_CTAS_PER_SM = 8;   // resident spread / gather CTAs per SM (one wave at ~1200 chunks)
-
-// _grid_coordinate (MeshKernels.jl:9-15)
-__device__ __forceinline__ float grid_coordinate(float x, float L, int K) {
-    float s = x / L;
-    s -= floorf(s);
-    float u = s * (float)K;
-    if (!isfinite(u)) return 0.f;
-    return u >= (float)K ? u - (float)K : u;
-}
-
-// window_stencil(::BSplineStencil{P}, u) (Windows.jl:209-223): first node k0 =
-// floor(u) - P + 1, weights M_P(u - k) in ascending node order and their
-// derivatives dM_P/du = M_{P-1}(u-k) - M_{P-1}(u-k-1), by the order recursion
-// of _bspline_step (Windows.jl:188-196).
-template <int P>
-__device__ __forceinline__ int bspline(float u, float *w, float *dw) {
-    const float fl = floorf(u);
-    const float t = u - fl;
-    float a[P];
-    a[0] = t;
-    a[1] = 1.f - t;
-#pragma unroll
-    for (int n = 2; n < P - 1; ++n) {
-        const float inv = 1.f / (float)n;
-#pragma unroll
-        for (int j = n; j >= 0; --j) {
-            const float left = j < n ? a[j] : 0.f;
-            const float right = j >= 1 ? a[j - 1] : 0.f;
-            a[j] = ((t + (float)j) * left + (((float)(n + 1) - t) - (float)j) * right) * inv;
-        }
-    }
-    {
-        const int n = P - 1;
-        const float inv = 1.f / (float)n;
-#pragma unroll
-        for (int j = 0; j < P; ++j) {
-            const float left = j < n ? a[j] : 0.f;
-            const float right = j >= 1 ? a[j - 1] : 0.f;
-            w[P - 1 - j] = ((t + (float)j) * left + (((float)(n + 1) - t) - (float)j) * right) * inv;
-        }
-    }
-    if (dw) {
-#pragma unroll
-        for (int i = 0; i < P; ++i) {
-            const int j = P - 1 - i;
-            const float left = j <= P - 2 ? a[j] : 0.f;
-            const float right = j >= 1 ? a[j - 1] : 0.f;
-            dw[i] = left - right;
-        }
-    }
-    return (int)fl - (P - 1);
-}
-
-__device__ __forceinline__ int wrap_node(int n, int K) {
-    n %= K;
-    return n < 0 ? n + K : n;
-}
-
-// Signed offset of node k from the reference node r on a periodic axis of K nodes, in [-K/2, K/2).
-__device__ __forceinline__ int signed_offset(int k, int r, int K) {
-    int d = (k - r) % K;
-    if (d < 0) d += K;
-    if (d >= (K + 1) / 2) d -= K;
-    return d;
-}
-
-// Brick of one chunk: first valid particle's stencil base is the reference;
-// every particle's base is expressed as an offset from it, and the brick is
-// the bounding box of the stencils.
-//
-// With vec (K1 a multiple of 4) the brick's x origin is aligned down to a
-// multiple of 4 nodes and its x extent rounded up to a multiple of 4, so every
-// brick row moves to and from the global grid as 16-byte vectors (a row of a
-// multiple-of-4 mesh never splits a vector across its periodic end).  The
-// wrapped global base of every brick row is tabulated once in shared memory.
-struct Brick {
-    int o1, o2, o3;   // global origin node (not wrapped)
-    int e1, e2, e3;   // extents
-    int fits;
-    int vec;
-};
-
-constexpr int ROWS_MAX = 512;   // brick rows tabulated in shared memory
-
-template <int P>
-__device__ __forceinline__ void chunk_brick(bool valid, int k1, int k2, int k3, int K1, int K2, int K3, int &d1,
-                                            int &d2, int &d3, Brick &b, int *sm /* >= 10 ints */,
-                                            unsigned *rowbase) {
-    // sm[0] first valid, sm[1..3] ref, sm[4..6] min, sm[7..9] max
-    const int t = threadIdx.x;
-    if (t == 0) {
-        sm[0] = 1 << 30;
-        sm[4] = sm[5] = sm[6] = 1 << 30;
-        sm[7] = sm[8] = sm[9] = -(1 << 30);
-    }
-    __syncthreads();
-    if (valid) atomicMin(&sm[0], t);
-    __syncthreads();
-    if (valid && sm[0] == t) {
-        sm[1] = k1;
-        sm[2] = k2;
-        sm[3] = k3;
-    }
-    __syncthreads();
-    const bool any = sm[0] < (1 << 30);
-    if (valid) {
-        d1 = signed_offset(k1, sm[1], K1);
-        d2 = signed_offset(k2, sm[2], K2);
-        d3 = signed_offset(k3, sm[3], K3);
-        atomicMin(&sm[4], d1);
-        atomicMin(&sm[5], d2);
-        atomicMin(&sm[6], d3);
-        atomicMax(&sm[7], d1);
-        atomicMax(&sm[8], d2);
-        atomicMax(&sm[9], d3);
-    }
-    __syncthreads();
-    b.vec = (K1 & 3) == 0;
-    if (any) {
-        int o1 = sm[1] + sm[4], e1 = sm[7] - sm[4] + P;
-        int shift = 0;
-        if (b.vec) {
-            shift = ((o1 % 4) + 4) % 4;
-            o1 -= shift;
-            e1 = (e1 + shift + 3) & ~3;
-        }
-        b.o1 = o1;
-        b.o2 = sm[2] + sm[5];
-        b.o3 = sm[3] + sm[6];
-        b.e1 = e1;
-        b.e2 = sm[8] - sm[5] + P;
-        b.e3 = sm[9] - sm[6] + P;
-        const long long nodes = (long long)b.e1 * b.e2 * b.e3;
-        b.fits = nodes <= TILE_MAX && b.e1 <= MESH_THREADS && (!b.vec || b.e1 <= K1) &&
-                 (long long)b.e2 * b.e3 <= ROWS_MAX;
-        if (valid) {
-            d1 += shift - sm[4];
-            d2 -= sm[5];
-            d3 -= sm[6];
-        }
-    } else {
-        b.o1 = b.o2 = b.o3 = 0;
-        b.e1 = b.e2 = b.e3 = 0;
-        b.fits = 1;
-    }
-    if (b.fits) {
-        const int nrows = b.e2 * b.e3;
-        for (int r = threadIdx.x; r < nrows; r += blockDim.x) {
-            const int l2 = r % b.e2, l3 = r / b.e2;
-            rowbase[r] = (unsigned)(((size_t)wrap_node(b.o3 + l3, K3) * K2 + wrap_node(b.o2 + l2, K2)) * K1);
-        }
-    }
-    __syncthreads();
-}
-
-// Move a brick between shared memory and the global grid: lanes are laid out as
-// (row, x vector) with MESH_THREADS / nv rows in flight, nv = vectors (or nodes)
-// per row; visit(tile_element, global_node) gets the first node of each
-// 4-node vector (vec) or single node.
-template <typename F>
-__device__ __forceinline__ void for_brick(const Brick &b, const unsigned *rowbase, int K1, F &&visit) {
-    const int per = b.vec ? 4 : 1;
-    const int nv = b.e1 / per;
-    if (nv == 0) return;
-    const int rpi = MESH_THREADS / nv;
-    const int t = threadIdx.x;
-    const int r0 = t / nv, v = t - r0 * nv;
-    if (r0 >= rpi) return;
-    const int x0 = wrap_node(b.o1 + per * v, K1);
-    const int nrows = b.e2 * b.e3;
-    for (int r = r0; r < nrows; r += rpi) visit(r * nv + v, (size_t)rowbase[r] + x0);
-}
-
-// Spread of chunks of packed (x, y, z, q) particles (the charge assignment of
-// _spread_lines_kernel!, MeshKernels.jl:247-276).  nchunk_dev (optional) holds
-// the number of active chunks (the cluster list's super-cluster count).
-template <int P>
-__global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_spread(const float4 *__restrict__ xq, int nchunks,
-                                                         const int *__restrict__ nchunk_dev, float *__restrict__ grid,
-                                                         int K1, int K2, int K3, float Lx, float Ly, float Lz) {
-    const int c = blockIdx.x;
-    if (nchunk_dev && c >= *nchunk_dev) return;
-    if (c >= nchunks) return;
-    __shared__ __align__(16) float tile[TILE_MAX];
-    __shared__ unsigned rowbase[ROWS_MAX];
-    __shared__ int sm[10];
-    const int t = threadIdx.x, p = t & (MESH_CHUNK - 1), h = t >> 6;
-    const float4 v = xq[c * MESH_CHUNK + p];
-    const bool valid = v.w != 0.f && isfinite(v.x) && isfinite(v.y) && isfinite(v.z);
-    float w1[P], w2[P], w3[P];
-    int k1 = 0, k2 = 0, k3 = 0;
-    if (valid) {
-        k1 = bspline<P>(grid_coordinate(v.x, Lx, K1), w1, nullptr);
-        k2 = bspline<P>(grid_coordinate(v.y, Ly, K2), w2, nullptr);
-        k3 = bspline<P>(grid_coordinate(v.z, Lz, K3), w3, nullptr);
-    }
-    int d1 = 0, d2 = 0, d3 = 0;
-    Brick b;
-    // both halves of a particle take part (their min/max contributions are identical)
-    chunk_brick<P>(valid, k1, k2, k3, K1, K2, K3, d1, d2, d3, b, sm, rowbase);
-    constexpr int PH = (P + 1) / 2;
-
-    if (b.fits) {
-        const int nb4 = (b.e1 * b.e2 * b.e3 + 3) >> 2;
-        float4 *tile4 = reinterpret_cast<float4 *>(tile);
-        for (int k = t; k < nb4; k += MESH_THREADS) tile4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-        __syncthreads();
-        if (valid) {
-#pragma unroll
-            for (int j3 = 0; j3 < P; ++j3) {   // this half's z nodes only (warp-uniform test)
-            if ((j3 < PH) != (h == 0)) continue;
-                const float q3 = v.w * w3[j3];
-#pragma unroll
-                for (int j2 = 0; j2 < P; ++j2) {
-                    const float q23 = q3 * w2[j2];
-                    float *row = tile + ((d3 + j3) * b.e2 + (d2 + j2)) * b.e1 + d1;
-#pragma unroll
-                    for (int j1 = 0; j1 < P; ++j1) red_add_shared(row + j1, q23 * w1[j1]);
-                }
-            }
-        }
-        __syncthreads();
-        if (b.vec) {
-            for_brick(b, rowbase, K1, [&](int kt, size_t kg) {
-                const float4 val = tile4[kt];
-                if (val.x != 0.f || val.y != 0.f || val.z != 0.f || val.w != 0.f)
-                    red_add_v4(grid + kg, val.x, val.y, val.z, val.w);
-            });
-        } else {
-            for_brick(b, rowbase, K1, [&](int kt, size_t kg) {
-                const float val = tile[kt];
-                if (val != 0.f) red_add(grid + kg, val);
-            });
-        }
-    } else if (valid) {
-#pragma unroll
-        for (int j3 = 0; j3 < P; ++j3) {   // this half's z nodes only (warp-uniform test)
-            if ((j3 < PH) != (h == 0)) continue;
-            const int n3 = wrap_node(k3 + j3, K3);
-            const float q3 = v.w * w3[j3];
-#pragma unroll
-            for (int j2 = 0; j2 < P; ++j2) {
-                const int n2 = wrap_node(k2 + j2, K2);
-                const float q23 = q3 * w2[j2];
-#pragma unroll
-                for (int j1 = 0; j1 < P; ++j1)
-                    red_add(grid + ((size_t)n3 * K2 + n2) * K1 + wrap_node(k1 + j1, K1), q23 * w1[j1]);
-            }
-        }
-    }
-}
 
 // Solve (_solve_kernel!, MeshKernels.jl:57-81): spec *= G; with energy the FP64
 // mesh energy 1/2 sum w |b|^2 G and the six virial sums; the consumed charge grid
@@ -364,310 +102,6 @@ __global__ void k_ik_field(float2 *__restrict__ out, const float2 *__restrict__ 
     out[idx] = make_float2(z.y * kd, -z.x * kd);
 }
 
-// AD gather of chunks (the sums of _gather_ad_lines_sums, MeshKernels.jl:281-311,
-// and _gather_ad_lines_kernel!, :313-333) with the potential brick staged in
-// shared memory.  JOIN adds the chunk's slot pair forces (and energies), writes
-// the total force in storage order and applies the closing half kick; without
-// JOIN the mesh force is stored (SET) or added to fx/fy/fz.
-struct GatherOut {
-    float *fx, *fy, *fz, *epot, *vir6;
-    float *vx, *vy, *vz;
-    const float *inv_mass;
-    float inv_mass_uniform, half_dt;
-    const int *ids;          // chunk entry -> particle (perm for the cluster slots, the order otherwise)
-    int n_entries;           // entries with an id (SoA path); slots use perm < 0 for padding
-    float4 *fc;              // JOIN: slot pair force + energy (cleared here)
-    float *vc;               // JOIN energy: slot pair virial (cleared here)
-    int nslot;
-    float half_c_self;       // JOIN energy: 0.5 C selfc
-    float bg;                // background potential per unit charge
-    const float4 *extra;     // JOIN: per-particle force added before the kick (learned correction), or null
-    const float4 *self_tab;  // self-force table of the mesh (T^3), or null: no self-force removal
-    int self_T;
-};
-
-// Spurious self force of a unit charge at grid coordinates (u1, u2, u3): trilinear interpolation of
-// the table sampled at the fractional positions t / T (t = 0 .. T-1) on each axis; the self force is
-// periodic with period one node on every axis.
-__device__ __forceinline__ float4 self_force(const float4 *__restrict__ tab, int T, float u1, float u2, float u3) {
-    int i[3], j[3];
-    float t[3];
-    const float u[3] = {u1, u2, u3};
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        const float f = (u[d] - floorf(u[d])) * (float)T;
-        int a = (int)f;
-        a = a < 0 ? 0 : (a >= T ? T - 1 : a);
-        i[d] = a;
-        j[d] = a + 1 == T ? 0 : a + 1;
-        t[d] = f - (float)a;
-    }
-    float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-        const int a1 = (c & 1) ? j[0] : i[0], a2 = (c & 2) ? j[1] : i[1], a3 = (c & 4) ? j[2] : i[2];
-        const float w = ((c & 1) ? t[0] : 1.f - t[0]) * ((c & 2) ? t[1] : 1.f - t[1]) * ((c & 4) ? t[2] : 1.f - t[2]);
-        const float4 v = __ldg(tab + ((size_t)a3 * T + a2) * T + a1);
-        r.x = fmaf(w, v.x, r.x);
-        r.y = fmaf(w, v.y, r.y);
-        r.z = fmaf(w, v.z, r.z);
-    }
-    return r;
-}
-
-// Grids a gather reads: AD the potential (g[0]); ik the three field components (g[0..2]) and, with
-// energy, the potential (g[3]).
-struct GatherGrids {
-    const float *g[4];
-};
-
-// IK: the ik gather (_gather_ik_kernel!, MeshKernels.jl:105-147), F_i = q_i sum W E, with the three
-// field grids staged through the same brick one after another.
-template <int P, int MODE, bool ENERGY, bool IK>   // MODE 0: add, 1: set, 2: join (+ kick)
-__global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_gather(const float4 *__restrict__ xq, int nchunks,
-                                                         const int *__restrict__ nchunk_dev, GatherGrids grids,
-                                                         int K1, int K2, int K3, float Lx, float Ly, float Lz,
-                                                         GatherOut o) {
-    const int c = blockIdx.x;
-    if (nchunk_dev && c >= *nchunk_dev) return;
-    if (c >= nchunks) return;
-    __shared__ __align__(16) float tile[TILE_MAX];
-    __shared__ unsigned rowbase[ROWS_MAX];
-    __shared__ int sm[10];
-    __shared__ float part[MESH_CHUNK][4];
-    const int t = threadIdx.x, p = t & (MESH_CHUNK - 1), h = t >> 6;
-    const int e = c * MESH_CHUNK + p;
-    const float4 v = xq[e];
-    const int id = (MODE == 2) ? o.ids[e] : (e < o.n_entries ? (o.ids ? o.ids[e] : e) : -1);
-    const bool charged = v.w != 0.f && isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && id >= 0;
-    // join: fetch the slot pair force and the particle's velocity now, so that their latency
-    // overlaps the brick set-up and the potential load below
-    float4 fpair = make_float4(0.f, 0.f, 0.f, 0.f);
-    float pvx = 0.f, pvy = 0.f, pvz = 0.f, pim = 0.f;
-    float4 fextra = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (MODE == 2 && h == 0 && id >= 0) {
-        fpair = o.fc[e];
-        if (o.extra) fextra = o.extra[id];
-        pvx = o.vx[id];
-        pvy = o.vy[id];
-        pvz = o.vz[id];
-        pim = o.inv_mass ? o.inv_mass[id] : o.inv_mass_uniform;
-    }
-    float w1[P], w2[P], w3[P], g1[P], g2[P], g3[P];
-    int k1 = 0, k2 = 0, k3 = 0;
-    float u1 = 0.f, u2 = 0.f, u3 = 0.f;
-    if (charged) {
-        u1 = grid_coordinate(v.x, Lx, K1);
-        u2 = grid_coordinate(v.y, Ly, K2);
-        u3 = grid_coordinate(v.z, Lz, K3);
-        k1 = bspline<P>(u1, w1, IK ? nullptr : g1);
-        k2 = bspline<P>(u2, w2, IK ? nullptr : g2);
-        k3 = bspline<P>(u3, w3, IK ? nullptr : g3);
-    }
-    int d1 = 0, d2 = 0, d3 = 0;
-    Brick b;
-    chunk_brick<P>(charged, k1, k2, k3, K1, K2, K3, d1, d2, d3, b, sm, rowbase);
-    constexpr int PH = (P + 1) / 2;
-    constexpr int NG = IK ? (ENERGY ? 4 : 3) : 1;   // grids read one after another
-
-    float phi = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
-    if (IK && b.fits) {
-#pragma unroll 1
-        for (int gi = 0; gi < NG; ++gi) {
-            const float *grid = grids.g[gi];
-            if (gi > 0) __syncthreads();   // every thread is done with the previous grid's brick
-            if (b.vec) {
-                float4 *tile4 = reinterpret_cast<float4 *>(tile);
-                for_brick(b, rowbase, K1, [&](int kt, size_t kg) {
-                    tile4[kt] = __ldg(reinterpret_cast<const float4 *>(grid + kg));
-                });
-            } else {
-                for_brick(b, rowbase, K1, [&](int kt, size_t kg) { tile[kt] = __ldg(grid + kg); });
-            }
-            __syncthreads();
-            if (charged) {
-                float acc = 0.f;
-#pragma unroll
-                for (int j3 = 0; j3 < P; ++j3) {   // this half's z nodes only (warp-uniform test)
-                    if ((j3 < PH) != (h == 0)) continue;
-                    float s0 = 0.f;
-#pragma unroll
-                    for (int j2 = 0; j2 < P; ++j2) {
-                        const float *row = tile + ((d3 + j3) * b.e2 + (d2 + j2)) * b.e1 + d1;
-                        float a0 = 0.f;
-#pragma unroll
-                        for (int j1 = 0; j1 < P; ++j1) a0 = fmaf(w1[j1], row[j1], a0);
-                        s0 = fmaf(w2[j2], a0, s0);
-                    }
-                    acc = fmaf(w3[j3], s0, acc);
-                }
-                if (gi == 0) gx = acc;
-                else if (gi == 1) gy = acc;
-                else if (gi == 2) gz = acc;
-                else phi = acc;
-            }
-        }
-    } else if (IK && charged) {
-#pragma unroll 1
-        for (int gi = 0; gi < NG; ++gi) {
-            const float *grid = grids.g[gi];
-            float acc = 0.f;
-#pragma unroll
-            for (int j3 = 0; j3 < P; ++j3) {   // this half's z nodes only (warp-uniform test)
-                if ((j3 < PH) != (h == 0)) continue;
-                const int n3 = wrap_node(k3 + j3, K3);
-                float s0 = 0.f;
-#pragma unroll
-                for (int j2 = 0; j2 < P; ++j2) {
-                    const int n2 = wrap_node(k2 + j2, K2);
-                    float a0 = 0.f;
-#pragma unroll
-                    for (int j1 = 0; j1 < P; ++j1)
-                        a0 = fmaf(w1[j1], grid[((size_t)n3 * K2 + n2) * K1 + wrap_node(k1 + j1, K1)], a0);
-                    s0 = fmaf(w2[j2], a0, s0);
-                }
-                acc = fmaf(w3[j3], s0, acc);
-            }
-            if (gi == 0) gx = acc;
-            else if (gi == 1) gy = acc;
-            else if (gi == 2) gz = acc;
-            else phi = acc;
-        }
-    } else if (b.fits) {
-        const float *grid = grids.g[0];
-        if (b.vec) {
-            float4 *tile4 = reinterpret_cast<float4 *>(tile);
-            for_brick(b, rowbase, K1, [&](int kt, size_t kg) {
-                tile4[kt] = __ldg(reinterpret_cast<const float4 *>(grid + kg));
-            });
-        } else {
-            for_brick(b, rowbase, K1, [&](int kt, size_t kg) { tile[kt] = __ldg(grid + kg); });
-        }
-        __syncthreads();
-        if (charged) {
-#pragma unroll
-            for (int j3 = 0; j3 < P; ++j3) {   // this half's z nodes only (warp-uniform test)
-            if ((j3 < PH) != (h == 0)) continue;
-                float s0 = 0.f, s1 = 0.f, s2 = 0.f;   // sum w1 w2 c, sum dw1 w2 c, sum w1 dw2 c over a z-plane
-#pragma unroll
-                for (int j2 = 0; j2 < P; ++j2) {
-                    const float *row = tile + ((d3 + j3) * b.e2 + (d2 + j2)) * b.e1 + d1;
-                    float a0 = 0.f, a1 = 0.f;
-#pragma unroll
-                    for (int j1 = 0; j1 < P; ++j1) {
-                        const float cval = row[j1];
-                        a0 = fmaf(w1[j1], cval, a0);
-                        a1 = fmaf(g1[j1], cval, a1);
-                    }
-                    s0 = fmaf(w2[j2], a0, s0);
-                    s1 = fmaf(w2[j2], a1, s1);
-                    s2 = fmaf(g2[j2], a0, s2);
-                }
-                phi = fmaf(w3[j3], s0, phi);
-                gz = fmaf(g3[j3], s0, gz);
-                gx = fmaf(w3[j3], s1, gx);
-                gy = fmaf(w3[j3], s2, gy);
-            }
-        }
-    } else if (charged) {
-        const float *grid = grids.g[0];
-#pragma unroll
-        for (int j3 = 0; j3 < P; ++j3) {   // this half's z nodes only (warp-uniform test)
-            if ((j3 < PH) != (h == 0)) continue;
-            const int n3 = wrap_node(k3 + j3, K3);
-            float s0 = 0.f, s1 = 0.f, s2 = 0.f;
-#pragma unroll
-            for (int j2 = 0; j2 < P; ++j2) {
-                const int n2 = wrap_node(k2 + j2, K2);
-                float a0 = 0.f, a1 = 0.f;
-#pragma unroll
-                for (int j1 = 0; j1 < P; ++j1) {
-                    const float cval = grid[((size_t)n3 * K2 + n2) * K1 + wrap_node(k1 + j1, K1)];
-                    a0 = fmaf(w1[j1], cval, a0);
-                    a1 = fmaf(g1[j1], cval, a1);
-                }
-                s0 = fmaf(w2[j2], a0, s0);
-                s1 = fmaf(w2[j2], a1, s1);
-                s2 = fmaf(g2[j2], a0, s2);
-            }
-            phi = fmaf(w3[j3], s0, phi);
-            gz = fmaf(g3[j3], s0, gz);
-            gx = fmaf(w3[j3], s1, gx);
-            gy = fmaf(w3[j3], s2, gy);
-        }
-    }
-    // combine the two z halves
-    if (h == 1) {
-        part[p][0] = phi;
-        part[p][1] = gx;
-        part[p][2] = gy;
-        part[p][3] = gz;
-    }
-    __syncthreads();
-    if (h == 1) return;
-    phi += part[p][0];
-    gx += part[p][1];
-    gy += part[p][2];
-    gz += part[p][3];
-    const float qi = v.w;
-    float Fx = 0.f, Fy = 0.f, Fz = 0.f, Ei = 0.f;
-    if (charged) {
-        if (IK) {
-            Fx = qi * gx;
-            Fy = qi * gy;
-            Fz = qi * gz;
-        } else {
-            Fx = -(qi * gx * ((float)K1 / Lx));
-            Fy = -(qi * gy * ((float)K2 / Ly));
-            Fz = -(qi * gz * ((float)K3 / Lz));
-        }
-        if (ENERGY) Ei = 0.5f * qi * phi + o.bg * qi;
-        if (!IK && o.self_tab) {   // remove the charge's own force through the mesh: F -= q^2 S(u)
-            const float4 sf = self_force(o.self_tab, o.self_T, u1, u2, u3);
-            const float q2 = qi * qi;
-            Fx = fmaf(-q2, sf.x, Fx);
-            Fy = fmaf(-q2, sf.y, Fy);
-            Fz = fmaf(-q2, sf.z, Fz);
-        }
-    }
-    if (MODE == 2) {
-        if (id < 0) return;
-        const float4 f = fpair;
-        o.fc[e] = make_float4(0.f, 0.f, 0.f, 0.f);
-        Fx += f.x + fextra.x;
-        Fy += f.y + fextra.y;
-        Fz += f.z + fextra.z;
-        o.fx[id] = Fx;
-        o.fy[id] = Fy;
-        o.fz[id] = Fz;
-        const float cm = o.half_dt * pim;
-        o.vx[id] = fmaf(cm, Fx, pvx);
-        o.vy[id] = fmaf(cm, Fy, pvy);
-        o.vz[id] = fmaf(cm, Fz, pvz);
-        if (ENERGY) {
-            o.epot[id] = Ei + f.w - o.half_c_self * qi * qi;
-#pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                o.vir6[(size_t)id * 6 + k] = o.vc[(size_t)k * o.nslot + e];
-                o.vc[(size_t)k * o.nslot + e] = 0.f;
-            }
-        }
-    } else {
-        if (id < 0) return;
-        if (MODE == 1) {
-            o.fx[id] = Fx;
-            o.fy[id] = Fy;
-            o.fz[id] = Fz;
-            if (ENERGY) o.epot[id] = Ei;
-        } else if (charged) {
-            o.fx[id] += Fx;
-            o.fy[id] += Fy;
-            o.fz[id] += Fz;
-            if (ENERGY) o.epot[id] += Ei;
-        }
-    }
-}
-
 // Particles of `order` packed as (x, y, z, q) in chunks of 64 (zero-charge padding).
 // Self-force table: a unit charge at grid coordinate t / T (t = 0 .. T-1 per axis) spreads the
 // weights W_b (b in the P^3 stencil) and gathers -grad W_a . phi_a with phi_a = sum_b Ghat(a - b) W_b,
@@ -730,17 +164,42 @@ __global__ void k_store_virial(float *vg, const double *acc, double ubg) {
 __device__ __forceinline__ int signed_mode(int m, int K) { return m <= K / 2 ? m : m - K; }
 __device__ __forceinline__ bool is_nyquist(int m, int K) { return (K % 2 == 0) && m == K / 2; }
 
-// spectral_g(::GaussianSpectral, k) (Splits.jl:220-224): g(k) and g'(k)/k
-__device__ __forceinline__ void spectral_g(double alpha, double k, double &g, double &gpk) {
+// Long-range transform of the split: Gaussian (alpha) or prolate (quadrature of c_hat on device).
+struct Spectral {
+    double alpha;
+    double rc;
+    int nq;
+    const double *xq, *wchi;   // prolate: nodes on [0, 1] and weights times chi; null for Gaussian
+};
+
+// spectral_g(::GaussianSpectral, k) and spectral_g(::ProlateSpectral, k) (Splits.jl:202-225): g(k)
+// and g'(k)/k, with g = 4 pi exp(-k^2 / 4 alpha^2) / k^2 or g = 4 pi c_hat(k r_c) / k^2,
+// c_hat(u) = sum_q wchi_q cos(u x_q).
+__device__ __forceinline__ void spectral_g(const Spectral &sp, double k, double &g, double &gpk) {
     const double k2 = k * k;
-    g = 4.0 * M_PI * exp(-k2 / (4.0 * alpha * alpha)) / k2;
-    gpk = g * (-2.0 / k2 - 1.0 / (2.0 * alpha * alpha));
+    if (!sp.xq) {
+        g = 4.0 * M_PI * exp(-k2 / (4.0 * sp.alpha * sp.alpha)) / k2;
+        gpk = g * (-2.0 / k2 - 1.0 / (2.0 * sp.alpha * sp.alpha));
+        return;
+    }
+    const double u = k * sp.rc;
+    double c = 0.0, dc = 0.0;
+    for (int q = 0; q < sp.nq; ++q) {
+        const double x = sp.xq[q], w = sp.wchi[q];
+        double sn, cs;
+        sincos(u * x, &sn, &cs);
+        c += w * cs;
+        dc -= w * x * sn;
+    }
+    g = 4.0 * M_PI * c / k2;
+    const double gp = 4.0 * M_PI * (sp.rc * dc / k2 - 2.0 * c / (k2 * k));
+    gpk = gp / k;
 }
 
-// _influence_ewald_kernel! (Influence.jl:35-67)
+// _influence_ewald_kernel! (Influence.jl:35-67): SPME and ESP with the plain deconvolution
 __global__ void k_influence_spme(float *__restrict__ G, float *__restrict__ Vc, const double *__restrict__ D1,
                                  const double *__restrict__ D2, const double *__restrict__ D3, int K1, int K2, int K3,
-                                 double L1, double L2, double L3, double C, double alpha) {
+                                 double L1, double L2, double L3, double C, Spectral sp) {
     const int K1h = K1 / 2 + 1;
     const int nmodes = K1h * K2 * K3;
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -756,7 +215,7 @@ __global__ void k_influence_spme(float *__restrict__ G, float *__restrict__ Vc, 
     const double kx = 2.0 * M_PI * s1 / L1, ky = 2.0 * M_PI * s2 / L2, kz = 2.0 * M_PI * s3 / L3;
     const double k = sqrt(kx * kx + ky * ky + kz * kz);
     double g, gpk;
-    spectral_g(alpha, k, g, gpk);
+    spectral_g(sp, k, g, gpk);
     const double D = D1[m1] * D2[m2] * D3[m3];
     const double Gm = CoverV * g * D;
     const double c = CoverV * D * gpk;
@@ -770,10 +229,10 @@ __global__ void k_influence_spme(float *__restrict__ G, float *__restrict__ Vc, 
     Vc[(size_t)5 * nmodes + idx] = (n2 || n3) ? 0.f : (float)(c * ky * kz);
 }
 
-// _influence_alias_kernel! (Influence.jl:77-181): optimal P3M influence for AD or ik.
+// _influence_alias_kernel! (Influence.jl:77-181): optimal influence for AD or ik (P3M, ESP).
 __global__ void k_influence_alias(float *__restrict__ G, float *__restrict__ Vc, const double *__restrict__ U1,
                                   const double *__restrict__ U2, const double *__restrict__ U3, int K1, int K2, int K3,
-                                  double L1, double L2, double L3, double C, double alpha, int nmax, int ik) {
+                                  double L1, double L2, double L3, double C, Spectral sp, int nmax, int ik) {
     const int K1h = K1 / 2 + 1;
     const int nmodes = K1h * K2 * K3;
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -810,7 +269,7 @@ __global__ void k_influence_alias(float *__restrict__ G, float *__restrict__ Vc,
                 const double qq = q1 * q1 + q2 * q2 + q3 * q3;
                 if (qq == 0.0) continue;
                 double g, gpk;
-                spectral_g(alpha, sqrt(qq), g, gpk);
+                spectral_g(sp, sqrt(qq), g, gpk);
                 if (ik) {
                     const double dq = dx * q1 + dy * q2 + dz * q3;
                     A += U2tot * g * dq;
@@ -930,8 +389,28 @@ static std::vector<double> bspline_alias_table(int P, int K, int nmax) {
     return U;
 }
 
+static bool plain_deconvolution(const pd_mesh *m) {
+    return m->p.kind == PD_MESH_SPME || m->p.kind == PD_MESH_ESP_DECONV;
+}
+
 static int compute_influence(pd_mesh *m) {
     const int K1 = m->K1, K2 = m->K2, K3 = m->K3, P = m->p.order;
+    const int threads = 128, blocks = (m->nmodes + threads - 1) / threads;
+    if (m->prolate) {   // the caller's window tables, the split's quadrature
+        const Spectral sp{0.0, m->split_rc, m->nquad, m->xq, m->wchi};
+        if (plain_deconvolution(m))
+            k_influence_spme<<<blocks, threads>>>(m->G, m->Vc, m->wtab[0], m->wtab[1], m->wtab[2], K1, K2, K3,
+                                                  m->box[0], m->box[1], m->box[2], m->p.C, sp);
+        else
+            k_influence_alias<<<blocks, threads>>>(m->G, m->Vc, m->wtab[0], m->wtab[1], m->wtab[2], K1, K2, K3,
+                                                   m->box[0], m->box[1], m->box[2], m->p.C, sp, m->p.alias_order, 0);
+        count_launch();
+        cudaError_t e = cudaGetLastError();
+        cudaError_t e2 = cudaDeviceSynchronize();
+        PD_CHECK(e == cudaSuccess && e2 == cudaSuccess, PD_ECUDA, "influence kernel failed: %s",
+                 cudaGetErrorString(e != cudaSuccess ? e : e2));
+        return PD_OK;
+    }
     std::vector<double> t1, t2, t3;
     if (m->p.kind == PD_MESH_SPME) {
         t1 = bspline_deconvolution(P, K1);
@@ -953,13 +432,13 @@ static int compute_influence(pd_mesh *m) {
     cudaMemcpy(d1, t1.data(), t1.size() * sizeof(double), cudaMemcpyHostToDevice);
     cudaMemcpy(d2, t2.data(), t2.size() * sizeof(double), cudaMemcpyHostToDevice);
     cudaMemcpy(d3, t3.data(), t3.size() * sizeof(double), cudaMemcpyHostToDevice);
-    const int threads = 128, blocks = (m->nmodes + threads - 1) / threads;
+    const Spectral sp{m->p.alpha, 0.0, 0, nullptr, nullptr};
     if (m->p.kind == PD_MESH_SPME) {
         k_influence_spme<<<blocks, threads>>>(m->G, m->Vc, d1, d2, d3, K1, K2, K3, m->box[0], m->box[1], m->box[2],
-                                              m->p.C, m->p.alpha);
+                                              m->p.C, sp);
     } else {
         k_influence_alias<<<blocks, threads>>>(m->G, m->Vc, d1, d2, d3, K1, K2, K3, m->box[0], m->box[1], m->box[2],
-                                               m->p.C, m->p.alpha, m->p.alias_order, m->p.kind == PD_MESH_P3M_IK);
+                                               m->p.C, sp, m->p.alias_order, m->p.kind == PD_MESH_P3M_IK);
     }
     count_launch();
     cudaError_t e = cudaGetLastError();
@@ -974,15 +453,13 @@ static int compute_influence(pd_mesh *m) {
 
 static void refresh_background(pd_mesh *m) {
     const double V = m->box[0] * m->box[1] * m->box[2];
-    const double bgcoef = M_PI / (2.0 * m->p.alpha * m->p.alpha);   // background_coefficient (Splits.jl:85)
+    // background_coefficient (Splits.jl:85-86): pi / (2 alpha^2) or pi r_c^2 m_2
+    const double bgcoef = m->prolate ? m->bg_coef : M_PI / (2.0 * m->p.alpha * m->p.alpha);
     m->bg = m->p.background ? (float)(-m->p.C * bgcoef * m->p.qtotal / V) : 0.f;
     m->ubg = m->p.background ? -m->p.C * bgcoef * m->p.qtotal * m->p.qtotal / V : 0.0;
 }
 
-#define PD_SPREAD_CASE(PP)                                                                                         \
-    case PP:                                                                                                       \
-        k_spread<PP><<<nchunks, MESH_THREADS, 0, s>>>(xq, nchunks, ns_dev, m->gridA, m->K1, m->K2, m->K3, Lx, Ly, Lz); \
-        break;
+static WindowPoly window_poly(const pd_mesh *m) { return WindowPoly{m->wpoly, m->wdeg}; }
 
 // Fill m->self_tab (T = m->self_T) for the current box and influence function (host boundary: runs on
 // the legacy stream and waits for it).  Leaves the charge grid zero, as every transform does.
@@ -1017,19 +494,14 @@ static int compute_self_table(pd_mesh *m) {
 
 int mesh_transform_packed(pd_mesh *m, const float4 *xq, int nchunks, const int *ns_dev, int energy, cudaStream_t s) {
     const float Lx = (float)m->box[0], Ly = (float)m->box[1], Lz = (float)m->box[2];
-    switch (m->p.order) {
-        PD_SPREAD_CASE(3)
-        PD_SPREAD_CASE(4)
-        PD_SPREAD_CASE(5)
-        PD_SPREAD_CASE(6)
-        PD_SPREAD_CASE(7)
-        PD_SPREAD_CASE(8)
-        PD_SPREAD_CASE(9)
-        PD_SPREAD_CASE(10)
-        PD_SPREAD_CASE(11)
-        PD_SPREAD_CASE(12)
-        default: set_error("unsupported order %d", m->p.order); return PD_EINVAL;
-    }
+    PD_CHECK(m->p.order >= MESH_ORDER_MIN && m->p.order <= MESH_ORDER_MAX, PD_EINVAL, "unsupported order %d",
+             m->p.order);
+    if (m->prolate)
+        launch_spread_t<WIN_PROLATE>(m->p.order, xq, nchunks, ns_dev, m->gridA, m->K1, m->K2, m->K3, Lx, Ly, Lz,
+                                     window_poly(m), s);
+    else
+        launch_spread_t<WIN_BSPLINE>(m->p.order, xq, nchunks, ns_dev, m->gridA, m->K1, m->K2, m->K3, Lx, Ly, Lz,
+                                     window_poly(m), s);
     PD_LAUNCHED();
     PD_CUFFT(cufftSetStream(m->fwd, s));
     PD_CUFFT(cufftExecR2C(m->fwd, m->gridA, m->spec));
@@ -1058,7 +530,6 @@ int mesh_transform_packed(pd_mesh *m, const float4 *xq, int nchunks, const int *
     }
     return PD_OK;
 }
-#undef PD_SPREAD_CASE
 
 int mesh_store_virial(pd_mesh *m, float *vglobal6, cudaStream_t s) {
     if (!vglobal6) return PD_OK;
@@ -1067,28 +538,24 @@ int mesh_store_virial(pd_mesh *m, float *vglobal6, cudaStream_t s) {
     return PD_OK;
 }
 
+// MODE 0 (add) or 1 (set) through the SoA entry point, 2 the join of the step.
 template <int MODE, bool ENERGY>
 static void launch_gather(pd_mesh *m, const float4 *xq, int nchunks, const int *ns_dev, const GatherOut &o,
                           cudaStream_t s) {
     const float Lx = (float)m->box[0], Ly = (float)m->box[1], Lz = (float)m->box[2];
-    const int K1 = m->K1, K2 = m->K2, K3 = m->K3;
-    const bool ik = m->p.kind == PD_MESH_P3M_IK;
-    GatherGrids g = {{m->gridB, nullptr, nullptr, nullptr}};
-    if (ik) g = GatherGrids{{m->field[0], m->field[1], m->field[2], m->gridB}};
-#define PD_G(PP)                                                                                                       \
-    case PP:                                                                                                           \
-        if (ik)                                                                                                        \
-            k_gather<PP, MODE, ENERGY, true><<<nchunks, MESH_THREADS, 0, s>>>(xq, nchunks, ns_dev, g, K1, K2, K3, Lx,  \
-                                                                              Ly, Lz, o);                              \
-        else                                                                                                           \
-            k_gather<PP, MODE, ENERGY, false><<<nchunks, MESH_THREADS, 0, s>>>(xq, nchunks, ns_dev, g, K1, K2, K3, Lx, \
-                                                                               Ly, Lz, o);                             \
-        break;
-    switch (m->p.order) {
-        PD_G(3) PD_G(4) PD_G(5) PD_G(6) PD_G(7) PD_G(8) PD_G(9) PD_G(10) PD_G(11) PD_G(12)
-        default: break;
+    const int K1 = m->K1, K2 = m->K2, K3 = m->K3, P = m->p.order;
+    GatherOut oo = o;
+    oo.wp = window_poly(m);
+    if (m->prolate) {
+        const GatherGrids g = {{m->gridB, nullptr, nullptr, nullptr}};
+        launch_gather_t<WIN_PROLATE, false, MODE>(P, ENERGY, xq, nchunks, ns_dev, g, K1, K2, K3, Lx, Ly, Lz, oo, s);
+    } else if (m->p.kind == PD_MESH_P3M_IK) {
+        const GatherGrids g = {{m->field[0], m->field[1], m->field[2], m->gridB}};
+        launch_gather_t<WIN_BSPLINE, true, MODE>(P, ENERGY, xq, nchunks, ns_dev, g, K1, K2, K3, Lx, Ly, Lz, oo, s);
+    } else {
+        const GatherGrids g = {{m->gridB, nullptr, nullptr, nullptr}};
+        launch_gather_t<WIN_BSPLINE, false, MODE>(P, ENERGY, xq, nchunks, ns_dev, g, K1, K2, K3, Lx, Ly, Lz, oo, s);
     }
-#undef PD_G
 }
 
 int mesh_gather_join(pd_mesh *m, pd_cluster *c, const float4 *xq, const int *perm, const int *ns_dev, int nchunks,
@@ -1140,6 +607,10 @@ static void free_mesh(pd_mesh *m) {
     dfree(m->packed);
     dfree(m->self_tab);
     m->self_T = 0;
+    dfree(m->xq);
+    dfree(m->wchi);
+    dfree(m->wpoly);
+    for (int d = 0; d < 3; ++d) dfree(m->wtab[d]);
     if (m->plans) {
         cufftDestroy(m->fwd);
         cufftDestroy(m->bwd);
@@ -1151,17 +622,40 @@ static void free_mesh(pd_mesh *m) {
 
 }  // namespace pdb
 
-extern "C" {
+namespace {
 
-int pd_mesh_create(pd_mesh **out, const pd_mesh_params *p, const double box[3]) {
-    PD_CHECK(out && p && box, PD_EINVAL, "pd_mesh_create: null argument");
-    *out = nullptr;
-    PD_CHECK(p->kind >= PD_MESH_SPME && p->kind <= PD_MESH_P3M_IK, PD_EINVAL, "Unknown influence kind %d.", p->kind);
-    PD_CHECK(p->order >= 3 && p->order <= 12, PD_EINVAL,
-             "B-spline assignment order must be between 3 and 12; got %d.", p->order);
-    PD_CHECK(p->alias_order >= 0 && p->alias_order <= 6, PD_EINVAL, "alias_order must be between 0 and 6.");
-    PD_CHECK(p->C > 0 && std::isfinite(p->C), PD_EINVAL, "coulomb constant must be finite and positive");
-    PD_CHECK(p->alpha > 0 && std::isfinite(p->alpha), PD_EINVAL, "Ewald alpha must be finite and positive.");
+// Device copy of the prolate split and window (pd_prolate) into m.
+int copy_prolate(pd_mesh *m, const pd_prolate *w) {
+    const int P = m->p.order, H = (P + 1) / 2;
+    m->prolate = true;
+    m->split_rc = w->cutoff;
+    m->bg_coef = w->background_coefficient;
+    m->nquad = w->nquad;
+    m->wdeg = w->deg;
+    std::vector<float> poly((size_t)(w->deg + 1) * H);
+    for (int k = 0; k <= w->deg; ++k)
+        for (int h = 0; h < H; ++h) poly[(size_t)k * H + h] = (float)w->poly[k][h];
+    int rc;
+    if ((rc = dalloc(&m->xq, (size_t)w->nquad)) || (rc = dalloc(&m->wchi, (size_t)w->nquad)) ||
+        (rc = dalloc(&m->wpoly, poly.size())))
+        return rc;
+    PD_CUDA(cudaMemcpy(m->xq, w->xq, sizeof(double) * w->nquad, cudaMemcpyHostToDevice));
+    PD_CUDA(cudaMemcpy(m->wchi, w->wchi, sizeof(double) * w->nquad, cudaMemcpyHostToDevice));
+    PD_CUDA(cudaMemcpy(m->wpoly, poly.data(), sizeof(float) * poly.size(), cudaMemcpyHostToDevice));
+    const int K[3] = {m->K1, m->K2, m->K3};
+    const int per = m->p.kind == PD_MESH_ESP ? 2 * m->p.alias_order + 1 : 1;
+    for (int d = 0; d < 3; ++d) {
+        const size_t len = (size_t)K[d] * per;
+        for (size_t i = 0; i < len; ++i)
+            PD_CHECK(std::isfinite(w->table[d][i]), PD_EINVAL, "prolate window table %d has a non-finite entry", d);
+        if ((rc = dalloc(&m->wtab[d], len))) return rc;
+        PD_CUDA(cudaMemcpy(m->wtab[d], w->table[d], sizeof(double) * len, cudaMemcpyHostToDevice));
+    }
+    return PD_OK;
+}
+
+int mesh_create(pd_mesh **out, const pd_mesh_params *p, const pd_prolate *w, const double box[3]) {
+    const bool esp = w != nullptr;
     for (int d = 0; d < 3; ++d)
         PD_CHECK(p->mesh[d] >= p->order, PD_EINVAL, "Every mesh dimension must be at least the assignment order.");
     const long long nnodes = (long long)p->mesh[0] * p->mesh[1] * p->mesh[2];
@@ -1225,13 +719,51 @@ int pd_mesh_create(pd_mesh **out, const pd_mesh_params *p, const double box[3]) 
     }
     cufftSetWorkArea(m->fwd, m->work);
     cufftSetWorkArea(m->bwd, m->work);
-    if ((rc = pd_mesh_set_box(m, box))) {
+    if ((esp && (rc = copy_prolate(m, w))) || (rc = pd_mesh_set_box(m, box))) {
         free_mesh(m);
         delete m;
         return rc;
     }
     *out = m;
     return PD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+
+int pd_mesh_create(pd_mesh **out, const pd_mesh_params *p, const double box[3]) {
+    PD_CHECK(out && p && box, PD_EINVAL, "pd_mesh_create: null argument");
+    *out = nullptr;
+    PD_CHECK(p->kind >= PD_MESH_SPME && p->kind <= PD_MESH_P3M_IK, PD_EINVAL,
+             "Unknown influence kind %d (ESP meshes come from pd_mesh_create_prolate).", p->kind);
+    PD_CHECK(p->order >= 3 && p->order <= 12, PD_EINVAL,
+             "B-spline assignment order must be between 3 and 12; got %d.", p->order);
+    PD_CHECK(p->alias_order >= 0 && p->alias_order <= 6, PD_EINVAL, "alias_order must be between 0 and 6.");
+    PD_CHECK(p->C > 0 && std::isfinite(p->C), PD_EINVAL, "coulomb constant must be finite and positive");
+    PD_CHECK(p->alpha > 0 && std::isfinite(p->alpha), PD_EINVAL, "Ewald alpha must be finite and positive.");
+    return mesh_create(out, p, nullptr, box);
+}
+
+int pd_mesh_create_prolate(pd_mesh **out, const pd_mesh_params *p, const pd_prolate *w, const double box[3]) {
+    PD_CHECK(out && p && w && box, PD_EINVAL, "pd_mesh_create_prolate: null argument");
+    *out = nullptr;
+    PD_CHECK(p->kind == PD_MESH_ESP || p->kind == PD_MESH_ESP_DECONV, PD_EINVAL,
+             "pd_mesh_create_prolate needs an ESP influence kind; got %d.", p->kind);
+    PD_CHECK(p->order >= 3 && p->order <= 12, PD_EINVAL,
+             "Prolate window width must be between 3 and 12 grid points in this build; got %d.", p->order);
+    PD_CHECK(p->alias_order >= 0 && p->alias_order <= 6, PD_EINVAL, "alias_order must be between 0 and 6.");
+    PD_CHECK(p->C > 0 && std::isfinite(p->C), PD_EINVAL, "coulomb constant must be finite and positive");
+    PD_CHECK(std::isfinite(w->cutoff) && w->cutoff > 0, PD_EINVAL, "ESP cutoff must be finite and positive.");
+    PD_CHECK(w->nquad >= 1 && w->nquad <= PD_PROLATE_MAX_QUAD, PD_EINVAL, "ESP quadrature needs 1..%d nodes",
+             PD_PROLATE_MAX_QUAD);
+    PD_CHECK(w->deg >= 1 && w->deg <= PD_PROLATE_MAX_DEG, PD_EINVAL, "node polynomial degree must be 1..%d",
+             PD_PROLATE_MAX_DEG);
+    PD_CHECK((p->order + 1) / 2 <= PD_PROLATE_MAX_NODES, PD_EINVAL, "too many window nodes");
+    PD_CHECK(w->table[0] && w->table[1] && w->table[2], PD_EINVAL, "pd_mesh_create_prolate: window tables missing");
+    PD_CHECK(std::isfinite(w->background_coefficient), PD_EINVAL, "background coefficient must be finite");
+    return mesh_create(out, p, w, box);
 }
 
 int pd_mesh_destroy(pd_mesh *m) {
@@ -1256,8 +788,8 @@ int pd_mesh_set_self_force_removal(pd_mesh *m, int table_size) {
     PD_CHECK(m, PD_EINVAL, "pd_mesh_set_self_force_removal: null handle");
     PD_CHECK(table_size == 0 || (table_size >= 4 && table_size <= 64), PD_EINVAL,
              "self-force table size must be 0 (off) or 4..64; got %d", table_size);
-    PD_CHECK(table_size == 0 || m->p.kind != PD_MESH_P3M_IK, PD_ENOTSUP,
-             "self-force removal needs analytic differentiation (SPME or P3M-AD)");
+    PD_CHECK(table_size == 0 || (m->p.kind != PD_MESH_P3M_IK && !m->prolate), PD_ENOTSUP,
+             "self-force removal needs a B-spline window with analytic differentiation (SPME or P3M-AD)");
     dfree(m->self_tab);
     m->self_T = 0;
     ++m->epoch;   // captured steps hold the old table pointer

@@ -1,0 +1,9 @@
+// AD gather of the prolate-window mesh (ESP) joined with the slot pair forces and the closing kick.
+// One translation unit per launcher family, so that the kernel variants compile in parallel.
+#include "mesh_kernels.cuh"
+
+namespace pdb {
+
+PD_GATHER_LAUNCHER(WIN_PROLATE, false, 2);
+
+}  // namespace pdb

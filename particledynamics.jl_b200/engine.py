@@ -17,7 +17,7 @@ import numpy as np
 import torch
 
 from . import _native as N
-from . import splits
+from . import prolates, splits
 
 
 def _ptr(t) -> int:
@@ -246,15 +246,21 @@ def _cudart():
 
 # ----------------------------------------------------------------------------- electrostatics
 
-_KINDS = {"spme": N.PD_MESH_SPME, "p3m_ad": N.PD_MESH_P3M_AD, "p3m_ik": N.PD_MESH_P3M_IK}
+_KINDS = {"spme": N.PD_MESH_SPME, "p3m_ad": N.PD_MESH_P3M_AD, "p3m_ik": N.PD_MESH_P3M_IK, "esp": N.PD_MESH_ESP,
+          "esp_deconvolution": N.PD_MESH_ESP_DECONV}
+_ESP = ("esp", "esp_deconvolution")
 
 
 @dataclass
 class ElectrostaticsSpec:
-    """Validated description of a mesh Coulomb solver (ElectrostaticsSpec, Spec.jl:31-102)."""
+    """Validated description of a mesh Coulomb solver (ElectrostaticsSpec, Spec.jl:31-102).
+
+    Gaussian split + B-spline window (``spme``, ``p3m_ad``, ``p3m_ik``: ``alpha``, ``order`` = B-spline
+    order) or prolate split + prolate window (``esp``, ``esp_deconvolution``: ``split_shape`` c,
+    ``window_shape`` c_1, ``order`` = window width in grid points)."""
     coulomb_prefactor: float
     real_cutoff: float
-    alpha: float
+    alpha: float | None = None
     influence: str = "spme"
     order: int = 4
     mesh: tuple | None = None
@@ -264,6 +270,8 @@ class ElectrostaticsSpec:
     net_charge: str = "error"
     real_space_modifier: str = "none"
     net_charge_tolerance: float = 1e-8
+    split_shape: float | None = None
+    window_shape: float | None = None
 
     def __post_init__(self):
         if not (math.isfinite(self.coulomb_prefactor) and self.coulomb_prefactor > 0):
@@ -274,8 +282,25 @@ class ElectrostaticsSpec:
             raise ValueError("real_cutoff must be finite and positive.")
         if self.influence not in _KINDS:
             raise ValueError(f"Unknown influence kind {self.influence}.")
-        if not (3 <= self.order <= 12):
-            raise ValueError(f"B-spline assignment order must be between 3 and 12; got {self.order}.")
+        if self.influence in _ESP:
+            if self.split_shape is None or self.window_shape is None:
+                raise ValueError("ESP requires a prolate split and a prolate window.")
+            if not (math.isfinite(self.split_shape) and self.split_shape > 0 and math.isfinite(self.window_shape)
+                    and self.window_shape > 0):
+                raise ValueError("Prolate shapes must be finite and positive.")
+            if not (3 <= self.order <= 12):
+                raise ValueError(f"Prolate window width must be between 3 and 12 grid points in this build; "
+                                 f"got {self.order}.")
+            pmax = prolates.max_prolate_order(self.window_shape)
+            if self.order > pmax:
+                raise ValueError(f"A prolate window of shape {self.window_shape:.3f} supports at most {pmax} grid "
+                                 f"points (P <= 2c/pi - 1/2); got {self.order}. Use a larger window shape (tighter "
+                                 "tolerance) or a narrower window.")
+        else:
+            if self.alpha is None or not (math.isfinite(self.alpha) and self.alpha > 0):
+                raise ValueError("Ewald alpha must be finite and positive.")
+            if not (3 <= self.order <= 12):
+                raise ValueError(f"B-spline assignment order must be between 3 and 12; got {self.order}.")
         if not (0 <= self.alias_order <= 6):
             raise ValueError("alias_order must be between 0 and 6.")
         if self.net_charge not in ("error", "background"):
@@ -293,6 +318,10 @@ class ElectrostaticsSpec:
     @property
     def C(self) -> float:
         return self.coulomb_prefactor / self.relative_permittivity
+
+    @property
+    def prolate(self) -> bool:
+        return self.influence in _ESP
 
 
 class ElectrostaticsSolver:
@@ -320,24 +349,65 @@ class ElectrostaticsSolver:
         self.qtotal = Q
         self.qsq = float((q * q).sum())
         self.C = spec.C
-        self.selfc = splits.self_coefficient(spec.alpha)
-        self.eshift = splits.cutoff_energy(spec.alpha, spec.real_cutoff) \
-            if spec.real_space_modifier == "potential_shift" else 0.0
+        if spec.prolate:
+            self.split = prolates.ProlateSplit(spec.real_cutoff, spec.split_shape)
+            self.window = prolates.ProlateWindow(spec.order, spec.window_shape)
+            if self.window.nyquist_attenuation() < prolates.min_nyquist_attenuation(np.float32):
+                raise ValueError(f"The prolate window (width {spec.order}, shape {spec.window_shape:.3f}) decays "
+                                 "below what an FP32 mesh solve resolves at the mesh Nyquist frequency; use a "
+                                 "larger window shape.")
+            self.selfc = self.split.self_coefficient()
+            self.eshift = 0.0    # the prolate split vanishes at the cutoff (cutoff_energy, Splits.jl:77-78)
+        else:
+            self.selfc = splits.self_coefficient(spec.alpha)
+            self.eshift = splits.cutoff_energy(spec.alpha, spec.real_cutoff) \
+                if spec.real_space_modifier == "potential_shift" else 0.0
         p = N.MeshParams()
         p.kind = _KINDS[spec.influence]
         p.order = spec.order
         p.alias_order = spec.alias_order
         for d in range(3):
             p.mesh[d] = self.mesh[d]
-        p.alpha = spec.alpha
+        p.alpha = spec.alpha if spec.alpha is not None else 0.0
         p.C = self.C
         p.background = 1 if spec.net_charge == "background" else 0
         p.qtotal = Q
         p.nmax = int(nmax if nmax is not None else len(q))
         self.params = p
         h = C.c_void_p()
-        N.call("pd_mesh_create", C.byref(h), C.byref(p), N.dbl3(box))
+        if spec.prolate:
+            self._prolate = self._prolate_tables(p)
+            N.call("pd_mesh_create_prolate", C.byref(h), C.byref(p), C.byref(self._prolate[0]), N.dbl3(box))
+        else:
+            N.call("pd_mesh_create", C.byref(h), C.byref(p), N.dbl3(box))
         self.handle = h
+
+    def _prolate_tables(self, p):
+        """pd_prolate of this solver: the split's quadrature of c_hat, the window's node polynomials (fitted
+        to FP32 round-off) and, per axis, the deconvolution (esp_deconvolution) or the alias table (esp)."""
+        w = N.Prolate()
+        sp, win = self.split, self.window
+        w.cutoff = sp.cutoff
+        w.nquad = len(sp.xq)
+        for i, (x, c) in enumerate(zip(sp.xq, sp.wchi)):
+            w.xq[i], w.wchi[i] = float(x), float(c)
+        w.background_coefficient = sp.background_coefficient()
+        Cp = win.node_polynomials(np.float32)
+        H, D1 = Cp.shape
+        w.deg = D1 - 1
+        for k in range(D1):
+            for hh in range(H):
+                w.poly[k][hh] = float(Cp[hh, k])
+        tabs = []
+        for d in range(3):
+            K = int(self.mesh[d])
+            if self.spec.influence == "esp":
+                t = np.ascontiguousarray(win.alias_table(K, self.spec.alias_order).T)   # m-major
+            else:
+                t = np.ascontiguousarray(win.deconvolution(K))
+            tabs.append(t)
+            w.table[d] = t.ctypes.data
+        return w, tabs
 
     def close(self, _destroy=_destroy):
         if getattr(self, "handle", None):
@@ -380,7 +450,9 @@ class ElectrostaticsSolver:
     def background_energy(self) -> float:
         if self.spec.net_charge != "background":
             return 0.0
-        return -self.C * splits.background_coefficient(self.spec.alpha) * self.qtotal ** 2 / np.prod(self.box)
+        coef = self.split.background_coefficient() if self.spec.prolate else \
+            splits.background_coefficient(self.spec.alpha)
+        return -self.C * coef * self.qtotal ** 2 / np.prod(self.box)
 
     def influence(self) -> tuple[np.ndarray, np.ndarray]:
         dims = (C.c_int * 3)()
@@ -392,7 +464,8 @@ class ElectrostaticsSolver:
         return G, Vc.reshape(6, -1)
 
     def coulomb_polynomial(self) -> splits.CoulombPolynomial:
-        return splits.coulomb_polynomial(self.spec.alpha, self.C, self.spec.real_cutoff, eshift=self.eshift)
+        corr = prolates.ProlateCorrection(self.split) if self.spec.prolate else self.spec.alpha
+        return splits.coulomb_polynomial(corr, self.C, self.spec.real_cutoff, eshift=self.eshift)
 
     def set_self_force_removal(self, table_size: int = 16):
         """Subtract each charge's own force through the mesh (AD gathers; 0 turns it off).

@@ -173,18 +173,22 @@ class CoulombPolynomial:
     pf: np.ndarray
 
 
-def coulomb_polynomial(alpha: float, C: float, cutoff: float, eshift: float = 0.0,
+def coulomb_polynomial(alpha, C: float, cutoff: float, eshift: float = 0.0,
                        tol: float | None = None, energy_tol: float | None = None) -> CoulombPolynomial:
-    """Fit the erf long-range correction on [0, r_c^2] for Float32 kernels (PairFunctor.jl:65-84)."""
+    """Fit the long-range correction of the split on [0, r_c^2] for Float32 kernels (PairFunctor.jl:65-84).
+
+    ``alpha`` is the Gaussian split's parameter (the erf correction), or a callable s -> (corr, fcorr)
+    giving another split's correction (the prolate split's ProlateCorrection)."""
     ftol = 1e-7 if tol is None else float(tol)
     etol = 1e-8 if energy_tol is None else float(energy_tol)
     rc2 = float(cutoff) ** 2
+    corr = alpha if callable(alpha) else (lambda s: long_range_correction(alpha, s))
 
     def s_of(x):
         return (x + 1.0) * rc2 / 2.0
 
-    ce = chebyshev_fit_adaptive(lambda x: -long_range_correction(alpha, s_of(x))[0], tol=etol)
-    cf = chebyshev_fit_adaptive(lambda x: long_range_correction(alpha, s_of(x))[1], tol=ftol)
+    ce = chebyshev_fit_adaptive(lambda x: -corr(s_of(x))[0], tol=etol)
+    cf = chebyshev_fit_adaptive(lambda x: corr(s_of(x))[1], tol=ftol)
     if max(len(ce), len(cf)) > 20:
         raise ValueError("Coulomb correction needs more than 20 coefficients at Float32 tolerances")
     return CoulombPolynomial(C=float(C), rc2=rc2, sx=2.0 / rc2, eshift=float(eshift), has_mesh=True,

@@ -24,7 +24,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
-from . import splits
+from . import prolates, splits
 from .engine import (ClusterPairEngine, DeviceEngine, ELLDeviceEngine, ELLEngine, ElectrostaticsSolver,
                      ElectrostaticsSpec)
 
@@ -115,16 +115,66 @@ class PPPM:
     neighborlist: object = None
 
 
+@dataclass
+class ESP:
+    """Ewald summation with prolates (Electrostatics.jl:101-155): the prolate split and a prolate window
+    of width ``order`` grid points.  Defaults follow the selection rules for a target relative force
+    error ``tolerance``: split shape c with psi(1) = tolerance, window shape from tolerance / 2 (the
+    smallest larger shape an FP32 mesh resolves, where that one is not), width from the table
+    (5, 5, 6, 7, 8 for 1e-3, 5e-4, 1e-4, 5e-5, 1e-5) and mesh spacing pi r_c / c."""
+    coulomb_prefactor: float | None = None
+    real_cutoff: float | None = None
+    tolerance: float | None = 1e-4
+    split_shape: float | None = None
+    window_shape: float | None = None
+    order: int | None = None
+    influence: str = "optimal"
+    alias_order: int = 2
+    mesh: tuple | None = None
+    mesh_spacing: float | None = None
+    relative_permittivity: float = 1.0
+    net_charge: str = "error"
+    boundary: str = "tin_foil"
+    real_space_modifier: str = "none"
+    exclusions: object = "topology"
+    exclude_bonded: bool = False
+    scaled_pairs: tuple = ()
+    pairs: str = "neighborlist"
+    neighborlist: object = None
+
+
+def _esp_spec(f: ESP) -> ElectrostaticsSpec:
+    """electrostatics_spec(::ESP, Float32) (src/workflow/Electrostatics.jl:253-272)."""
+    if f.split_shape is None or f.window_shape is None or f.order is None:
+        if f.tolerance is None:
+            raise ValueError("ESP needs `tolerance`, or explicit `split_shape`, `window_shape` and `order`.")
+    eps = None if f.tolerance is None else float(f.tolerance)
+    rc = float(f.real_cutoff)
+    c = prolates.prolate_shape_for_tolerance(eps) if f.split_shape is None else float(f.split_shape)
+    P = prolates.esp_order_for_tolerance(eps) if f.order is None else int(f.order)
+    c1 = prolates.esp_window_shape(eps, P, np.float32) if f.window_shape is None else float(f.window_shape)
+    spacing = math.pi * rc / c if (f.mesh is None and f.mesh_spacing is None) else f.mesh_spacing
+    if f.influence not in ("optimal", "deconvolution"):
+        raise ValueError(f"ESP influence must be optimal or deconvolution; got {f.influence}.")
+    return ElectrostaticsSpec(coulomb_prefactor=float(f.coulomb_prefactor), real_cutoff=rc,
+                              influence="esp" if f.influence == "optimal" else "esp_deconvolution", order=P,
+                              mesh=f.mesh, mesh_spacing=spacing, alias_order=f.alias_order,
+                              relative_permittivity=float(f.relative_permittivity), net_charge=f.net_charge,
+                              real_space_modifier=f.real_space_modifier, split_shape=c, window_shape=c1)
+
+
 def electrostatics_spec(f) -> ElectrostaticsSpec:
-    """Validated solver spec of a PME/PPPM descriptor."""
+    """Validated solver spec of a PME, PPPM or ESP descriptor."""
     if f.coulomb_prefactor is None or f.real_cutoff is None:
         raise ValueError(f"{type(f).__name__} requires coulomb_prefactor and real_cutoff.")
     if f.boundary != "tin_foil":
         raise ValueError(f"Only conducting (tin-foil) boundary conditions are implemented; got {f.boundary}.")
-    if (f.alpha is None) == (f.real_space_tolerance is None):
-        raise ValueError("Provide exactly one of alpha and real_space_tolerance.")
     if f.exclusions not in ("topology", None, ()) or f.exclude_bonded or len(f.scaled_pairs) > 0:
         raise NotImplementedError("Coulomb exceptions are not supported by this build of the cluster-pair path.")
+    if isinstance(f, ESP):
+        return _esp_spec(f)
+    if (f.alpha is None) == (f.real_space_tolerance is None):
+        raise ValueError("Provide exactly one of alpha and real_space_tolerance.")
     alpha = float(f.alpha) if f.alpha is not None else splits.alpha_from_tolerance(f.real_cutoff,
                                                                                     f.real_space_tolerance)
     if isinstance(f, PME):
@@ -268,7 +318,7 @@ class SimulationState:
 
     def _compile(self, system, forces):
         vdw = [f for f in forces if isinstance(f, (LennardJones, WCA))]
-        elec = [f for f in forces if isinstance(f, (PME, PPPM))]
+        elec = [f for f in forces if isinstance(f, (PME, PPPM, ESP))]
         if len(vdw) > 1 or len(elec) > 1:
             raise ValueError("at most one short-range vdW force and one electrostatics force")
         self.ell = None

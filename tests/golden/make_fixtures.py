@@ -88,9 +88,29 @@ def solver_cases() -> list[dict]:
     return [dict(C=C, rc=rc, box=box, n=120, cases=out, source="test/test_electrostatics.jl:299-341")]
 
 
+def esp_kats() -> dict:
+    """Prolate shapes of Table 2 (test/test_electrostatics.jl:55-58), the symmetric window value
+    (:88-91) and the ESP solver case of the Ewald comparison (:309)."""
+    lines = _lines("test/test_electrostatics.jl")
+    txt = "\n".join(lines[54:58])
+    table = [[float(a), float(b)] for a, b in re.findall(r"\(([0-9e.-]+), ([0-9.]+)\)", txt)]
+    rtol = float(re.search(r"rtol=([0-9e.-]+)", txt).group(1))
+    win = "\n".join(lines[87:91])
+    P, shape = re.search(r"ProlateWindow\((\d+), ([0-9.]+)\)", win).groups()
+    u = float(re.search(r"window_stencil\(pst, ([0-9.]+)\)", win).group(1))
+    k0 = int(re.search(r"k0 == (\d+)", win).group(1))
+    case = "\n".join(lines[308:309])
+    eps, mesh, Pm, ftol, etol = re.search(
+        r'\("ESP", _esp\(C, rc, ([0-9e.-]+), \(([0-9, ]+)\), (\d+)\), ([0-9e.-]+), ([0-9e.-]+)\)', case).groups()
+    return dict(shape_table=table, shape_rtol=rtol, source_table="test/test_electrostatics.jl:55-58",
+                window=dict(order=int(P), shape=float(shape), u=float(u), k0=k0, source="test/test_electrostatics.jl:88-91"),
+                solver=dict(eps=float(eps), mesh=[int(v) for v in mesh.split(",")], order=int(Pm), ftol=float(ftol),
+                            etol=float(etol), source="test/test_electrostatics.jl:309"))
+
+
 def main():
     data = dict(two_atom_lj=two_atom_lj(), face=face_positions(), neighbor_rows=neighbor_kats(),
-                electrostatics=solver_cases()[0],
+                electrostatics=solver_cases()[0], esp=esp_kats(),
                 self_energy="-C alpha/sqrt(pi) sum q^2 (test/test_electrostatics.jl:321)",
                 background_energy="-C pi (sum q)^2 / (2 alpha^2 V) (test/test_electrostatics.jl:409)")
     (HERE / "reference_kats.json").write_text(json.dumps(data, indent=1) + "\n")
