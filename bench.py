@@ -296,6 +296,153 @@ def run_ell_workload(pd, args, world, rank):
                                      "cap": post["cap"], "l2": "not flushed"}}))
 
 
+def pairs_within(pos, box, rc):
+    """Pairs closer than rc (each counted once), periodic, from a k-d tree on the host."""
+    from scipy.spatial import cKDTree
+    L = np.asarray(box, float)
+    p = np.asarray(pos, float) % L
+    return int(len(cKDTree(p, boxsize=L).query_pairs(rc, output_type="ndarray")))
+
+
+def load_peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        return {}
+
+
+def fp32_peak_tflops(peaks):
+    import torch
+    nsm = torch.cuda.get_device_properties(0).multi_processor_count
+    return nsm * 128 * 2 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
+
+
+def ell_config(pd, name, steps, warmup, peaks):
+    """One uncharged configuration on the ELL route, measured for the default bench line: atom-steps/s of
+    the captured step, the row pair kernel against the FP32 rate (algorithmic work: pairs inside r_c,
+    Newton-3 counted once, 20 flop per 3D LJ/WCA force pair, 16 in 2D) and the row build against HBM
+    (algorithmic bytes: positions read, rows and counts written)."""
+    import torch
+    if name in ("lj4k", "lj1m"):
+        ncell = 64 if name == "lj1m" else 10
+        pos, box = pd.synthetic.fcc_lattice(ncell, 0.8442, 0.05)
+        m = np.ones(len(pos))
+        v = pd.synthetic.maxwell_boltzmann(m, 0.72, seed=SEED)
+        force = pd.LennardJones(epsilon=1.0, sigma=1.0, cutoff=2.5, pairs="neighborlist",
+                                neighborlist=pd.CellList(buffer=0.3, capacity=96, rebuild_interval=10))
+        methods, dt, rc, fpair = [pd.ConstantVolume()], 0.005, 2.5, 20
+        desc = f"3D LJ fluid N={len(pos)} rho=0.8442 T=0.72 r_c=2.5 skin 0.3, NVE dt=0.005"
+    else:
+        pos, box = pd.synthetic.hex_random_2d(1024, 0.7, 1.0, 0.25, seed=SEED)
+        m = np.ones(len(pos))
+        v = pd.synthetic.maxwell_boltzmann(m, 1.0, seed=SEED, dim=2)
+        force = pd.WCA(epsilon=10.0, sigma=1.0, pairs="neighborlist",
+                       neighborlist=pd.CellList(buffer=0.4, capacity=32, rebuild_interval=10))
+        methods, dt, rc, fpair = [pd.Langevin(gamma=50.0, kT=1.0)], 2e-4, 2 ** (1 / 6), 16
+        desc = f"2D WCA disks N={len(pos)} packing 0.7 eps 10, Langevin gamma 50 kT 1, dt=2e-4"
+    sim = pd.Simulation(pd.ParticleSystem(pos, box, masses=m, velocities=v),
+                        pd.Integrator(dt=dt, forces=[force], methods=methods), seed=SEED)
+    st = sim.state
+    pd.evaluate_forces_into_f(sim)
+    st.step(warmup)
+    st.synchronize()
+    pre = st._ell_check()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st.stream)
+    st.step(steps)
+    e1.record(st.stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    post = st._ell_check()
+    n = st.n
+    # the row pair kernel alone and the row build alone (same stream, warm)
+    ell, s = st.ell, st.stream
+    xs = [t for t in (st.x, st.y, st.z) if t is not None]
+    f = [torch.empty(n, device="cuda") for _ in range(len(xs))]
+    pad = [None] * (3 - len(xs))
+    reps = 20
+    with torch.cuda.stream(s):
+        for _ in range(3):
+            ell.forces(*xs, *pad, *f, *pad, stream=s)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        for _ in range(reps):
+            ell.forces(*xs, *pad, *f, *pad, stream=s)
+        b.record(s)
+        b.synchronize()
+        pair_ms = a.elapsed_time(b) / reps
+        for _ in range(2):
+            ell.request(stream=s)
+            ell.update(*xs, *pad, stream=s)
+        a.record(s)
+        for _ in range(reps):
+            ell.request(stream=s)
+            ell.update(*xs, *pad, stream=s)
+        b.record(s)
+        b.synchronize()
+        build_ms = a.elapsed_time(b) / reps
+    entries = int(ell.counts_host().astype(np.int64).sum())
+    P = st.positions()
+    npairs = pairs_within(P if P.shape[1] == 3 else np.c_[P, np.zeros(len(P))],
+                          box if len(box) == 3 else (box[0], box[1], 10.0), rc)
+    fp32 = fp32_peak_tflops(peaks)
+    achieved = npairs * fpair / (pair_ms * 1e-3) / 1e12
+    dim = len(box)
+    build_bytes = 4 * dim * n + 4 * entries + 4 * n
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    gbs = build_bytes / (build_ms * 1e-3) / 1e9
+    return {"metric": "atom-steps/s", "value": n * 1000.0 / ms, "unit": "atom-steps/s", "ms_per_step": ms,
+            "steps": steps, "warmup": warmup, "workload": desc, "route": "ELL (cell list rows)",
+            "timed_builds": post["builds"] - pre["builds"], "lanes": post["lanes"], "cap": post["cap"],
+            "l2": "warm (step graph replayed back to back)",
+            "roofline": {"kernel": "row pair kernel (force only)", "bound": "fp32", "achieved": achieved,
+                         "peak": fp32, "unit": "TFLOP/s", "frac": achieved / fp32, "per_launch_ms": pair_ms,
+                         "pairs_within_rc": npairs, "flop_per_pair": fpair,
+                         "peak_source": "nominal FP32 FMA rate at sm_max_mhz"},
+            "row_build": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                          "per_build_ms": build_ms, "algorithmic_bytes": build_bytes,
+                          "note": "positions read, row entries and counts written (cell binning not counted)",
+                          "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback"}}
+
+
+def batch_config(pd, steps, warmup, peaks, replicas=512):
+    """The 512 LJ/WCA replicas as one batch (skin 0.45, lanes by the autotuner) for the default bench line:
+    atom-steps/s of the captured batched step and the batched pair kernel against the FP32 rate."""
+    import torch
+    specs = pd.synthetic.replica_set(replicas, seed=SEED)
+    systems = pd.batch.make_systems(specs)
+    b = pd.batch.BatchedReplicas(systems, skin=0.45)
+    b.evaluate()
+    tune = b.autotune_lanes()
+    b.step(warmup, 0.005)
+    b.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(b.stream)
+    b.step(steps, 0.005)
+    e1.record(b.stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    if b.status()["error"]:
+        raise RuntimeError(f"batch rows failed: {b.status()}")
+    ntot = sum(sy["n"] for sy in systems)
+    npairs = 0
+    for k, sy in enumerate(systems):
+        pos = np.stack([b.replica(k, t).double().cpu().numpy() for t in (b.x, b.y, b.z)], 1)
+        npairs += pairs_within(pos, sy["box"], 2.5 if sy["kind"] == "lj" else 2 ** (1 / 6))
+    pair_ms = tune["ms"][tune["lanes"]]
+    fp32 = fp32_peak_tflops(peaks)
+    achieved = npairs * 20 / (pair_ms * 1e-3) / 1e12
+    return {"metric": "atom-steps/s", "value": ntot * 1000.0 / ms, "unit": "atom-steps/s", "ms_per_step": ms,
+            "steps": steps, "warmup": warmup,
+            "workload": f"{replicas} LJ/WCA 3D replicas (total {ntot}), skin 0.45, one launch per stage, NVE dt 0.005",
+            "lanes": tune["lanes"], "l2": "warm",
+            "roofline": {"kernel": "k_batch_pairs (force only)", "bound": "fp32", "achieved": achieved, "peak": fp32,
+                         "unit": "TFLOP/s", "frac": achieved / fp32, "per_launch_ms": pair_ms,
+                         "pairs_within_rc": npairs, "flop_per_pair": 20,
+                         "peak_source": "nominal FP32 FMA rate at sm_max_mhz"}}
+
+
 def profiled_traffic(name: str):
     """DRAM bytes per launch (read + write) of one ncu capture, from its committed summary."""
     import re
@@ -381,7 +528,7 @@ def run_learned_form(pd, args, st, system, dt, flush):
         Fk, _ = pd.learned.ewald_oracle(rq, box, spec.C, spec.alpha, digits=10, parts=2)
         Ft, _ = pd.learned.ewald_oracle(rq, box, spec.C, spec.alpha, digits=10, parts=3)
         den = torch.sqrt((Ft ** 2).sum())
-        held.append(((x.clone(), y.clone(), z.clone()), Fk, den))
+        held.append(((x.clone(), y.clone(), z.clone()), Fk, den, Ft))
         fine = tr.mesh_forces(tr.fine, x, y, z).double()
         coarse = tr.mesh_forces(tr.coarse, x, y, z).double()
         V = tr.corr.correction(ones, x, y, z, tr.q, tr.typ)[:, :3].double()
@@ -408,6 +555,9 @@ def run_learned_form(pd, args, st, system, dt, flush):
     st2.evaluate_forces_into_f(False)
     ms_coarse = time_md_steps(st2, dt, args.steps, args.warmup, flush, args.no_flush)
     st2.solver.set_self_force_removal(SELF_FORCE_TABLE)
+    st2.engine.set_learned(tr.corr, None)   # the radial term alone: the learned form's lower bound in time
+    st2.evaluate_forces_into_f(False)
+    ms_radial = time_md_steps(st2, dt, args.steps, args.warmup, flush, args.no_flush)
     st2.engine.set_learned(tr.corr, tr.net)
     st2.evaluate_forces_into_f(False)
     ms_learned = time_md_steps(st2, dt, args.steps, args.warmup, flush, args.no_flush)
@@ -423,13 +573,26 @@ def run_learned_form(pd, args, st, system, dt, flush):
     equal = equal_error_comparison(pd, args, tr, spec, box, sys2, dt, flush, held, err["learned"], ms_learned,
                                    ms_coarse)
     ms_ik, mesh_ik = plain_step_ms(pd, args, sys2, dt, flush, "p3m_ik", 1.0, 5)
+    # ESP at the 1e-5 rules (width 8, spacing pi r_c / c): the reference's cheapest form at that accuracy
+    e_esp, mesh_esp, sp_esp = esp_error(pd, held, box, st.q.double().cpu().numpy(), dt, 1e-5)
+    ms_esp = esp_step_ms(pd, args, sys2, dt, flush, 1e-5)
     return {"ms_per_step": ms_learned, "value": ns_per_day(ms_learned),
             "learned_vs_plain_equal_error": equal,
+            "esp_at_1e-5": {"ms_per_step": ms_esp, "value": ns_per_day(ms_esp), "unit": "ns/day",
+                            "mesh": f"ESP tolerance 1e-5: {'x'.join(str(k) for k in mesh_esp)}, width {sp_esp.order}, "
+                                    f"spacing {sp_esp.mesh_spacing:.3f} A, split shape {sp_esp.split_shape:.3f}, "
+                                    f"window shape {sp_esp.window_shape:.3f}",
+                            "force_error_vs_fp64_ewald": e_esp,
+                            "error_note": "total Coulomb force (prolate real space + mesh) against the full FP64 "
+                                          "Ewald force, over its RMS"},
             "pppm_ik": {"ms_per_step": ms_ik, "value": ns_per_day(ms_ik), "unit": "ns/day",
                         "mesh": f"P3M-ik 1.0 A ({'x'.join(str(k) for k in mesh_ik)}), order 5, alias order 2 "
                                 "(the configuration's PPPM variant)",
                         "force_error_vs_fp64_ewald": err["plain_pppm_ik"]},
             "coarse_only": {"ms_per_step": ms_coarse, "value": ns_per_day(ms_coarse)},
+            "coarse_radial_no_network": {"ms_per_step": ms_radial, "value": ns_per_day(ms_radial),
+                                         "note": "coarse mesh, self force removed, fitted radial term (s = 1): "
+                                                 "descriptors and rows without the network"},
             "plain_e5": {"ms_per_step": ms_e5, "value": ns_per_day(ms_e5),
                          "mesh": f"SPME {E5_SPACING} A ({'x'.join(str(k) for k in solver_e5.mesh)}), order {E5_ORDER}"},
             "force_error_vs_fp64_ewald": err,
@@ -456,10 +619,46 @@ def mesh_error(pd, tr, solver, held):
     held-out snapshots (over the RMS of the full Ewald force)."""
     import torch
     e = []
-    for (x, y, z), Fk, den in held:
+    for (x, y, z), Fk, den, _ in held:
         f = tr.mesh_forces(solver, x, y, z).double()
         e.append(float(torch.sqrt(((f - Fk) ** 2).sum()) / den))
     return float(np.mean(e))
+
+
+ESP_TOLERANCES = (3e-3, 1e-3, 1e-4)   # ESP settings of the equal-error sweep (workflow rules per tolerance; the
+#                                      rules give no valid window above about 3e-3)
+
+
+def esp_error(pd, held, box, q64, dt, tol):
+    """Mean relative RMS error of the ESP solver's total Coulomb force (prolate real space + mesh) against
+    the full FP64 Ewald force on the held-out snapshots (the prolate split differs from the Gaussian one, so
+    the comparison is of total forces).  Returns (error, mesh dims)."""
+    import torch
+    el = pd.ESP(coulomb_prefactor=pd.synthetic.COULOMB_EV_A, real_cutoff=RC, tolerance=tol)
+    st = None
+    e = []
+    for (x, y, z), _, den, Ft in held:
+        if st is None:
+            pos = torch.stack([x, y, z], 1).double().cpu().numpy()
+            system = pd.ParticleSystem(pos, box, charges=q64, masses=np.ones(len(q64)))
+            st = pd.Simulation(system, pd.Integrator(dt=dt, forces=[el])).state
+        else:
+            st.x.copy_(x)
+            st.y.copy_(y)
+            st.z.copy_(z)
+            torch.cuda.synchronize()
+        st.evaluate_forces_into_f(False)
+        F = torch.stack([st.fx, st.fy, st.fz], 1).double()
+        e.append(float(torch.sqrt(((F - Ft) ** 2).sum()) / den))
+    return float(np.mean(e)), st.solver.mesh, st.solver.spec
+
+
+def esp_step_ms(pd, args, sys2, dt, flush, tol):
+    """Device time of the captured NVE step of the melt with LJ + ESP at a tolerance."""
+    el = pd.ESP(coulomb_prefactor=pd.synthetic.COULOMB_EV_A, real_cutoff=RC, tolerance=tol)
+    st = pd.Simulation(sys2, pd.Integrator(dt=dt, forces=forces(pd, args.buffer, args.prune)[:1] + [el])).state
+    st.evaluate_forces_into_f(False)
+    return time_md_steps(st, dt, min(args.steps, 40), args.warmup, flush, args.no_flush)
 
 
 def plain_step_ms(pd, args, sys2, dt, flush, kind, spacing, order):
@@ -495,10 +694,20 @@ def equal_error_comparison(pd, args, tr, spec, box, sys2, dt, flush, held, targe
                 solver.close()
                 if e <= target:
                     break
+    for tol in ESP_TOLERANCES:   # coarsest first
+        e, mesh, sp = esp_error(pd, held, box, q64, dt, tol)
+        sweep.append({"kind": "esp", "tolerance": tol, "spacing": round(sp.mesh_spacing, 4), "order": sp.order,
+                      "mesh": "x".join(str(k) for k in mesh), "error": e,
+                      "error_note": "total Coulomb force against the full Ewald force"})
+        if e <= target:
+            break
     timed = []
     for c in sweep:
         if c["error"] <= target:
-            ms, _ = plain_step_ms(pd, args, sys2, dt, flush, c["kind"], c["spacing"], c["order"])
+            if c["kind"] == "esp":
+                ms = esp_step_ms(pd, args, sys2, dt, flush, c["tolerance"])
+            else:
+                ms, _ = plain_step_ms(pd, args, sys2, dt, flush, c["kind"], c["spacing"], c["order"])
             c["ms_per_step"] = ms
             timed.append(c)
     best = min(timed, key=lambda c: c["ms_per_step"]) if timed else None
@@ -781,6 +990,8 @@ def main():
     ap.add_argument("--epochs", type=int, default=4, help="Adam epochs of the learned form")
     ap.add_argument("--heldout", type=int, default=4, help="held-out snapshots for the force errors")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned coarse-mesh form")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the short runs of the other configurations (LJ 4k / 1M, 2D WCA 1M, 512 replicas)")
     ap.add_argument("--form", default="plain", choices=["plain", "learned"],
                     help="with --profile: profile the plain step or the learned coarse-mesh step")
     ap.add_argument("--profile", action="store_true",
@@ -935,8 +1146,10 @@ def main():
         learned = run_learned_form(pd, args, st, system, dt, flush)
         learned["value"] = world * learned["value"]
         learned["coarse_only"]["value"] = world * learned["coarse_only"]["value"]
+        learned["coarse_radial_no_network"]["value"] = world * learned["coarse_radial_no_network"]["value"]
         learned["plain_e5"]["value"] = world * learned["plain_e5"]["value"]
         learned["pppm_ik"]["value"] = world * learned["pppm_ik"]["value"]
+        learned["esp_at_1e-5"]["value"] = world * learned["esp_at_1e-5"]["value"]
         learned["ms_per_step"] = max_over_ranks(world, learned["ms_per_step"])
     # the headline is the learned form only where it reaches the plain form's force error
     form = "plain: fine-mesh SPME (learned coarse-mesh form measured under forms.learned_coarse)"
@@ -946,6 +1159,14 @@ def main():
             value = learned["value"]
             ms_step = learned["ms_per_step"]
             form = "learned coarse-mesh: coarse SPME + network at or below the plain form's force error"
+    configs = None
+    if not args.no_configs:
+        configs = {"config0_lj4k": ell_config(pd, "lj4k", 200, args.warmup, peaks),
+                   "config1a_lj1m": ell_config(pd, "lj1m", 30, args.warmup, peaks),
+                   "config1b_wca2d1m": ell_config(pd, "wca2d1m", 30, args.warmup, peaks),
+                   "config4_batch512": batch_config(pd, 30, args.warmup, peaks)}
+        for c in configs.values():
+            c["value"] = world * c["value"]
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         ora = ge.load_oracle()
@@ -974,11 +1195,13 @@ def main():
                                            "(the configuration's settings)"},
                          "plain_at_1e-5_vs_ewald": learned.pop("plain_e5") if learned else None,
                          "pppm_ik": learned.pop("pppm_ik") if learned else None,
+                         "esp_at_1e-5": learned.pop("esp_at_1e-5") if learned else None,
                          "learned_vs_plain_equal_error": learned.pop("learned_vs_plain_equal_error")
                          if learned else None,
                          "learned_coarse": learned},
                "e2e": {"value": world * ns_per_day(e2e_ms), "unit": "ns/day", "h2d_bytes_per_step": 24 * n,
                        "d2h_bytes_per_step": 24 * n, "ms_per_step": e2e_ms},
+               "configs": configs,
                "gpu_launches": gpu_launches,
                "kernels": {"every_step": kernels_always, "per_build": KERNELS_BUILD,
                            "cufft_per_step": "2 transforms (library kernels, not counted)"},

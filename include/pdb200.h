@@ -472,7 +472,8 @@ int pd_learned_status(pd_learned *h, pd_ell_stats *out);
 int pd_learned_resize(pd_learned *h, int cap);
 /* Attach (or with NULL detach) the correction to a step engine: every force pass then adds
  * corr = s V to the forces before the closing kick (the descriptors and the network run on a
- * third stream beside the pair pass and the mesh). */
+ * third stream beside the pair pass and the mesh).  net = NULL attaches the radial term alone
+ * (corr = V, s = 1: the descriptors run, the network does not). */
 int pd_md_set_learned(pd_md *md, pd_learned *h, pd_mlp *net);
 
 /* ------------------------------------------------------------------------------------------

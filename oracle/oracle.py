@@ -112,11 +112,39 @@ def pairs_cells(pos, box, *, q=None, kind=1, sigma=1.0, eps=1.0, rc_lj=2.5, eshi
     return dict(F=np.stack([fx, fy, fz], 1), E=e, W=w)
 
 
+def pair_term_scales(pos, box, *, kind=1, sigma=1.0, eps=1.0, rc_lj=2.5, band=1e-6):
+    """(S_i, S_E, A_i): S_i = sum_j (|f_rep| + |f_att|)_ij per particle and S_E = sum over pairs of
+    |u_rep| + |u_att| + |e_shift| (WCA: e_shift = -eps), the scales of the FP32 rounding error of the
+    force and energy sums of LJ (kind 1) or WCA (kind 2) pairs inside r_c (see pair_force_abs_sums);
+    A_i = sum of |f_ij| over the pairs within a relative ``band`` of r_c, which FP32 rounding of r^2 may
+    put on either side of the cutoff (the truncated LJ force does not vanish there)."""
+    S = pair_force_abs_sums(pos, box, kind=kind, sigma=sigma, eps=eps, rc_lj=rc_lj)
+    from scipy.spatial import cKDTree
+    L = np.asarray(box, float)
+    p = np.asarray(pos, float) % L
+    tree = cKDTree(p, boxsize=L)
+    ij = tree.query_pairs(rc_lj * (1.0 + band), output_type="ndarray")
+    d = p[ij[:, 0]] - p[ij[:, 1]]
+    d -= L * np.round(d / L)
+    r2 = (d * d).sum(1)
+    inside = r2 < rc_lj * rc_lj
+    ir6 = (sigma * sigma / r2) ** 3
+    esh = eps if kind == 2 else 0.0
+    SE = float((4.0 * eps * (ir6 * ir6 + ir6) + esh)[inside].sum())
+    edge = np.abs(np.sqrt(r2) - rc_lj) <= band * rc_lj
+    fe = np.abs(24.0 * eps * (2.0 * ir6 - 1.0) * ir6 / np.sqrt(r2)) * edge
+    A = np.zeros(len(p))
+    np.add.at(A, ij[:, 0], fe)
+    np.add.at(A, ij[:, 1], fe)
+    return S, SE, A
+
+
 def pair_force_abs_sums(pos, box, *, kind=1, sigma=1.0, eps=1.0, rc_lj=2.5):
-    """S_i = sum_j |f_ij| over the LJ (kind 1) or WCA (kind 2) pairs inside r_c, in FP64: the scale of
-    the rounding error of an FP32 sum of pair forces (each pair force is computed to a few ulps of its
-    own magnitude, so |F_i(FP32) - F_i| stays within a small multiple of eps_32 S_i however much the
-    pair forces cancel in F_i)."""
+    """S_i = sum_j (|f_rep| + |f_att|)_ij over the LJ (kind 1) or WCA (kind 2) pairs inside r_c, in FP64:
+    the scale of the rounding error of an FP32 sum of pair forces.  Each pair force is the difference of
+    a repulsive 48 eps sigma^12 / r^13 and an attractive 24 eps sigma^6 / r^7 term, computed to a few ulps
+    of their magnitudes (they cancel where the force changes sign, at the WCA cutoff), so
+    |F_i(FP32) - F_i| stays within a small multiple of eps_32 S_i however much the terms cancel."""
     from scipy.spatial import cKDTree
     L = np.asarray(box, float)
     p = np.asarray(pos, float) % L
@@ -127,7 +155,7 @@ def pair_force_abs_sums(pos, box, *, kind=1, sigma=1.0, eps=1.0, rc_lj=2.5):
     r2 = (d * d).sum(1)
     ir2 = sigma * sigma / r2
     ir6 = ir2 * ir2 * ir2
-    f = np.abs(24.0 * eps * (2.0 * ir6 - 1.0) * ir6 / np.sqrt(r2))
+    f = 24.0 * eps * (2.0 * ir6 + 1.0) * ir6 / np.sqrt(r2)
     S = np.zeros(len(p))
     np.add.at(S, ij[:, 0], f)
     np.add.at(S, ij[:, 1], f)

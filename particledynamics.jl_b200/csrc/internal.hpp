@@ -192,6 +192,7 @@ int mlp_forward_launch(const pd_mlp *q, const void *X, int n, float *s, const fl
 int learned_correction_launch(pd_learned *h, const pd_mlp *net, const float *x, const float *y, const float *z,
                               const float *q, const int *type, float4 *corr, cudaStream_t s);
 const float4 *learned_corr(const pd_learned *h);
+const float4 *learned_radial(const pd_learned *h);
 int ell_sort_cells_launch(const int *cell_of, int n, int ncell, int *cell_count, int *cell_off, int *sorted, int *tmp,
                           long long *st, cudaStream_t s);
 

@@ -273,10 +273,12 @@ int learned_correction_launch(pd_learned *h, const pd_mlp *net, const float *x, 
                               const float *q, const int *type, float4 *corr, cudaStream_t s) {
     int rc;
     if ((rc = descriptors_launch(h, x, y, z, q, type, h->X, h->V, nullptr, s))) return rc;
+    if (!net) return PD_OK;   // radial term only: the correction is V itself (s = 1)
     return mlp_forward_launch(net, h->X, h->n, nullptr, h->V, corr ? corr : h->corr, s);
 }
 
 const float4 *learned_corr(const pd_learned *h) { return h->corr; }
+const float4 *learned_radial(const pd_learned *h) { return h->V; }
 
 static void learned_free(pd_learned *h) {
     if (h->ell) pd_ell_destroy(h->ell);

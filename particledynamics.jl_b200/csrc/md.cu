@@ -251,7 +251,10 @@ static int enqueue_forces(pd_md *md, int energy, float half_dt, cudaStream_t s) 
         if (md->learned) PD_CUDA(cudaStreamWaitEvent(s, md->ev_join2, 0));
         rc = mesh_gather_join(m, c, c->xq, c->perm, c->counts + W_NS, c->nsmax, st.fx, st.fy, st.fz, st.vx, st.vy,
                               st.vz, st.inv_mass, st.inv_mass_uniform, half_dt, st.epot, st.vir6, st.vglobal6, st.q,
-                              md->half_c_self, md->learned ? learned_corr(md->learned) : nullptr, energy, s);
+                              md->half_c_self,
+                              md->learned ? (md->net ? learned_corr(md->learned) : learned_radial(md->learned))
+                                          : nullptr,
+                              energy, s);
         if (rc) return rc;
     } else {
         const int blocks = (c->nslot + 255) / 256;
@@ -419,7 +422,7 @@ int pd_md_evaluate(pd_md *md, int energy, pd_stream_t sp) {
 
 int pd_md_set_learned(pd_md *md, pd_learned *h, pd_mlp *net) {
     PD_CHECK(md, PD_EINVAL, "pd_md_set_learned: null handle");
-    PD_CHECK(!h == !net, PD_EINVAL, "pd_md_set_learned: the correction needs both the handle and the network");
+    PD_CHECK(h || !net, PD_EINVAL, "pd_md_set_learned: a network needs the correction handle");
     PD_CHECK(!h || md->m, PD_EINVAL, "pd_md_set_learned: the correction needs a mesh");
     if (h && !md->side2) {
         int prio_lo = 0, prio_hi = 0;

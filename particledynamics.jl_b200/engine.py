@@ -532,7 +532,8 @@ class DeviceEngine:
 
     def set_learned(self, correction=None, net=None):
         """Attach the learned coarse-mesh correction (``learned.LearnedCorrection`` + ``learned.MLPNetwork``):
-        every force pass then adds s_i V_i before the closing kick.  None detaches it."""
+        every force pass then adds s_i V_i before the closing kick.  A correction without a network adds the
+        radial term V_i alone (s = 1); None detaches it."""
         N.call("pd_md_set_learned", self.handle, correction.handle if correction is not None else None,
                net.handle if net is not None else None)
         self._learned = (correction, net)
@@ -620,6 +621,15 @@ class ELLEngine:
 
     def resize(self, capacity: int):
         N.call("pd_ell_resize", self.handle, int(capacity))
+
+    def counts_host(self) -> np.ndarray:
+        """Host copy of the row lengths."""
+        r, c = C.c_void_p(), C.c_void_p()
+        N.call("pd_ell_rows", self.handle, C.byref(r), C.byref(c))
+        counts = torch.empty(self.n, dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        _memcpy_d2d(counts.data_ptr(), c.value, 4 * self.n)
+        return counts.cpu().numpy()
 
     def rows_host(self):
         """Host copies of the rows (as a list of neighbour-id arrays, truncated at the capacity)."""

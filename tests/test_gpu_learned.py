@@ -215,6 +215,17 @@ def test_step_engine_adds_the_correction(pd, cuda):
     st2.synchronize()
     assert np.allclose(st1.positions(), st2.positions(), rtol=0, atol=1e-4)
     assert net.error() == 0 and lc.status()["error"] == 0
+    # the radial term alone (no network): the forces gain V, the correction at s = 1
+    st3 = make()
+    lc3 = pd.learned.LearnedCorrection(n, box)
+    lc3.set_radial(lc.coef)
+    st3.engine.set_learned(lc3, None)
+    st3.evaluate_forces_into_f(False)
+    f3 = st3.forces()
+    ones = pd.learned.MLPNetwork(pd.learned.init_params(0, s0=1.0, out_scale=0.0))
+    V = lc3.correction(ones, st3.x, st3.y, st3.z, st3.q, st3.typ).cpu().numpy()
+    assert np.abs(V[:, :3]).max() > 0
+    assert np.allclose(f3 - f0, V[:, :3], rtol=1e-4, atol=1e-5 * np.abs(f0).max())
 
 
 def test_trained_network_beats_the_coarse_mesh(pd, cuda):
