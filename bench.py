@@ -1064,6 +1064,16 @@ def main():
     st.cluster.set_pair_shape(*(int(v) for v in best.split("x")))
     tune["step_ms"] = step_ms
     tune["nsplit"], tune["warps"] = (int(v) for v in best.split("x"))
+    # where the pair pass starts in the step (after the prune, the mesh spread or the forward transform),
+    # timed the same way: a later start leaves the critical mesh chain more of the GPU
+    sched_ms = {}
+    for mode in (0, 1, 2):
+        st.engine.set_schedule(mode)
+        sched_ms[mode] = time_md_steps(st, dt, 40, 3, flush, args.no_flush)
+    best_sched = min(sched_ms, key=sched_ms.get)
+    st.engine.set_schedule(best_sched)
+    tune["schedule_step_ms"] = {("after prune", "after spread", "after forward FFT")[k]: v for k, v in sched_ms.items()}
+    tune["pair_wait"] = best_sched
     # kernels of one eager step: the always-run part (the prune kernel included: it is launched every
     # step and returns at once unless the device decision asks for a prune) plus the build kernels, which
     # the captured graph launches only inside its conditional node on steps that rebuild the list
@@ -1186,6 +1196,7 @@ def main():
                           "list_buffer_A": args.buffer, "prune_buffer_A": args.prune,
                           "pair_shape": {"nsplit": tune["nsplit"], "warps": tune["warps"],
                                          "pair_pass_ms": tune["ms"], "step_ms": tune["step_ms"]},
+                          "schedule": {"pair_wait": tune["pair_wait"], "step_ms": tune["schedule_step_ms"]},
                           "l2": "flushed (256 MiB write) before every timed step" if not args.no_flush else "warm",
                           "timed_builds": timed_builds, "timed_prunes": timed_prunes},
                "roofline": roofline, "cpu_baseline": cpu,

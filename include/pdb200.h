@@ -318,6 +318,11 @@ int pd_md_evaluate(pd_md *md, int energy, pd_stream_t s);
  * step dt; energies on the last step when energy_last = 1.  use_graph = 1 replays one captured
  * CUDA graph per step (captured on the first call); 0 launches the kernels directly. */
 int pd_md_step(pd_md *md, int nsteps, float dt, int energy_last, int use_graph, pd_stream_t s);
+/* Schedule of the step (no counterpart in the reference; a tuning knob of this build): the pair
+ * pass, which runs beside the mesh chain, starts after the prune (pair_wait 0), after the mesh
+ * chain's spread (1) or after its forward transform (2).  Later starts leave the critical mesh chain
+ * more of the GPU; the forces are the same.  Captured steps are captured again after a change. */
+int pd_md_set_schedule(pd_md *md, int pair_wait);
 /* Steps through the C ABI with host buffers: copies x, v (pinned host, 3n floats each,
  * [x..., y..., z...]) to the device, runs nsteps, copies them back with the potential energy
  * sum (double) of the last step.  The positions are copied back on an internal stream as soon as

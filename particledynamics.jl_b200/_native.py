@@ -149,6 +149,7 @@ _SIGS = {
     "pd_cluster_order": (_fp, [_p]),
     "pd_cluster_buffers": (C.c_int, [_p, C.POINTER(_p), C.POINTER(_p), C.POINTER(_p), C.POINTER(_p),
                                      C.POINTER(_p), C.POINTER(_p)]),
+    "pd_md_set_schedule": (C.c_int, [_p, C.c_int]),
     "pd_mesh_create": (C.c_int, [C.POINTER(_p), C.POINTER(MeshParams), C.POINTER(C.c_double)]),
     "pd_mesh_create_prolate": (C.c_int, [C.POINTER(_p), C.POINTER(MeshParams), C.POINTER(Prolate),
                                          C.POINTER(C.c_double)]),

@@ -171,7 +171,9 @@ struct pd_mesh {
 
 namespace pdb {
 // Mesh internals used by the step engine.
-int mesh_transform_packed(pd_mesh *m, const float4 *xq, int nchunks, const int *ns_dev, int energy, cudaStream_t s);
+// ev_spread / ev_r2c (optional) are recorded once the spread / the forward transform are enqueued.
+int mesh_transform_packed(pd_mesh *m, const float4 *xq, int nchunks, const int *ns_dev, int energy, cudaStream_t s,
+                          cudaEvent_t ev_spread = nullptr, cudaEvent_t ev_r2c = nullptr);
 int mesh_gather_join(pd_mesh *m, pd_cluster *c, const float4 *xq, const int *perm, const int *ns_dev, int nchunks,
                      float *fx, float *fy, float *fz, float *vx, float *vy, float *vz, const float *inv_mass,
                      float inv_mass_uniform, float half_dt, float *epot, float *vir6, float *vglobal6, const float *q,

@@ -32,6 +32,11 @@ struct pd_md {
     cudaStream_t body = nullptr;   // captures the bodies of the conditional nodes
     bool cond_nodes = true;        // false after a failed conditional capture: gated kernels instead
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // schedule: the pair pass starts after the prune (0), or also waits until the mesh chain has
+    // finished its spread (1) or its forward transform (2), so that the critical mesh chain meets
+    // less contention from the pair pass's CTAs (pd_md_set_schedule; the bench times the three)
+    int pair_wait = 0;
+    cudaEvent_t ev_spread = nullptr, ev_r2c = nullptr;
     cudaGraphExec_t exec[2] = {nullptr, nullptr};   // [energy]
     float exec_dt[2] = {0.f, 0.f};
     cudaStream_t exec_stream[2] = {nullptr, nullptr};
@@ -220,7 +225,9 @@ static int fork_mesh(pd_md *md, int energy, cudaStream_t s) {
     int rc;
     PD_CUDA(cudaEventRecord(md->ev_fork, s));
     PD_CUDA(cudaStreamWaitEvent(md->side, md->ev_fork, 0));
-    if ((rc = mesh_transform_packed(md->m, c->xq, c->nsmax, c->counts + W_NS, energy, md->side))) return rc;
+    if ((rc = mesh_transform_packed(md->m, c->xq, c->nsmax, c->counts + W_NS, energy, md->side, md->ev_spread,
+                                    md->ev_r2c)))
+        return rc;
     PD_CUDA(cudaEventRecord(md->ev_join, md->side));
     return PD_OK;
 }
@@ -245,6 +252,7 @@ static int enqueue_forces(pd_md *md, int energy, float half_dt, cudaStream_t s) 
     pd_mesh *m = md->m;
     pd_md_state &st = md->st;
     int rc;
+    if (m && md->pair_wait) PD_CUDA(cudaStreamWaitEvent(s, md->pair_wait == 1 ? md->ev_spread : md->ev_r2c, 0));
     if ((rc = cluster_pairs_launch(c, energy, s))) return rc;
     if (m) {
         PD_CUDA(cudaStreamWaitEvent(s, md->ev_join, 0));
@@ -349,6 +357,8 @@ int pd_md_create(pd_md **out, pd_cluster *c, pd_mesh *m, const pd_md_state *st, 
     if (cudaStreamCreateWithPriority(&md->side, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
         cudaStreamCreateWithFlags(&md->body, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&md->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&md->ev_spread, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&md->ev_r2c, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&md->ev_join, cudaEventDisableTiming) != cudaSuccess ||
         cudaStreamCreateWithFlags(&md->copy, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&md->ev_pos, cudaEventDisableTiming) != cudaSuccess ||
@@ -367,6 +377,8 @@ int pd_md_destroy(pd_md *md) {
     for (int k = 0; k < 2; ++k)
         if (md->exec[k]) cudaGraphExecDestroy(md->exec[k]);
     if (md->ev_fork) cudaEventDestroy(md->ev_fork);
+    if (md->ev_spread) cudaEventDestroy(md->ev_spread);
+    if (md->ev_r2c) cudaEventDestroy(md->ev_r2c);
     if (md->ev_join) cudaEventDestroy(md->ev_join);
     if (md->ev_pos) cudaEventDestroy(md->ev_pos);
     if (md->ev_copied) cudaEventDestroy(md->ev_copied);
@@ -439,6 +451,20 @@ int pd_md_set_learned(pd_md *md, pd_learned *h, pd_mlp *net) {
             cudaGraphExecDestroy(md->exec[k]);
             md->exec[k] = nullptr;
         }
+    return PD_OK;
+}
+
+int pd_md_set_schedule(pd_md *md, int pair_wait) {
+    PD_CHECK(md, PD_EINVAL, "pd_md_set_schedule: null handle");
+    PD_CHECK(pair_wait >= 0 && pair_wait <= 2, PD_EINVAL, "pd_md_set_schedule: pair_wait 0, 1 or 2");
+    if (md->pair_wait != pair_wait) {
+        md->pair_wait = pair_wait;
+        for (int k = 0; k < 2; ++k)   // captured steps hold the old dependencies
+            if (md->exec[k]) {
+                cudaGraphExecDestroy(md->exec[k]);
+                md->exec[k] = nullptr;
+            }
+    }
     return PD_OK;
 }
 

@@ -492,7 +492,8 @@ static int compute_self_table(pd_mesh *m) {
     return PD_OK;
 }
 
-int mesh_transform_packed(pd_mesh *m, const float4 *xq, int nchunks, const int *ns_dev, int energy, cudaStream_t s) {
+int mesh_transform_packed(pd_mesh *m, const float4 *xq, int nchunks, const int *ns_dev, int energy, cudaStream_t s,
+                          cudaEvent_t ev_spread, cudaEvent_t ev_r2c) {
     const float Lx = (float)m->box[0], Ly = (float)m->box[1], Lz = (float)m->box[2];
     PD_CHECK(m->p.order >= MESH_ORDER_MIN && m->p.order <= MESH_ORDER_MAX, PD_EINVAL, "unsupported order %d",
              m->p.order);
@@ -503,8 +504,10 @@ int mesh_transform_packed(pd_mesh *m, const float4 *xq, int nchunks, const int *
         launch_spread_t<WIN_BSPLINE>(m->p.order, xq, nchunks, ns_dev, m->gridA, m->K1, m->K2, m->K3, Lx, Ly, Lz,
                                      window_poly(m), s);
     PD_LAUNCHED();
+    if (ev_spread) PD_CUDA(cudaEventRecord(ev_spread, s));
     PD_CUFFT(cufftSetStream(m->fwd, s));
     PD_CUFFT(cufftExecR2C(m->fwd, m->gridA, m->spec));
+    if (ev_r2c) PD_CUDA(cudaEventRecord(ev_r2c, s));
     if (energy) PD_CUDA(cudaMemsetAsync(m->acc, 0, 7 * sizeof(double), s));
     const int blocks = (m->nmodes + 255) / 256;
     if (energy)

@@ -281,35 +281,51 @@ __global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_spread(const
     constexpr int PH = (P + 1) / 2;
 
     if (b.fits) {
+        // The brick accumulates in 32-bit fixed point: integer shared-memory reductions are native
+        // (a float reduction is not), and integer sums are exact, so a chunk's brick does not depend
+        // on the order of its atomics.  The window weights lie in [0, 1], so no node of the brick
+        // exceeds the chunk's sum of |q| in magnitude; the scale is the largest power of two that
+        // keeps that sum below 2^30.  Each contribution rounds to a step of at most sum|q| / 2^30.
+        __shared__ float s_qabs[MESH_THREADS / 32];
+        float qa = (valid && h == 0) ? fabsf(v.w) : 0.f;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) qa += __shfl_xor_sync(0xffffffffu, qa, off);
+        if ((t & 31) == 0) s_qabs[t >> 5] = qa;
         const int nb4 = (b.e1 * b.e2 * b.e3 + 3) >> 2;
-        float4 *tile4 = reinterpret_cast<float4 *>(tile);
-        for (int k = t; k < nb4; k += MESH_THREADS) tile4[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        int4 *itile4 = reinterpret_cast<int4 *>(tile);
+        int *itile = reinterpret_cast<int *>(tile);
+        for (int k = t; k < nb4; k += MESH_THREADS) itile4[k] = make_int4(0, 0, 0, 0);
         __syncthreads();
+        const float qsum = fmaxf(s_qabs[0] + s_qabs[1] + s_qabs[2] + s_qabs[3], 1e-30f);
+        const int ex = min(30 - (int)ceilf(log2f(qsum)), 126);   // qsum * 2^ex <= 2^30, 2^ex finite
+        const float scale = ldexpf(1.f, ex), inv_scale = ldexpf(1.f, -ex);
         if (valid) {
+            const float qs = v.w * scale;
 #pragma unroll
             for (int j3 = 0; j3 < P; ++j3) {   // this half's z nodes only (warp-uniform test)
             if ((j3 < PH) != (h == 0)) continue;
-                const float q3 = v.w * w3[j3];
+                const float q3 = qs * w3[j3];
 #pragma unroll
                 for (int j2 = 0; j2 < P; ++j2) {
                     const float q23 = q3 * w2[j2];
-                    float *row = tile + ((d3 + j3) * b.e2 + (d2 + j2)) * b.e1 + d1;
+                    int *row = itile + ((d3 + j3) * b.e2 + (d2 + j2)) * b.e1 + d1;
 #pragma unroll
-                    for (int j1 = 0; j1 < P; ++j1) red_add_shared(row + j1, q23 * w1[j1]);
+                    for (int j1 = 0; j1 < P; ++j1) atomicAdd(row + j1, __float2int_rn(q23 * w1[j1]));
                 }
             }
         }
         __syncthreads();
         if (b.vec) {
             for_brick(b, rowbase, K1, [&](int kt, size_t kg) {
-                const float4 val = tile4[kt];
-                if (val.x != 0.f || val.y != 0.f || val.z != 0.f || val.w != 0.f)
-                    red_add_v4(grid + kg, val.x, val.y, val.z, val.w);
+                const int4 iv = itile4[kt];
+                if (iv.x != 0 || iv.y != 0 || iv.z != 0 || iv.w != 0)
+                    red_add_v4(grid + kg, (float)iv.x * inv_scale, (float)iv.y * inv_scale, (float)iv.z * inv_scale,
+                               (float)iv.w * inv_scale);
             });
         } else {
             for_brick(b, rowbase, K1, [&](int kt, size_t kg) {
-                const float val = tile[kt];
-                if (val != 0.f) red_add(grid + kg, val);
+                const int iv = itile[kt];
+                if (iv != 0) red_add(grid + kg, (float)iv * inv_scale);
             });
         }
     } else if (valid) {

@@ -538,6 +538,11 @@ class DeviceEngine:
                net.handle if net is not None else None)
         self._learned = (correction, net)
 
+    def set_schedule(self, pair_wait: int):
+        """Start the pair pass after the prune (0), the mesh spread (1) or the forward transform (2)."""
+        N.call("pd_md_set_schedule", self.handle, int(pair_wait))
+        self.pair_wait = int(pair_wait)
+
     def step(self, nsteps: int, dt: float, energy_last=False, use_graph=True, stream=None):
         N.call("pd_md_step", self.handle, int(nsteps), float(dt), int(bool(energy_last)), int(bool(use_graph)),
                _stream(stream))

@@ -177,3 +177,25 @@ def test_warmed_calls_allocate_nothing(pd, cuda, kind):
     torch.cuda.synchronize()
     free1, alloc1 = torch.cuda.mem_get_info()[0], torch.cuda.memory_allocated()
     assert free1 == free0 and alloc1 == alloc0, (free0 - free1, alloc1 - alloc0)
+
+
+def test_schedules_give_the_same_step(pd, cuda):
+    # the pair pass may start after the prune, the mesh spread or the forward transform (a scheduling
+    # knob of the captured step): forces and trajectories agree up to the order of float reductions
+    ref = None
+    for mode in (0, 1, 2):
+        sim, q, box = _melt_sim(pd, 4000, seed=31)
+        st = sim.state
+        st.engine.set_schedule(mode)
+        pd.evaluate_forces_into_f(sim, energy=True)
+        F0 = st.forces()
+        st.step(20, energy_last=True, use_graph=True)
+        out = (F0, st.positions(), st.potential_energy())
+        if ref is None:
+            ref = out
+            continue
+        assert np.linalg.norm(out[0] - ref[0]) <= 1e-6 * np.linalg.norm(ref[0])
+        D = out[1] - ref[1]
+        D -= np.array(box) * np.round(D / np.array(box))
+        assert np.max(np.abs(D)) < 1e-3
+        assert abs(out[2] - ref[2]) < 1e-4 * abs(ref[2])
