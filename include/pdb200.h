@@ -117,6 +117,8 @@ typedef struct {
     int nsmax, nslot;       /* super-cluster bound and slot count of this geometry */
     int last_build, last_prune; /* decision flags of the last pd_cluster_decide */
     long long tile_bits;    /* live (i-atom, j-half) tile bits of the working list */
+    int mask_entries;       /* outer entries holding an exception pair (exclusion masks) */
+    int outside_pairs;      /* exception pairs computed outside the tiles (counts[CL_NP]) */
 } pd_cluster_stats;
 
 /* ClusterPairEngine(T, N, box; ...) + setup! (Engine.jl:54-97, 130-139).  Copies *p. */
@@ -166,6 +168,28 @@ int pd_cluster_scatter(pd_cluster *c, float *fx, float *fy, float *fz, float *ep
 int pd_cluster_compute(pd_cluster *c, const float *x, const float *y, const float *z,
                        const float *q, const int *type, float *fx, float *fy, float *fz,
                        float *epot, float *vir6, int energy, pd_stream_t s);
+/* Exceptions on the cluster route: Coulomb exclusions and scaled pairs, with optional bond
+ * exclusions of the Lennard-Jones term.  Follows normalize_exceptions (src/electrostatics/Spec.jl:
+ * 200-227), bond_exclusion_rows (src/clusterpairs/Engine.jl:274-290), the exclusion masks of
+ * _exclusion_kernel! (src/clusterpairs/List.jl:634-688), the excluded branch of pair_force
+ * (PairFunctor.jl:127-156) and _scaled_pairs_kernel!, _lj_restore_kernel!, _coulomb_shift_kernel!
+ * (src/clusterpairs/Kernels.jl:244-339).
+ *
+ * (pi[k], pj[k], scale[k]): 0-based storage indices and a finite scale >= 0 (0 = excluded).  A pair
+ * listed twice must carry the same scale; scale 1 is an ordinary pair and is dropped.  The pair's
+ * Coulomb term becomes scale * C qi qj / r: a pair inside the list takes the excluded branch in its
+ * tile (minus the mesh part, which is the whole 1/r beyond the real-space cutoff when the engine has
+ * a mesh) and the scaled term is added outside the tiles; a pair beyond the list adds (scale - 1) *
+ * C qi qj / r outside the tiles.
+ * (bi[k], bj[k]): bonded pairs whose LJ term is dropped (the engine needs an LJ term).  The masks
+ * cover the union: a bonded pair that is no Coulomb exception keeps its full Coulomb term (scale 1
+ * and, energy only, the potential shift of an ordinary pair inside the cutoff); a Coulomb exception
+ * that is not bonded keeps its LJ term.
+ * n = nbond = 0 removes every exception.  Requests a build; captured steps re-capture.  Host
+ * boundary (allocates).  Errors: PD_EINVAL with the reference's messages for out-of-range or
+ * self pairs, negative or non-finite scales and conflicting duplicates. */
+int pd_cluster_set_exceptions(pd_cluster *c, int n, const int *pi, const int *pj, const double *scale,
+                              int nbond, const int *bi, const int *bj);
 /* Allocation-free force evaluation.  This entry point has no counterpart in the reference.
  *
  * It serves callers that cannot call cudaMalloc: a plugin inside a host program whose own memory

@@ -340,6 +340,57 @@ def pme_total(pos, q, box, *, C, alpha, rc, K, P, kind="spme", nmax=2, lj=None, 
     return dict(F=pr["F"] + ms["F"], E=E, Etot=float(E.sum()), W=W, F_pair=pr["F"], F_mesh=ms["F"])
 
 
+def exception_terms(pos, q, box, pairs, *, C, rc, eshift=0.0, bonded=(), lj=None):
+    """Change of the forces, per-particle energies and per-particle virial rows (xx, yy, zz, xy, xz, yz)
+    that exceptions make, in FP64, minimum image.
+
+    pairs: 0-based (i, j, scale).  The pair's Coulomb term becomes scale * C qi qj / r in place of the
+    full 1/r that the real-space sum and the mesh carry together (the excluded branch of pair_force,
+    PairFunctor.jl:127-156, with _scaled_pairs_kernel!, Kernels.jl:307-339): a change of
+    (scale - 1) C qi qj / r, and inside the real-space cutoff the ordinary pair's potential shift
+    -C qi qj eshift goes too.  bonded: pairs whose LJ term is dropped (bond_exclusion_rows,
+    Engine.jl:274-290); lj = dict(c6, c12, rc2, esh).  A bonded pair that is no Coulomb exception keeps
+    its whole Coulomb term, so only its LJ term changes."""
+    R = np.asarray(pos, float)
+    q = np.asarray(q, float)
+    L = np.asarray(box, float)
+    n = len(R)
+    F = np.zeros((n, 3))
+    E = np.zeros(n)
+    W = np.zeros((n, 6))
+
+    def add(i, j, f, e, d):
+        F[i] += f * d
+        F[j] -= f * d
+        E[i] += 0.5 * e
+        E[j] += 0.5 * e
+        w = 0.5 * f * np.array([d[0] * d[0], d[1] * d[1], d[2] * d[2], d[0] * d[1], d[0] * d[2], d[1] * d[2]])
+        W[i] += w
+        W[j] += w
+
+    for i, j, s in pairs:
+        if s == 1.0:
+            continue
+        d = R[i] - R[j]
+        d -= L * np.round(d / L)
+        r2 = float(d @ d)
+        r = math.sqrt(r2)
+        cq = C * q[i] * q[j]
+        e = (s - 1.0) * cq / r + (cq * eshift if r2 < rc * rc else 0.0)
+        add(i, j, (s - 1.0) * cq / (r2 * r), e, d)
+    for i, j in bonded:
+        d = R[i] - R[j]
+        d -= L * np.round(d / L)
+        r2 = float(d @ d)
+        if r2 >= lj["rc2"]:
+            continue
+        ir6 = 1.0 / r2 ** 3
+        f = (12.0 * lj["c12"] * ir6 - 6.0 * lj["c6"]) * ir6 / r2
+        e = (lj["c12"] * ir6 - lj["c6"]) * ir6 - lj["esh"]
+        add(i, j, -f, -e, d)
+    return dict(F=F, E=E, W=W)
+
+
 # ------------------------------------------------------------------ cluster list
 
 def displacement_ratios(pos, ref_build, ref_prune, box, skin, prune_buffer):

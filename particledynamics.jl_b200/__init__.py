@@ -10,8 +10,8 @@ from .engine import (ClusterPairEngine, DeviceEngine, ELLDeviceEngine, ELLEngine
                      ElectrostaticsSpec)
 from .workflow import (  # noqa: F401
     BAOA, BAOAB, ESP, PME, PPPM, WCA, CellList, ClusterPairList, ConstantVolume, Integrator, Langevin, LennardJones,
-    ParticleSystem, Simulation, SimulationState, Stage, VelocityVerlet, electrostatics_spec, evaluate_forces_into_f,
-    run, state, step,
+    ParticleSystem, Simulation, SimulationState, Stage, Topology, VelocityVerlet, electrostatic_exceptions,
+    electrostatics_spec, evaluate_forces_into_f, run, state, step,
 )
 
 __version__ = "0.1.0"

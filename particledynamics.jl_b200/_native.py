@@ -48,6 +48,7 @@ class ClusterStats(C.Structure):
         ("builds", C.c_int), ("prunes", C.c_int), ("nsmax", C.c_int), ("nslot", C.c_int),
         ("last_build", C.c_int), ("last_prune", C.c_int),
         ("tile_bits", C.c_longlong),
+        ("mask_entries", C.c_int), ("outside_pairs", C.c_int),
     ]
 
 
@@ -146,6 +147,7 @@ _SIGS = {
     "pd_cluster_compute_static": (C.c_int, [C.POINTER(ClusterParams), C.POINTER(C.c_double), _fp, _fp, _fp, _fp,
                                             _fp, _fp, _fp, _fp, _fp, _fp, C.c_int, _p]),
     "pd_cluster_status": (C.c_int, [_p, C.POINTER(ClusterStats), _p]),
+    "pd_cluster_set_exceptions": (C.c_int, [_p, C.c_int, _p, _p, _p, C.c_int, _p, _p]),
     "pd_cluster_order": (_fp, [_p]),
     "pd_cluster_buffers": (C.c_int, [_p, C.POINTER(_p), C.POINTER(_p), C.POINTER(_p), C.POINTER(_p),
                                      C.POINTER(_p), C.POINTER(_p)]),

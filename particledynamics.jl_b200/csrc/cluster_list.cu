@@ -563,11 +563,17 @@ __device__ __forceinline__ int face_code(float x, float y, float z, float slx, f
     return c;
 }
 
+// With exceptions (xid != null) a tile that holds an excluded pair is kept whatever its distances
+// (the pair kernel removes that pair's mesh part), the working entry is marked (bit 17) and its mask
+// slot copied to wxid (Kernels.jl:370-373).
 __global__ void __launch_bounds__(256) k_prune(const float4 *__restrict__ xq, const int *__restrict__ perm,
                                                const int *__restrict__ scio, const uint32_t *__restrict__ cjo,
                                                uint2 *__restrict__ cjw, int *__restrict__ nw,
                                                float4 *__restrict__ ref_prune, float Lx, float Ly, float Lz,
-                                               float rp2, float pbuf, int *__restrict__ counts, int gated) {
+                                               float rp2, float pbuf, int *__restrict__ counts, int gated,
+                                               const int *__restrict__ xid,
+                                               const unsigned long long *__restrict__ xmask,
+                                               int *__restrict__ wxid) {
     if (gated && counts[W_PRUNE] == 0) return;
     if (counts[W_ERR] != 0) return;
     const int S = blockIdx.x;
@@ -578,6 +584,7 @@ __global__ void __launch_bounds__(256) k_prune(const float4 *__restrict__ xq, co
     __shared__ float4 s_blo[8], s_bhi[8];   // current i-cluster boxes
     __shared__ uint32_t s_ent[PRUNE_CHUNK];
     __shared__ uint32_t s_res[PRUNE_CHUNK];
+    __shared__ int s_xid[PRUNE_CHUNK];
     __shared__ int s_wtot[8];
     const int t = threadIdx.x;
     const float wlx = __fsub_rn(__fmul_rn(0.5f, Lx), __fmul_rn(0.5f, pbuf));
@@ -634,7 +641,10 @@ __global__ void __launch_bounds__(256) k_prune(const float4 *__restrict__ xq, co
     int nkeep = 0;
     for (int cb = e0; cb < e1; cb += PRUNE_CHUNK) {
         const int nch = min(e1 - cb, PRUNE_CHUNK);
-        for (int k = t; k < nch; k += blockDim.x) s_ent[k] = cjo[cb + k];
+        for (int k = t; k < nch; k += blockDim.x) {
+            s_ent[k] = cjo[cb + k];
+            s_xid[k] = xid ? xid[cb + k] : 0;
+        }
         __syncthreads();
         const int ngroups = (nch + 3) >> 2;
         // loader role: atom (lane & 7) of entry 4 g + (lane >> 3)
@@ -738,7 +748,14 @@ __global__ void __launch_bounds__(256) k_prune(const float4 *__restrict__ xq, co
                     }
                 }
                 bits = __reduce_or_sync(0xffffffffu, bits);
-                if (lane == 0) s_res[k] = bits | (mark ? 0x10000u : 0u);
+                const int x = s_xid[k];
+                if (x > 0 && lane < 8) {   // half tiles of excluded pairs: tj < 4 (low nibbles), tj >= 4
+                    const unsigned long long mk = xmask[(size_t)(x - 1) * 8 + lane];
+                    const uint32_t xb = ((mk & 0x0F0F0F0F0F0F0F0Full) ? (1u << lane) : 0u) |
+                                        ((mk & 0xF0F0F0F0F0F0F0F0ull) ? (0x100u << lane) : 0u);
+                    bits |= __reduce_or_sync(0xffu, xb);
+                }
+                if (lane == 0) s_res[k] = bits | (mark ? 0x10000u : 0u) | (x > 0 ? 0x20000u : 0u);
             }
         }
         __syncthreads();
@@ -757,7 +774,11 @@ __global__ void __launch_bounds__(256) k_prune(const float4 *__restrict__ xq, co
                 off += v < w ? c : 0;
                 tot += c;
             }
-            if (live) cjw[e0 + nkeep + off + __popc(bal & ((1u << lane) - 1u))] = make_uint2(s_ent[k] >> 8, m);
+            if (live) {
+                const int ew = e0 + nkeep + off + __popc(bal & ((1u << lane) - 1u));
+                cjw[ew] = make_uint2(s_ent[k] >> 8, m);
+                if (wxid) wxid[ew] = (m & 0x20000u) ? s_xid[k] : 0;
+            }
             nkeep += tot;
             __syncthreads();
         }
@@ -875,6 +896,8 @@ int cluster_set_word(pd_cluster *c, int word, int value, cudaStream_t s) {
 static void free_entries(pd_cluster *c) {
     dfree(c->cjo);
     dfree(c->cjw);
+    dfree(c->xid);
+    dfree(c->wxid);
 }
 
 static int alloc_entries(pd_cluster *c, int necap) {
@@ -883,7 +906,92 @@ static int alloc_entries(pd_cluster *c, int necap) {
     int rc;
     if ((rc = dalloc(&c->cjo, (size_t)necap))) return rc;
     if ((rc = dalloc(&c->cjw, (size_t)necap))) return rc;
+    if (c->nexc > 0) {   // exclusion slots follow the entry storage
+        if ((rc = dalloc(&c->xid, (size_t)necap)) || (rc = dalloc(&c->wxid, (size_t)necap))) return rc;
+        PD_CUDA(cudaMemset(c->xid, 0, sizeof(int) * (size_t)necap));
+        PD_CUDA(cudaMemset(c->wxid, 0, sizeof(int) * (size_t)necap));
+    }
     return PD_OK;
+}
+
+// ---------------------------------------------------------------- exceptions
+// _exclusion_kernel! (List.jl:629-688) after a build.  An exception pair belongs to the tile of its
+// lower cluster (the lower slot inside one cluster): super-cluster S = ci / 8, i-cluster k = ci % 8.
+// Pass 1 finds the outer entry of S holding cj with bit k set and gives it a mask slot (xid, from 1);
+// pass 2 sets the pair's bit (ti * 8 + tj) in that slot's mask of i-cluster k and records the pairs
+// computed outside the tiles: in-list pairs with a nonzero scale (coef = scale, added to the
+// excluded tile pair's zero) and pairs beyond the list (coef = scale - 1, the mesh holds their 1/r).
+
+__global__ void k_excl_begin(int *__restrict__ xid, const int *__restrict__ scio, int *__restrict__ counts, int gated) {
+    if (gated && counts[W_BUILD] == 0) return;
+    if (counts[W_ERR] != 0) return;   // an overflowed list is rebuilt after growth
+    const int ne = scio[counts[W_NS]];
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ne; e += gridDim.x * blockDim.x) xid[e] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        counts[W_NX] = 0;
+        counts[W_NP] = 0;
+    }
+}
+
+// One warp per particle i takes its exception pairs in turn (the orientation with the lower slot);
+// the warp finds the pair's outer entry (super-cluster S = ci / 8 with j-cluster cj and i-cluster
+// bit k = ci % 8) by scanning S's segment 32 entries at a time.
+template <int PASS>
+__global__ void k_excl_pass(int n, const int *__restrict__ exo, const int *__restrict__ exj,
+                            const float *__restrict__ exs, const int *__restrict__ slot_of,
+                            const int *__restrict__ scio, const uint32_t *__restrict__ cjo, int *__restrict__ xid,
+                            unsigned long long *__restrict__ xmask, int *__restrict__ xpi, int *__restrict__ xpj,
+                            float *__restrict__ xpc, int *__restrict__ counts, int gated) {
+    if (gated && counts[W_BUILD] == 0) return;
+    if (counts[W_ERR] != 0) return;
+    const int lane = threadIdx.x & 31;
+    const int i = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (i >= n) return;   // uniform over the warp
+    const int si = slot_of[i];
+    for (int p = exo[i]; p < exo[i + 1]; ++p) {
+        const int j = exj[p];
+        const int sj = slot_of[j];
+        const int ci = si >> 3, cj = sj >> 3;
+        if (!(ci < cj || (ci == cj && (si & 7) < (sj & 7)))) continue;   // the other orientation
+        const int S = ci >> 3, k = ci & 7;
+        const int b1 = scio[S + 1];
+        int e = -1;
+        for (int b = scio[S]; b < b1 && e < 0; b += 32) {
+            bool hit = false;
+            if (b + lane < b1) {
+                const uint32_t ent = cjo[b + lane];
+                hit = (int)(ent >> 8) == cj && ((ent >> k) & 1u);
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (m) e = b + __ffs(m) - 1;
+        }
+        if (lane == 0) {
+            const float sc = exs[p];
+            if (PASS == 1) {
+                if (e >= 0 && atomicCAS(&xid[e], 0, -1) == 0) xid[e] = atomicAdd(&counts[W_NX], 1) + 1;
+            } else if (e >= 0) {
+                const unsigned long long bit = 1ull << ((si & 7) * 8 + (sj & 7));
+                atomicOr(&xmask[(size_t)(xid[e] - 1) * 8 + k], bit);
+                if (sc != 0.f) {
+                    const int m = atomicAdd(&counts[W_NP], 1);
+                    xpi[m] = i;
+                    xpj[m] = j;
+                    xpc[m] = sc;
+                }
+            } else {
+                const int m = atomicAdd(&counts[W_NP], 1);
+                xpi[m] = i;
+                xpj[m] = j;
+                xpc[m] = sc - 1.f;
+            }
+        }
+    }
+}
+
+__global__ void k_excl_masks_clear(unsigned long long *__restrict__ xmask, int *__restrict__ counts, int gated) {
+    if (gated && counts[W_BUILD] == 0) return;
+    const int m = 8 * counts[W_NX];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) xmask[k] = 0ull;
 }
 
 static void free_geometry(pd_cluster *c) {
@@ -942,6 +1050,19 @@ int cluster_build_launch(pd_cluster *c, const float *x, const float *y, const fl
                                             c->sbc, c->sbh, Lx, Ly, Lz, rl2, c->cnt_sc, c->colcnt, c->ncs, c->scio,
                                             c->cjo, c->counts, g);
     PD_LAUNCHED();
+    if (c->nexc > 0) {
+        const int nb = (int)(((long long)N * 32 + 255) / 256);
+        k_excl_begin<<<2 * c->num_sms, 256, 0, s>>>(c->xid, c->scio, c->counts, g);
+        PD_LAUNCHED();
+        k_excl_pass<1><<<nb, 256, 0, s>>>(N, c->exo, c->exj, c->exs, c->slot_of, c->scio, c->cjo, c->xid, c->xmask,
+                                          c->xpi, c->xpj, c->xpc, c->counts, g);
+        PD_LAUNCHED();
+        k_excl_masks_clear<<<2 * c->num_sms, 256, 0, s>>>(c->xmask, c->counts, g);
+        PD_LAUNCHED();
+        k_excl_pass<2><<<nb, 256, 0, s>>>(N, c->exo, c->exj, c->exs, c->slot_of, c->scio, c->cjo, c->xid, c->xmask,
+                                          c->xpi, c->xpj, c->xpc, c->counts, g);
+        PD_LAUNCHED();
+    }
     return PD_OK;
 }
 
@@ -949,7 +1070,8 @@ int cluster_prune_launch(pd_cluster *c, int conditional, cudaStream_t s) {
     const double rp = c->p.rmax + c->p.prune_buffer;
     const float rp2 = (float)rp * (float)rp;
     k_prune<<<c->nsmax, 256, 0, s>>>(c->xq, c->perm, c->scio, c->cjo, c->cjw, c->nw, c->ref_prune, c->L[0], c->L[1],
-                                     c->L[2], rp2, (float)c->p.prune_buffer, c->counts, conditional ? 1 : 0);
+                                     c->L[2], rp2, (float)c->p.prune_buffer, c->counts, conditional ? 1 : 0,
+                                     c->nexc > 0 ? c->xid : nullptr, c->xmask, c->nexc > 0 ? c->wxid : nullptr);
     PD_LAUNCHED();
     return PD_OK;
 }
@@ -1024,6 +1146,7 @@ void cluster_pair_params(const pd_cluster_params *p, const double box[3], PairPa
     pp->eshift = p->coul_eshift;
     pp->ne = p->coulomb ? p->coul_ne : 1;
     pp->nf = p->coulomb ? p->coul_nf : 1;
+    pp->has_mesh = p->coulomb ? p->coul_has_mesh : 0;
     for (int k = 0; k < PD_MAX_POLY; ++k) {   // coefficients past the fitted length are zero (exact padding)
         pp->pe[k] = k < pp->ne ? p->coul_pe[k] : 0.f;
         pp->pf[k] = k < pp->nf ? p->coul_pf[k] : 0.f;
@@ -1089,6 +1212,7 @@ int pd_cluster_destroy(pd_cluster *c) {
     if (!c) return PD_OK;
     free_geometry(c);
     free_entries(c);
+    cluster_free_exceptions(c);
     dfree(c->counts);
     dfree(c->slot_of);
     dfree(c->order);
@@ -1293,6 +1417,8 @@ int pd_cluster_status(pd_cluster *c, pd_cluster_stats *out, pd_stream_t s) {
         }
         out->working_entries = (int)tot;
         out->tile_bits = bits;
+        out->mask_entries = h[W_NX];
+        out->outside_pairs = h[W_NP];
     }
     return PD_OK;
 }

@@ -29,6 +29,8 @@ enum CountWord {
     W_FLAG_BUILD = 11, // max displacement ratio since the build as float bits
     W_NWORK = 12,    // working entries (sum over super-clusters, diagnostics)
     W_TICKET = 13,   // blocks of the step's kick kernel that have reported (last one decides)
+    W_NX = 14,       // outer entries holding an excluded pair (exceptions)
+    W_NP = 15,       // exception pairs computed outside the tiles (scaled in-list, or out of the list)
     W_LEN = 16
 };
 

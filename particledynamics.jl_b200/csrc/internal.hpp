@@ -70,6 +70,8 @@ struct PairParams {
     int coulomb;
     float C, rc2, sx, eshift;
     int ne, nf;
+    int has_mesh;                 // excluded pairs beyond r_c remove the mesh's full 1/r (coul_has_mesh)
+    int lj_excl;                  // masked pairs also drop their LJ term (bond exclusions)
     float pe[PD_MAX_POLY];
     float pf[PD_MAX_POLY];
 };
@@ -130,6 +132,27 @@ struct pd_cluster {
     float *vc = nullptr;       // 6 nslot
     float4 *ref_build = nullptr, *ref_prune = nullptr;  // N
     float *lj_table = nullptr; // ntypes^2 x 4 (device)
+    // Coulomb exceptions (pd_cluster_set_exceptions): CSR rows by particle (both orientations),
+    // per outer entry its slot in the exclusion masks (0: none), per working entry the same, the
+    // 64-bit pair masks of the flagged entries (8 per entry, one per i-cluster) and the pairs
+    // computed outside the tiles: in-list pairs with a nonzero scale (coef = scale) and pairs
+    // beyond the list (coef = scale - 1)
+    int nexc = 0;              // canonical exception pairs
+    int *exo = nullptr;        // N + 1
+    int *exj = nullptr;        // 2 nexc
+    float *exs = nullptr;      // 2 nexc
+    int *xid = nullptr;        // necap
+    int *wxid = nullptr;       // necap
+    unsigned long long *xmask = nullptr;  // 8 nexc
+    int *xpi = nullptr, *xpj = nullptr;   // nexc
+    float *xpc = nullptr;      // nexc
+    // Bond exclusions (lj_excl): the masks also drop LJ; the corrections restore the LJ term of
+    // masked pairs that are not bonded (lr) and the Coulomb potential shift of bonded pairs that
+    // carry their full Coulomb term (sh, energy only); storage indices
+    int lj_excl = 0;
+    int nlr = 0, nsh = 0;
+    int *lri = nullptr, *lrj = nullptr;
+    int *shi = nullptr, *shj = nullptr;
     pdb::PairParams pp;
 };
 
@@ -182,10 +205,17 @@ int mesh_store_virial(pd_mesh *m, float *vglobal6, cudaStream_t s);
 // Cluster internals used by the step engine.
 int cluster_decide_launch(pd_cluster *c, const float *x, const float *y, const float *z, int fixed, cudaStream_t s);
 int cluster_pairs_launch(pd_cluster *c, int energy, cudaStream_t s);
+// The pair pass of an engine with exceptions (tiles with exclusion masks, then the pairs outside them).
+int cluster_pairs_launch_excl(pd_cluster *c, int energy, cudaStream_t s);
 int cluster_build_launch(pd_cluster *c, const float *x, const float *y, const float *z, const float *q,
                          const int *type, int conditional, cudaStream_t s);
 int cluster_prune_launch(pd_cluster *c, int conditional, cudaStream_t s);
 int cluster_read_counts(pd_cluster *c, int *host, cudaStream_t s);
+// Exception pairs computed outside the tiles and the bond-exclusion corrections, added to the slot
+// accumulators (part of the pair pass: cluster_pairs_launch runs it after the tiles).
+int cluster_exceptions_launch(pd_cluster *c, int energy, cudaStream_t s);
+// Frees an engine's exception buffers.
+void cluster_free_exceptions(pd_cluster *c);
 int cluster_set_word(pd_cluster *c, int word, int value, cudaStream_t s);
 // ELL, network and learned-correction internals used by the learned form and the step engine.
 int ell_capacity(const pd_ell *e);

@@ -174,6 +174,34 @@ class ClusterPairEngine:
         return {"nsplit": best[0], "warps": best[1], "default": [n0, w0],
                 "ms": {f"{k[0]}x{k[1]}": v for k, v in times.items()}}
 
+    def set_exceptions(self, exceptions=(), bonds=()):
+        """Coulomb exceptions and bond exclusions (0-based storage indices).
+
+        ``exceptions``: ``(i, j)`` (excluded) or ``(i, j, scale)`` items, normalised as
+        ``normalize_exceptions`` (Spec.jl:200-227) does; ``bonds``: ``(i, j)`` pairs whose LJ term is
+        dropped, with the corrections of ``bond_exclusion_rows`` (Engine.jl:274-290).  Empty lists
+        remove every exception.  The next evaluation rebuilds the list."""
+        pi, pj, sc = [], [], []
+        for item in exceptions:
+            if len(item) not in (2, 3):
+                raise ValueError("Each electrostatic exception must be (i, j) or (i, j, scale).")
+            pi.append(int(item[0]))
+            pj.append(int(item[1]))
+            sc.append(float(item[2]) if len(item) == 3 else 0.0)
+        bi, bj = [], []
+        for item in bonds:
+            if len(item) != 2:
+                raise ValueError("Each bonded pair must be (i, j).")
+            bi.append(int(item[0]))
+            bj.append(int(item[1]))
+        a = np.array(pi, np.int32)
+        b = np.array(pj, np.int32)
+        s = np.array(sc, np.float64)
+        c = np.array(bi, np.int32)
+        d = np.array(bj, np.int32)
+        N.call("pd_cluster_set_exceptions", self.handle, len(a), a.ctypes.data, b.ctypes.data, s.ctypes.data,
+               len(c), c.ctypes.data, d.ctypes.data)
+
     def grow(self):
         N.call("pd_cluster_grow", self.handle)
 

@@ -169,8 +169,6 @@ def electrostatics_spec(f) -> ElectrostaticsSpec:
         raise ValueError(f"{type(f).__name__} requires coulomb_prefactor and real_cutoff.")
     if f.boundary != "tin_foil":
         raise ValueError(f"Only conducting (tin-foil) boundary conditions are implemented; got {f.boundary}.")
-    if f.exclusions not in ("topology", None, ()) or f.exclude_bonded or len(f.scaled_pairs) > 0:
-        raise NotImplementedError("Coulomb exceptions are not supported by this build of the cluster-pair path.")
     if isinstance(f, ESP):
         return _esp_spec(f)
     if (f.alpha is None) == (f.real_space_tolerance is None):
@@ -237,10 +235,69 @@ class Stage:
     progress: bool = False
 
 
-class ParticleSystem:
-    """Positions (N x D, D = 2 or 3 from the box), box, types, per-type masses and charges (host data)."""
+def _pair_tuples(values, label):
+    """_normalize_pair_tuples (src/workflow/System.jl:39-50): 1-based (i, j) pairs."""
+    out = []
+    for item in values:
+        if len(item) != 2:
+            raise ValueError(f"Each {label} entry must have length 2.")
+        i, j = int(item[0]), int(item[1])
+        if i <= 0 or j <= 0:
+            raise ValueError(f"{label} indices must be positive.")
+        out.append((i, j))
+    return out
 
-    def __init__(self, positions, box, types=("A",), typeids=None, masses=None, charges=None, velocities=None):
+
+@dataclass
+class Topology:
+    """Bonds and exclusions of a system (Topology, src/workflow/System.jl:89-150), 1-based particle ids.
+
+    The nonbonded path uses ``bonds`` (with ``exclude_bonded``) and ``exclusions`` (the default
+    ``exclusions="topology"`` of the electrostatics descriptors); bonded force terms are not part of it."""
+    bonds: list = field(default_factory=list)
+    exclusions: list = field(default_factory=list)
+
+    def __post_init__(self):
+        self.bonds = _pair_tuples(self.bonds, "bond")
+        self.exclusions = _pair_tuples(self.exclusions, "exclusion")
+
+
+def electrostatic_exceptions(system, f) -> list:
+    """Exception list implied by a descriptor's ``exclusions``, ``exclude_bonded`` and ``scaled_pairs``
+    (electrostatic_exceptions, src/workflow/Electrostatics.jl:281-306): sorted 1-based (i, j, scale)."""
+    scales = {}
+
+    def key(i, j):
+        i, j = int(i), int(j)
+        return (i, j) if i < j else (j, i)
+
+    topo = getattr(system, "topology", None) or Topology()
+    excl = f.exclusions
+    if isinstance(excl, str) and excl == "topology":
+        for i, j in topo.exclusions:
+            scales[key(i, j)] = 0.0
+    elif excl is None or (isinstance(excl, str) and excl == "none"):
+        pass
+    else:
+        for item in excl:
+            scales[key(item[0], item[1])] = 0.0
+    if f.exclude_bonded:
+        for i, j in topo.bonds:
+            scales[key(i, j)] = 0.0
+    for item in f.scaled_pairs:
+        if len(item) != 3:
+            raise ValueError("scaled_pairs entries must be (i, j, scale).")
+        scales[key(item[0], item[1])] = float(item[2])
+    return [(k[0], k[1], s) for k, s in sorted(scales.items())]
+
+
+class ParticleSystem:
+    """Positions (N x D, D = 2 or 3 from the box), box, types, per-type masses and charges (host data),
+    and an optional :class:`Topology`."""
+
+    def __init__(self, positions, box, types=("A",), typeids=None, masses=None, charges=None, velocities=None,
+                 topology=None):
+        self.topology = topology if topology is not None else Topology()
         self.box = tuple(float(b) for b in box)
         if len(self.box) not in (2, 3):
             raise ValueError("periodic boxes are 2D or 3D")
@@ -378,6 +435,10 @@ class SimulationState:
         pb = min(pb, skin)
         self.cluster = ClusterPairEngine(self.n, self.box, rmax=rmax, skin=skin, prune_buffer=pb, lj=lj,
                                          coulomb=coul, selfc=selfc)
+        self.exceptions = electrostatic_exceptions(system, elec[0]) if elec else []
+        if self.exceptions:
+            # build-time ids are 1-based; the engine takes storage indices (the same order here)
+            self.cluster.set_exceptions([(i - 1, j - 1, s) for i, j, s in self.exceptions])
         state = dict(x=self.x, y=self.y, z=self.z, vx=self.vx, vy=self.vy, vz=self.vz, fx=self.fx, fy=self.fy,
                      fz=self.fz, q=self.q if coul is not None else None, type=self.typ, inv_mass=self.inv_mass,
                      epot=self.epot, vir6=self.vir6, vglobal=self.vglobal)
