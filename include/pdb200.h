@@ -551,6 +551,94 @@ int pd_batch_step(pd_batch *b, int nsteps, float dt, int use_graph, pd_stream_t 
 int pd_ewald_oracle(int n, const double *rq4, const double box[3], double C, double alpha, double digits, int parts,
                     double *F, double *E);
 
+/* ======================================================================
+ * Snapshot I/O: the GSD file layer (version 2.0) that the reference's trajectory writer and
+ * restart reader drive through GSDFiles.jl (src/io/GSDIO.jl:104-203, 380-615,
+ * src/io/RestartIO.jl:20-511), and a device kernel that packs one frame's per-particle chunks
+ * for a single device-to-host copy.  These calls are host file I/O: they take HOST buffers and
+ * are not stream-ordered (pd_snapshot_pack is the exception).
+ * ====================================================================== */
+typedef struct pd_gsd pd_gsd;
+
+/* GSD type codes (RestartIO.jl:27-39) */
+enum pd_gsd_type {
+    PD_GSD_UINT8 = 1, PD_GSD_UINT16 = 2, PD_GSD_UINT32 = 3, PD_GSD_UINT64 = 4, PD_GSD_INT8 = 5,
+    PD_GSD_INT16 = 6, PD_GSD_INT32 = 7, PD_GSD_INT64 = 8, PD_GSD_FLOAT = 9, PD_GSD_DOUBLE = 10,
+    PD_GSD_CHARACTER = 11
+};
+enum pd_gsd_mode { PD_GSD_CREATE = 0, PD_GSD_APPEND = 1, PD_GSD_READ = 2 };
+
+/* One index entry as stored in the file (32 bytes). */
+typedef struct {
+    uint64_t frame;
+    uint64_t N;
+    int64_t location;
+    uint32_t M;
+    uint16_t id;
+    uint8_t type;
+    uint8_t flags;
+} pd_gsd_index_entry;
+
+/* gsd_open(path; application, schema, schema_version, append) (GSDIO.jl:167-175, 140-165):
+ * PD_GSD_CREATE truncates or creates the file and writes an empty version-2.0 layout;
+ * PD_GSD_APPEND continues an existing file after its last committed frame; PD_GSD_READ reads.
+ * schema_version = (major << 16) | minor (HOOMD schema 1.4: 0x00010004).  An invalid magic or a
+ * truncated file returns PD_EINVAL (the reference's "Invalid GSD magic", GSDIO.jl:113). */
+int pd_gsd_open(const char *path, int mode, const char *application, const char *schema, uint32_t schema_version,
+                pd_gsd **out);
+/* gsd_close(h) (GSDIO.jl:203).  Chunks written after the last pd_gsd_end_frame are dropped. */
+int pd_gsd_close(pd_gsd *h);
+/* write_chunk(name; type, N, M, data) (GSDFiles' write_chunk_raw!, GSDIO.jl:307-310): N x M values
+ * of `type`, row-major, from host memory, into the frame being written.  A name appears at most
+ * once per frame. */
+int pd_gsd_write_chunk(pd_gsd *h, const char *name, int type, uint64_t N, uint32_t M, const void *data);
+/* end_frame!(h) (GSDIO.jl:599): commits the frame (index entries, new names, header). */
+int pd_gsd_end_frame(pd_gsd *h);
+/* sync!(h) (GSDIO.jl:600-610): fsync of the file. */
+int pd_gsd_flush(pd_gsd *h);
+/* nframes(reader) (test/test_io_gsd.jl:90): committed frames. */
+uint64_t pd_gsd_nframes(const pd_gsd *h);
+/* Header fields: file layer and schema versions, application and schema names (64-byte buffers). */
+int pd_gsd_header(const pd_gsd *h, uint32_t *gsd_version, uint32_t *schema_version, char *application,
+                  char *schema);
+/* _maybe_one(r, entries_for_frame(frame), name) (RestartIO.jl:141-149): *found = 1 and the entry
+ * when `frame` holds a chunk `name`, else *found = 0. */
+int pd_gsd_find_chunk(const pd_gsd *h, uint64_t frame, const char *name, pd_gsd_index_entry *out, int *found);
+/* read_chunk(entry) (RestartIO.jl:41-52): the entry's N x M values into a host buffer of `bytes`. */
+int pd_gsd_read_chunk(const pd_gsd *h, const pd_gsd_index_entry *e, void *buf, uint64_t bytes);
+/* _entries_for_frame(r, frame) (RestartIO.jl:141): the frame's entries (up to cap); *count = all. */
+int pd_gsd_frame_entries(const pd_gsd *h, uint64_t frame, pd_gsd_index_entry *out, int cap, int *count);
+/* r.names[id + 1] (RestartIO.jl:227): the name of chunk id into buf (size bytes). */
+int pd_gsd_name(const pd_gsd *h, int id, char *buf, int size);
+
+/* One frame's per-particle device arrays (structure of arrays, build order).  z, vz, fz are NULL
+ * in 2D; velocities, forces, types and virial rows are optional (NULL = chunk absent).  `type`
+ * holds 1-based type ids; `vir` is n x 6 (3D: xx, yy, zz, xy, xz, yz) or n x 3 (2D: xx, yy, xy),
+ * row-major. */
+typedef struct {
+    int n;
+    int dim;
+    const float *x, *y, *z;
+    const float *vx, *vy, *vz;
+    const float *fx, *fy, *fz;
+    const int *type;
+    const float *vir;
+} pd_snapshot_src;
+
+/* Byte offsets of the packed chunks inside the staging buffer (~0 = absent), each 16-byte
+ * aligned: particles/position (float32 n x 3), particles/velocity (n x 3), particles/force
+ * (n x 3), particles/typeid (uint32 n, 0-based), particles/virial (float32 n x virial_columns). */
+typedef struct {
+    uint64_t position, velocity, force, typeid_, virial;
+    int virial_columns;
+    uint64_t bytes;
+} pd_snapshot_offsets;
+int pd_snapshot_layout(const pd_snapshot_src *src, pd_snapshot_offsets *out);
+/* Packs the frame into the device buffer dst (16-byte aligned, dst_bytes >= layout.bytes) on
+ * stream s, in the chunks' on-disk layout (_soa_to_posmat / _soa_to_velmat / _soa_to_frcmat and
+ * the 0-based type ids of GSDIO.jl:228-299, 451-454).  Stream-ordered, allocates nothing. */
+int pd_snapshot_pack(const pd_snapshot_src *src, void *dst, uint64_t dst_bytes, pd_stream_t s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -41,6 +41,23 @@ class ClusterParams(C.Structure):
     ]
 
 
+class GsdIndexEntry(C.Structure):
+    """pd_gsd_index_entry: one 32-byte GSD index entry (include/pdb200.h)."""
+    _fields_ = [("frame", C.c_uint64), ("N", C.c_uint64), ("location", C.c_int64), ("M", C.c_uint32),
+                ("id", C.c_uint16), ("type", C.c_uint8), ("flags", C.c_uint8)]
+
+
+class SnapshotSrc(C.Structure):
+    """pd_snapshot_src: one frame's per-particle device arrays (include/pdb200.h)."""
+    _fields_ = [("n", C.c_int), ("dim", C.c_int)] + [(k, C.c_void_p) for k in (
+        "x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz", "type", "vir")]
+
+
+class SnapshotOffsets(C.Structure):
+    _fields_ = [("position", C.c_uint64), ("velocity", C.c_uint64), ("force", C.c_uint64), ("typeid", C.c_uint64),
+                ("virial", C.c_uint64), ("virial_columns", C.c_int), ("bytes", C.c_uint64)]
+
+
 class ClusterStats(C.Structure):
     _fields_ = [
         ("superclusters", C.c_int), ("outer_entries", C.c_int), ("working_entries", C.c_int),
@@ -221,6 +238,19 @@ _SIGS = {
     "pd_batch_step": (C.c_int, [_p, C.c_int, C.c_float, C.c_int, _p]),
     "pd_ewald_oracle": (C.c_int, [C.c_int, _fp, C.POINTER(C.c_double), C.c_double, C.c_double, C.c_double, C.c_int,
                                   _fp, C.POINTER(C.c_double)]),
+    "pd_gsd_open": (C.c_int, [C.c_char_p, C.c_int, C.c_char_p, C.c_char_p, C.c_uint32, C.POINTER(_p)]),
+    "pd_gsd_close": (C.c_int, [_p]),
+    "pd_gsd_write_chunk": (C.c_int, [_p, C.c_char_p, C.c_int, C.c_uint64, C.c_uint32, _p]),
+    "pd_gsd_end_frame": (C.c_int, [_p]),
+    "pd_gsd_flush": (C.c_int, [_p]),
+    "pd_gsd_nframes": (C.c_uint64, [_p]),
+    "pd_gsd_header": (C.c_int, [_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.c_char_p, C.c_char_p]),
+    "pd_gsd_find_chunk": (C.c_int, [_p, C.c_uint64, C.c_char_p, C.POINTER(GsdIndexEntry), C.POINTER(C.c_int)]),
+    "pd_gsd_read_chunk": (C.c_int, [_p, C.POINTER(GsdIndexEntry), _p, C.c_uint64]),
+    "pd_gsd_frame_entries": (C.c_int, [_p, C.c_uint64, C.POINTER(GsdIndexEntry), C.c_int, C.POINTER(C.c_int)]),
+    "pd_gsd_name": (C.c_int, [_p, C.c_int, C.c_char_p, C.c_int]),
+    "pd_snapshot_layout": (C.c_int, [C.POINTER(SnapshotSrc), C.POINTER(SnapshotOffsets)]),
+    "pd_snapshot_pack": (C.c_int, [C.POINTER(SnapshotSrc), _fp, C.c_uint64, _p]),
 }
 
 EXPORTED = tuple(_SIGS)

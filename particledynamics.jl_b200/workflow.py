@@ -227,6 +227,42 @@ class Integrator:
 
 
 @dataclass
+class GSDWriter:
+    """Scheduled GSD trajectory writer (src/workflow/Writers.jl:50-90): a frame every ``every`` steps
+    (and at the stage start with ``write_start``); ``mode`` "replace" starts a new file, "append" (or
+    ``append=True``) continues an existing one.  ``types`` and ``diameter`` "automatic" take the
+    system's type names and the element covalent diameters.  Frames are packed and copied on the
+    device after their steps and written to the file while the next steps run."""
+    filename: str
+    every: int | None = None
+    schedule: object = None
+    group: object = None
+    write_start: bool = True
+    mode: str = "replace"
+    append: bool = False
+    types: object = "automatic"
+    diameter: object = "automatic"
+    write_unwrapped: bool = False
+    sync_on_write: bool = True
+    write_forces: bool = False
+    write_virial: bool = False
+    observables: list = field(default_factory=list)
+
+    def __post_init__(self):
+        if self.mode not in ("replace", "append"):
+            raise ValueError(f"GSDWriter mode must be replace or append; got {self.mode}")
+        if self.every is not None and int(self.every) <= 0:
+            raise ValueError("GSDWriter every must be positive")
+        if self.schedule is not None:
+            raise NotImplementedError("GSDWriter schedules other than `every` are not part of this build")
+        if self.group is not None:
+            raise NotImplementedError("GSDWriter groups other than the whole system are not part of this build")
+        if self.write_unwrapped:
+            raise ValueError("GSDWriter(write_unwrapped=true) requires unwrapped position buffers, which this "
+                             "build's state does not keep")
+
+
+@dataclass
 class Stage:
     """A run stage (RunLoop.jl): name, steps, and how often energies are evaluated (0 = last step only)."""
     name: str = "run"
@@ -322,6 +358,26 @@ class ParticleSystem:
     @property
     def n(self) -> int:
         return len(self.positions)
+
+    @staticmethod
+    def from_gsd(path, frame: int = -1) -> "ParticleSystem":
+        """ParticleSystem.from_gsd(path; frame=-1) (src/workflow/System.jl:455-531): positions, box, types,
+        type ids, masses, charges, velocities and bonds of a GSD frame (-1 = the last)."""
+        from .gsdio import read_gsd_frame
+
+        fr = read_gsd_frame(path) if frame == -1 else read_gsd_frame(path, step=frame)
+        cols = [fr.rx, fr.ry] + ([fr.rz] if fr.D == 3 else [])
+        vcols = [fr.vx, fr.vy] + ([fr.vz] if fr.D == 3 else [])
+        props = fr.particle_properties
+        bonds = [tuple(int(v) for v in t) for t in fr.topology.bonds["tuples"]] if fr.topology else []
+        system = ParticleSystem(np.stack(cols, 1).astype(float), fr.box, types=fr.types, typeids=fr.typeid,
+                                masses=props.get("mass"), charges=props.get("charge"),
+                                velocities=np.stack(vcols, 1).astype(float), topology=Topology(bonds=bonds))
+        system.metadata = dict(step=fr.step, source_path=str(path), particle_properties=props,
+                               per_type_properties=fr.per_type_properties)
+        if "diameter" in props:
+            system.metadata["diameters"] = props["diameter"]
+        return system
 
 
 # ----------------------------------------------------------------------------- state
@@ -558,7 +614,8 @@ class SimulationState:
 class Simulation:
     """System + integrator on one GPU (the reference's Simulation, src/workflow)."""
 
-    def __init__(self, system: ParticleSystem, integrator: Integrator, precision="f32", seed: int = 0):
+    def __init__(self, system: ParticleSystem, integrator: Integrator, precision="f32", seed: int = 0,
+                 writers=()):
         if precision not in ("f32", np.float32, "Float32"):
             raise ValueError("this build runs the Float32 force path")
         if len(integrator.methods) != 1:
@@ -578,6 +635,54 @@ class Simulation:
         # Langevin under the velocity-Verlet scheme is the Grønbech-Jensen-Farago integrator
         # (the reference's Langevin/GJF `velocityverlet` path, IntegratorSpecs.jl:158)
         self.state.langevin_scheme = "gjf" if vv else ("baoa" if baoa else "baoab")
+        self.writers = list(writers)
+        for w in self.writers:
+            if not isinstance(w, GSDWriter):
+                raise NotImplementedError(f"writer {type(w).__name__} is not part of this build")
+        self._gsd = {}       # writer index -> (GSDFile, FrameStager, pending slot, pending step)
+        self._opened = set()
+
+    def _writer_handle(self, k: int):
+        from .gsdio import FrameStager, gsd_open
+
+        if k not in self._gsd:
+            w = self.writers[k]
+            # a file this simulation has written before is continued by later runs
+            append = w.append or w.mode == "append" or w.filename in self._opened
+            h = gsd_open(w.filename, append=append)
+            self._opened.add(w.filename)
+            stager = FrameStager(self.state, forces=w.write_forces, virial=w.write_virial)
+            self._gsd[k] = [h, stager, None, None]
+        return self._gsd[k]
+
+    def _stage_frame(self, k: int):
+        """Pack and copy the state's frame for writer k on the device; the previous pending frame of the
+        writer is written to its file meanwhile."""
+        rec = self._writer_handle(k)
+        slot = rec[1].stage()
+        self._write_pending(k)
+        rec[2], rec[3] = slot, self.state.step_count
+
+    def _write_pending(self, k: int):
+        from .gsdio import write_gsd_frame
+
+        rec = self._gsd.get(k)
+        if rec is None or rec[2] is None:
+            return
+        w = self.writers[k]
+        h, stager, slot, stp = rec
+        types = self.system.types if w.types == "automatic" else list(w.types)
+        diam = None if w.diameter == "automatic" else w.diameter
+        write_gsd_frame(h, self.state, diameter=diam, types_names=types, step=int(stp),
+                        write_forces=w.write_forces, write_virial=w.write_virial, sync_on_write=w.sync_on_write,
+                        stager=stager, staged=slot, topology=self.system.topology)
+        rec[2] = rec[3] = None
+
+    def close_writers(self):
+        """Write every pending frame and close the writers' files (a later run appends to them)."""
+        for k in list(self._gsd):
+            self._write_pending(k)
+            self._gsd.pop(k)[0].close()
 
 
 def state(sim: Simulation) -> SimulationState:
@@ -585,19 +690,37 @@ def state(sim: Simulation) -> SimulationState:
 
 
 def run(sim: Simulation, stage: Stage) -> Simulation:
-    """run!(sim, stage) (RunLoop.jl:403-457): stage.steps NVE steps on the device."""
+    """run!(sim, stage) (RunLoop.jl:403-457): stage.steps steps on the device, with the writers' frames
+    at the stage start (``write_start``) and every ``every`` steps of the running step count."""
     st = sim.state
-    if stage.steps <= 0:
-        return sim
-    every = stage.energy_every
-    if every and every > 0:
+    writers = getattr(sim, "writers", [])
+    needs_forces = any(w.write_forces or w.write_virial for w in writers)
+    if writers and needs_forces and not st.forces_valid:
+        st.evaluate_forces_into_f(True)
+    for k, w in enumerate(writers):
+        if w.write_start:
+            sim._stage_frame(k)
+    if stage.steps > 0:
+        every = stage.energy_every if stage.energy_every and stage.energy_every > 0 else 0
+        marks = {stage.steps}
+        if every:
+            marks |= set(range(every, stage.steps, every))
+        for w in writers:
+            if w.every:
+                e = int(w.every)
+                first = e - st.step_count % e
+                marks |= set(range(first, stage.steps + 1, e))
         done = 0
-        while done < stage.steps:
-            k = min(every, stage.steps - done)
-            st.step(k, energy_last=True)
-            done += k
-    else:
-        st.step(stage.steps, energy_last=True)
+        base = st.step_count
+        for m in sorted(marks):
+            if m <= done:
+                continue
+            st.step(m - done, energy_last=True)
+            done = m
+            for k, w in enumerate(writers):
+                if w.every and (base + done) % int(w.every) == 0:
+                    sim._stage_frame(k)
+    sim.close_writers()
     st.synchronize()
     return sim
 
