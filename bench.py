@@ -859,77 +859,119 @@ def run_batch_workload(pd, args, world, rank):
                           "clocks": clk.summary()}))
 
 
-def run_melts_workload(pd, args, world, rank):
-    """64 independent charged melts (N log-uniform in [2 000, 32 000] at 0.0375 ions per cubic Angstrom, the
-    64 000-ion melt's LJ and SPME settings with its 1 A mesh, order 5): each system's captured step replayed
-    on one of 16 streams, so that the systems' latency-bound steps overlap, against the same replays one after
-    another on one stream.  The mesh path is not batched into one launch per stage (one cuFFT plan per mesh
-    size); this measures the concurrent replay of the per-system graphs."""
-    import torch
+def melts_sizes(nmelts: int, rank: int = 0):
+    """Sizes of the batched charged melts: N log-uniform in [2 000, 32 000], even (half +1, half -1)."""
     rng = np.random.default_rng(SEED + 64 + rank)
-    ns = [int(round(math.exp(rng.uniform(math.log(2000), math.log(32000))))) for _ in range(args.melts)]
-    ns = [n + (n % 2) for n in ns]   # neutral: half +1, half -1
+    ns = [int(round(math.exp(rng.uniform(math.log(2000), math.log(32000))))) for _ in range(nmelts)]
+    return [n + (n % 2) for n in ns]
+
+
+def melts_measure(pd, ns, steps, warmup, skin, buffer, prune, world=1, compare=True):
+    """The charged melts as one batch (one launch per force stage, the step one captured graph, lanes per row
+    and spread tile by the autotuner), and, with ``compare``, each melt's own captured single-system step
+    replayed concurrently on 16 streams and one after another.  Returns the result dict (ms per step,
+    atom-steps/s)."""
+    import torch
     dt = DT_FS / pd.synthetic.TIME_UNIT_FS
-    states = []
-    for k, n in enumerate(ns):
-        L = (n / RHO) ** (1.0 / 3.0)
-        pos, q, box = pd.synthetic.ionic_melt(n, L, 2.2, seed=SEED + 1000 + k)
-        m = pd.synthetic.melt_masses(q)
-        v = pd.synthetic.maxwell_boltzmann(m, T_INIT, seed=SEED + 2000 + k, kB=pd.synthetic.KB_EV)
-        system = pd.ParticleSystem(pos, box, types=["Na", "Cl"], typeids=np.where(q > 0, 1, 2), masses=m,
-                                   charges=q, velocities=v)
-        st = pd.Simulation(system, pd.Integrator(dt=dt, forces=forces(pd, args.buffer, args.prune))).state
-        st.evaluate_forces_into_f(False)
-        states.append(st)
     total = sum(ns)
+    systems = pd.batch.melt_systems(ns, rho=RHO, T=T_INIT, seed=SEED)
+    alpha = pd.splits.alpha_from_tolerance(RC, 1e-5)
+    el = dict(alpha=alpha, C=pd.synthetic.COULOMB_EV_A, rc=RC, order=5, kind="spme", spacing=1.0)
+    batch = pd.batch.BatchedReplicas(systems, skin=skin, electrostatics=el)
+    batch.evaluate()
+    tuned = batch.autotune(dt)
+    batch.step(warmup, dt)
+    torch.cuda.synchronize()
+    s0 = batch.stream
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(s0)
+    batch.step(steps, dt)
+    t1.record(s0)
+    torch.cuda.synchronize()
+    st = batch.status()
+    if st["error"]:
+        raise RuntimeError(f"batched melts: list error {st['error']}")
+    ms_batch = max_over_ranks(world, t0.elapsed_time(t1) / steps)
+    info = batch.mesh_info()
+    out = {"metric": "atom-steps/s", "value": world * total * 1000.0 / ms_batch, "unit": "atom-steps/s",
+           "ms_per_step": ms_batch, "steps": steps, "warmup": warmup,
+           "workload": f"{len(ns)} charged melts, N log-uniform [2000, 32000] (total {total}), 0.0375 A^-3, "
+                       f"LJ + SPME 1 A order 5, NVE 1 fs",
+           "path": "batched: one launch per force stage, one captured graph per step",
+           "skin": skin, "fft_plans": info["groups"], "mesh_nodes": info["nodes"], "list_builds": st["builds"],
+           "autotune": tuned, "l2": "inputs larger than L2 (rows and grids)"}
+    del batch
+    torch.cuda.empty_cache()
+    if not compare:
+        return out
+    states = []
+    for sysd in systems:
+        system = pd.ParticleSystem(sysd["positions"], sysd["box"], types=["Na", "Cl"],
+                                   typeids=np.where(sysd["charges"] > 0, 1, 2), masses=sysd["masses"],
+                                   charges=sysd["charges"], velocities=sysd["velocities"])
+        sst = pd.Simulation(system, pd.Integrator(dt=dt, forces=forces(pd, buffer, prune))).state
+        sst.evaluate_forces_into_f(False)
+        states.append(sst)
     nstream = 16
     streams = [torch.cuda.Stream() for _ in range(nstream)]
 
-    def replay(steps, concurrent):
+    def replay(nsteps, concurrent):
         # system k always replays on stream k % 16 (its captured graph is bound to that stream); the
         # sequential replay chains the systems with events, the concurrent one lets them overlap
         prev = None
-        for _ in range(steps):
-            for k, st in enumerate(states):
+        for _ in range(nsteps):
+            for k, sst in enumerate(states):
                 s = streams[k % nstream]
                 if not concurrent and prev is not None:
                     s.wait_event(prev)
-                st.engine.step(1, dt, energy_last=False, use_graph=True, stream=s)
+                sst.engine.step(1, dt, energy_last=False, use_graph=True, stream=s)
                 if not concurrent:
                     prev = torch.cuda.Event()
                     prev.record(s)
 
-    replay(args.warmup, True)
+    replay(warmup, True)
     torch.cuda.synchronize()
-    out = {}
     for conc in (False, True):
-        t0 = torch.cuda.Event(enable_timing=True)
-        t1 = torch.cuda.Event(enable_timing=True)
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
-        t0.record(streams[0])
+        a.record(streams[0])
         for s in streams[1:]:
-            s.wait_event(t0)
-        replay(args.steps, conc)
+            s.wait_event(a)
+        replay(steps, conc)
         for s in streams[1:]:
             ev = torch.cuda.Event()
             ev.record(s)
             streams[0].wait_event(ev)
-        t1.record(streams[0])
+        b.record(streams[0])
         torch.cuda.synchronize()
-        ms = max_over_ranks(world, t0.elapsed_time(t1) / args.steps)
-        out["concurrent" if conc else "sequential"] = {"ms_per_step": ms, "value": world * total * 1000.0 / ms}
-    for st in states:
-        if st.cluster.statistics()["error"]:
+        ms = max_over_ranks(world, a.elapsed_time(b) / steps)
+        key = "concurrent_replay" if conc else "sequential_replay"
+        out[key] = {"ms_per_step": ms, "value": world * total * 1000.0 / ms,
+                    "path": ("each melt's captured single-system step, 16 streams" if conc
+                             else "each melt's captured single-system step, one after another")}
+    for sst in states:
+        if sst.cluster.statistics()["error"]:
             raise RuntimeError("cluster list error during the melts run")
+    out["batched_vs_sequential"] = out["sequential_replay"]["ms_per_step"] / ms_batch
+    out["batched_vs_concurrent"] = out["concurrent_replay"]["ms_per_step"] / ms_batch
+    return out
+
+
+def run_melts_workload(pd, args, world, rank):
+    """64 independent charged melts (the 64 000-ion melt's density, LJ and SPME settings, 1 A mesh, order 5)
+    as one batch, against each melt's own captured step replayed concurrently and one after another."""
+    ns = melts_sizes(args.melts, rank)
+    res = melts_measure(pd, ns, args.steps, args.warmup, args.melt_skin, args.buffer, args.prune, world=world,
+                        compare=not args.no_compare)
     if rank == 0:
-        print(json.dumps({"metric": "atom-steps/s", "value": out["concurrent"]["value"], "unit": "atom-steps/s",
-                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-                          "ms_per_step": out["concurrent"]["ms_per_step"], "higher_is_better": True,
-                          "scaling": "weak", "dtype": "f32", "data": "synthetic",
-                          "config": {"workload": f"{args.melts} charged melts, N log-uniform [2000, 32000] "
-                                                 f"(total {total}), 0.0375 A^-3, LJ + SPME 1 A order 5, NVE 1 fs",
-                                     "parallelism": f"replicas x{world}", "streams": nstream},
-                          "sequential_replay": out["sequential"]}))
+        line = {"metric": res.pop("metric"), "value": res.pop("value"), "unit": res.pop("unit"), "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": res.pop("ms_per_step"),
+                "higher_is_better": True, "scaling": "weak", "dtype": "f32", "data": "synthetic",
+                "config": {"workload": res.pop("workload"), "parallelism": f"replicas x{world}"}}
+        line.update(res)
+        print(json.dumps(line))
 
 
 def run_reference(args, world, rank):
@@ -980,6 +1022,9 @@ def main():
     ap.add_argument("--prune", type=float, default=PRUNE, help="prune buffer (Angstrom)")
     ap.add_argument("--replicas", type=int, default=512, help="replicas of the batch512 workload")
     ap.add_argument("--melts", type=int, default=64, help="charged melts of the melts64 workload")
+    ap.add_argument("--melt-skin", type=float, default=1.0, help="row-list skin of the batched melts (Angstrom)")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="melts64: time the batched path only (no single-system replays), e.g. for a launch list")
     ap.add_argument("--workload", default="melt64k",
                     choices=["melt64k", "melt512k", "lj1m", "wca2d1m", "lj4k", "batch512", "melts64"],
                     help="melt64k: the headline run; melt512k: the same forms at 512 000 ions (L = 239 A); lj4k / "
@@ -1174,7 +1219,9 @@ def main():
         configs = {"config0_lj4k": ell_config(pd, "lj4k", 200, args.warmup, peaks),
                    "config1a_lj1m": ell_config(pd, "lj1m", 30, args.warmup, peaks),
                    "config1b_wca2d1m": ell_config(pd, "wca2d1m", 30, args.warmup, peaks),
-                   "config4_batch512": batch_config(pd, 30, args.warmup, peaks)}
+                   "config4_batch512": batch_config(pd, 30, args.warmup, peaks),
+                   "config4_melts64": melts_measure(pd, melts_sizes(64), 20, args.warmup, 1.0, args.buffer,
+                                                    args.prune)}
         for c in configs.values():
             c["value"] = world * c["value"]
     cpu = None

@@ -537,6 +537,31 @@ int pd_batch_status(pd_batch *b, pd_ell_stats *out);
  * t * n + k, entries are cell-order positions), their lengths (n, by position) and the cell order
  * (n particle indices). */
 int pd_batch_rows(pd_batch *b, int **rows, int **counts, int **order);
+
+/* Charged replicas (the batched ionic melts): every replica's real-space Coulomb term is the
+ * cluster route's fitted polynomial of the Gaussian split (pair_force, PairFunctor.jl:127-156:
+ * f/r = C qq (r^-3 - P_f(x)), e = C qq (1/r + P_e(x) - eshift), x = r^2 sx - 1, inside rc2), and
+ * selfc = 2 alpha / sqrt(pi) gives the per-particle self energy -C selfc q^2 / 2.  The charges come
+ * from the bound state (pd_md_state.q).  rc2 must lie inside the list radius of the batch. */
+typedef struct {
+    float C, rc2, sx, eshift;
+    int ne, nf;                     /* coefficients (<= 16 each), constant term first */
+    float pe[PD_MAX_POLY], pf[PD_MAX_POLY];
+    float selfc;
+} pd_batch_coulomb;
+int pd_batch_set_coulomb(pd_batch *b, const pd_batch_coulomb *c);
+/* One SPME or P3M-AD mesh per replica (meshes: nrep x (K1, K2, K3), the replica's own box at the
+ * shared spacing), B-spline order 4..6, with its FP64 influence function from the single-system
+ * setup (compute_influence!, Influence.jl:190-227).  The replicas' meshes are transformed by one
+ * batched cuFFT plan per mesh size; spread, influence multiply and gather are one launch each over
+ * all replicas.  Neutral replicas only (net_charge = :error).  Host boundary: allocates. */
+int pd_batch_set_mesh(pd_batch *b, int kind, int order, double alpha, double C, const int *meshes);
+/* Spread tile of the batched meshes, the autotuner's choice: 32 or 64 particles (cell-order
+ * neighbours of one replica) per spread / gather CTA.  Host boundary: may reallocate. */
+int pd_batch_set_spread_tile(pd_batch *b, int chunk);
+/* Batched-mesh sizes: FFT plan groups (mesh sizes), grid nodes and modes of all replicas, the tile
+ * size and the number of tiles. */
+int pd_batch_mesh_info(pd_batch *b, int *groups, long long *nodes, long long *modes, int *chunk, int *nchunk);
 /* Step state (x, v, f, per-particle inverse masses, optional epot) of all replicas, concatenated. */
 int pd_batch_bind(pd_batch *b, const pd_md_state *st);
 int pd_batch_evaluate(pd_batch *b, int energy, pd_stream_t st);

@@ -20,7 +20,7 @@ ROOT = HERE.parent
 # the mesh's gather and spread variants are spread over several units so that they compile in parallel
 SOURCES = ["mesh_gather_ad.cu", "mesh_gather_ik.cu", "mesh_gather_esp.cu", "mesh_gather_ad_join.cu",
            "mesh_gather_ik_join.cu", "mesh_gather_esp_join.cu", "mesh_spread.cu", "cluster_pairs.cu", "cluster_pairs_excl.cu", "ell.cu",
-           "batch.cu", "mesh.cu", "cluster_list.cu", "md.cu", "noalloc.cu", "mlp.cu", "learned.cu", "ewald.cu",
+           "batch.cu", "batch_mesh.cu", "mesh.cu", "cluster_list.cu", "md.cu", "noalloc.cu", "mlp.cu", "learned.cu", "ewald.cu",
            "gsd.cpp", "snapshot.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -132,6 +132,16 @@ class BatchReplica(C.Structure):
     ]
 
 
+class BatchCoulomb(C.Structure):
+    """pd_batch_coulomb: the real-space Coulomb polynomial of charged replicas (include/pdb200.h)."""
+    _fields_ = [
+        ("C", C.c_float), ("rc2", C.c_float), ("sx", C.c_float), ("eshift", C.c_float),
+        ("ne", C.c_int), ("nf", C.c_int),
+        ("pe", C.c_float * PD_MAX_POLY), ("pf", C.c_float * PD_MAX_POLY),
+        ("selfc", C.c_float),
+    ]
+
+
 class LearnedParams(C.Structure):
     _fields_ = [
         ("rcut", C.c_float), ("skin", C.c_float), ("cap", C.c_int),
@@ -236,6 +246,11 @@ _SIGS = {
     "pd_batch_bind": (C.c_int, [_p, C.POINTER(MDState)]),
     "pd_batch_evaluate": (C.c_int, [_p, C.c_int, _p]),
     "pd_batch_step": (C.c_int, [_p, C.c_int, C.c_float, C.c_int, _p]),
+    "pd_batch_set_coulomb": (C.c_int, [_p, C.POINTER(BatchCoulomb)]),
+    "pd_batch_set_mesh": (C.c_int, [_p, C.c_int, C.c_int, C.c_double, C.c_double, C.POINTER(C.c_int)]),
+    "pd_batch_set_spread_tile": (C.c_int, [_p, C.c_int]),
+    "pd_batch_mesh_info": (C.c_int, [_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                                     C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "pd_ewald_oracle": (C.c_int, [C.c_int, _fp, C.POINTER(C.c_double), C.c_double, C.c_double, C.c_double, C.c_int,
                                   _fp, C.POINTER(C.c_double)]),
     "pd_gsd_open": (C.c_int, [C.c_char_p, C.c_int, C.c_char_p, C.c_char_p, C.c_uint32, C.POINTER(_p)]),

@@ -1,10 +1,13 @@
-"""Batched replicas: host side of ``batch.cu``.
+"""Batched replicas: host side of ``batch.cu`` and ``batch_mesh.cu``.
 
 Hundreds of independent 3D LJ / WCA systems of uneven size run as one device batch: their
 particles are concatenated, every stage of the NVE step is one launch over all replicas and the
-step is captured into one CUDA graph.  ``autotune_lanes`` picks the pair kernel's lanes per row by
-timing the candidates on the batch itself.  The reference steps one system per engine; looping
-the single-system ELL engines (``ELLDeviceEngine``) is the comparison.
+step is captured into one CUDA graph.  Charged replicas (ionic melts) add the real-space Coulomb
+polynomial to the pair kernel and one SPME / P3M-AD mesh per replica, spread, multiplied and
+gathered in one launch each over all replicas, transformed by one batched cuFFT plan per mesh size.
+``autotune_lanes`` picks the pair kernel's lanes per row, ``autotune`` the lanes per row and the
+spread tile of charged batches, by timing the candidates on the batch itself.  The reference steps
+one system per engine; looping the single-system engines is the comparison.
 """
 from __future__ import annotations
 
@@ -14,7 +17,7 @@ import numpy as np
 import torch
 
 from . import _native as N
-from . import synthetic
+from . import splits, synthetic
 from .engine import WCA_RC2_FACTOR, _destroy, _ptr, _stream
 
 LJ_RC = 2.5
@@ -39,18 +42,23 @@ def replica_params(kind: str, box, n: int, eps: float = 1.0, sigma: float = 1.0,
 class BatchedReplicas:
     """Device batch of replicas (``pd_batch``) with its concatenated step state."""
 
-    def __init__(self, systems, *, skin: float = 0.3, cap: int | None = None, lanes: int = 4, device="cuda"):
+    def __init__(self, systems, *, skin: float = 0.3, cap: int | None = None, lanes: int = 4, device="cuda",
+                 electrostatics: dict | None = None):
         """``systems``: list of dicts with n, box, kind, positions (n, 3) centred, velocities (n, 3),
-        masses (n,) or a float.  ``cap`` (row capacity) defaults to 1.4x the mean row length at the
-        densest replica, plus 16."""
+        masses (n,) or a float, and optionally eps, sigma, rc (default 1, 1, 2.5) and charges (n,).
+        ``cap`` (row capacity) defaults to 1.4x the mean row length at the densest replica, plus 16.
+        ``electrostatics`` (charged replicas): dict with alpha, C, rc (real-space cutoff), order,
+        kind ("spme" or "p3m_ad") and spacing (mesh spacing; each replica's mesh follows its box)."""
         self.systems = systems
+        rcut = max(float(s.get("rc", LJ_RC)) for s in systems)
         if cap is None:
-            rl = LJ_RC + skin
+            rl = rcut + skin
             rho = max(s["n"] / float(np.prod(s["box"])) for s in systems)
             cap = int(1.4 * rho * 4.18879 * rl ** 3) + 16
         reps = (N.BatchReplica * len(systems))()
         for k, s in enumerate(systems):
-            reps[k] = replica_params(s["kind"], s["box"], s["n"])
+            reps[k] = replica_params(s["kind"], s["box"], s["n"], eps=s.get("eps", 1.0), sigma=s.get("sigma", 1.0),
+                                     rc=s.get("rc", LJ_RC))
         h = C.c_void_p()
         N.call("pd_batch_create", C.byref(h), reps, len(systems), float(skin), int(cap), int(lanes))
         self.cap = int(cap)
@@ -68,14 +76,58 @@ class BatchedReplicas:
         self.fx, self.fy, self.fz = (torch.zeros(self.n, **f32) for _ in range(3))
         self.epot = torch.zeros(self.n, **f32)
         self.inv_mass = torch.tensor(1.0 / mass, **f32)
+        charged = any("charges" in s for s in systems)
+        self.q = (torch.tensor(np.concatenate([np.asarray(s.get("charges", np.zeros(s["n"])), float) for s in systems]),
+                               **f32) if charged else None)
         st = N.MDState()
         st.n = self.n
-        for k in ("x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz", "epot", "inv_mass"):
+        for k in ("x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz", "epot", "inv_mass", "q"):
             setattr(st, k, _ptr(getattr(self, k)))
         self._state = st
         N.call("pd_batch_bind", h, C.byref(st))
         self.lanes = int(lanes)
         self.stream = torch.cuda.Stream(device=device)
+        self.electrostatics = None
+        self.spread_tile = 64
+        if electrostatics is not None:
+            self._set_electrostatics(electrostatics)
+
+    def _set_electrostatics(self, el: dict):
+        """Real-space Coulomb polynomial (the cluster route's fit) and one mesh per replica."""
+        if self.q is None:
+            raise ValueError("electrostatics needs per-particle charges in the systems")
+        for k, s in enumerate(self.systems):
+            qt = float(np.sum(s["charges"]))
+            if abs(qt) > 1e-8 * max(1.0, float(np.abs(s["charges"]).sum())):
+                raise ValueError(f"replica {k} has net charge {qt}; batched meshes take neutral replicas")
+        alpha, Cc, rc = float(el["alpha"]), float(el["C"]), float(el["rc"])
+        order = int(el.get("order", 5))
+        kind = {"spme": N.PD_MESH_SPME, "p3m_ad": N.PD_MESH_P3M_AD}[el.get("kind", "spme")]
+        poly = splits.coulomb_polynomial(alpha, Cc, rc, eshift=0.0)
+        c = N.BatchCoulomb()
+        c.C, c.rc2, c.sx, c.eshift = poly.C, poly.rc2, poly.sx, poly.eshift
+        c.ne, c.nf = len(poly.pe), len(poly.pf)
+        for k, v in enumerate(poly.pe):
+            c.pe[k] = float(v)
+        for k, v in enumerate(poly.pf):
+            c.pf[k] = float(v)
+        c.selfc = 2.0 * alpha / np.sqrt(np.pi)
+        N.call("pd_batch_set_coulomb", self.handle, C.byref(c))
+        meshes = [splits.resolve_mesh(el.get("mesh"), el.get("spacing"), s["box"], order) for s in self.systems]
+        arr = (C.c_int * (3 * len(meshes)))(*[int(v) for m in meshes for v in m])
+        N.call("pd_batch_set_mesh", self.handle, kind, order, alpha, Cc, arr)
+        self.meshes = meshes
+        self.electrostatics = dict(el, order=order, meshes=meshes)
+
+    def set_spread_tile(self, tile: int):
+        N.call("pd_batch_set_spread_tile", self.handle, int(tile))
+        self.spread_tile = int(tile)
+
+    def mesh_info(self) -> dict:
+        g, ch, nc = C.c_int(), C.c_int(), C.c_int()
+        nn, nm = C.c_longlong(), C.c_longlong()
+        N.call("pd_batch_mesh_info", self.handle, C.byref(g), C.byref(nn), C.byref(nm), C.byref(ch), C.byref(nc))
+        return dict(groups=g.value, nodes=nn.value, modes=nm.value, tile=ch.value, tiles=nc.value)
 
     def close(self, _destroy=_destroy):
         if getattr(self, "handle", None):
@@ -132,6 +184,38 @@ class BatchedReplicas:
         return {"lanes": best, "ms": times}
 
 
+    def autotune(self, dt: float, lanes=(1, 2, 4, 8), tiles=(32, 64), steps: int = 10) -> dict:
+        """Time the captured step for every (lanes per row, spread tile) pair on this batch and keep the
+        fastest (the step's pair pass and mesh branch overlap, so whole steps are timed).  The state is
+        restored afterwards."""
+        saved = [t.clone() for t in (self.x, self.y, self.z, self.vx, self.vy, self.vz, self.fx, self.fy, self.fz)]
+        s = self.stream
+        times = {}
+        for g in lanes:
+            for tile in (tiles if self.electrostatics is not None else (self.spread_tile,)):
+                self.set_lanes(g)
+                if self.electrostatics is not None:
+                    self.set_spread_tile(tile)
+                self.step(2, dt)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                with torch.cuda.stream(s):
+                    a.record(s)
+                    self.step(steps, dt)
+                    b.record(s)
+                b.synchronize()
+                times[(g, tile)] = a.elapsed_time(b) / steps
+        best = min(times, key=times.get)
+        self.set_lanes(best[0])
+        if self.electrostatics is not None:
+            self.set_spread_tile(best[1])
+        torch.cuda.synchronize()
+        for t, v in zip((self.x, self.y, self.z, self.vx, self.vy, self.vz, self.fx, self.fy, self.fz), saved):
+            t.copy_(v)
+        torch.cuda.synchronize()
+        self.evaluate()
+        return {"lanes": best[0], "spread_tile": best[1], "ms": {f"{k[0]}x{k[1]}": v for k, v in times.items()}}
+
+
 def make_systems(specs, mass: float = 1.0):
     """Positions (fcc fill at the replica's density) and Maxwell-Boltzmann velocities for replica specs
     (``synthetic.replica_set``)."""
@@ -141,6 +225,23 @@ def make_systems(specs, mass: float = 1.0):
         vel = synthetic.maxwell_boltzmann(np.full(sp["n"], mass), sp["T"], seed=sp["seed"] + 1)
         out.append(dict(n=sp["n"], box=box, kind=sp["kind"], positions=pos, velocities=vel, masses=mass,
                         T=sp["T"], rho=sp["rho"]))
+    return out
+
+
+def melt_systems(ns, rho: float = 0.0375, T: float = 1200.0, seed: int = 0, min_sep: float = 2.2):
+    """Charged melts of the given sizes (half +1, half -1) at number density rho, seeded rejection
+    placement with min_sep, Na/Cl masses, Maxwell-Boltzmann velocities at T (eV units, A/fs scaled by
+    the synthetic module's time unit), LJ eps 0.01 eV, sigma 2.8 A, r_c 9 A; positions centred."""
+    out = []
+    for k, n in enumerate(ns):
+        L = (n / rho) ** (1.0 / 3.0)
+        pos, q, box = synthetic.ionic_melt(int(n), L, min_sep, seed=seed + 1000 + k)
+        Lb = np.asarray(box, float)
+        pos = pos - Lb * np.floor(pos / Lb + 0.5)   # centred image
+        m = synthetic.melt_masses(q)
+        v = synthetic.maxwell_boltzmann(m, T, seed=seed + 2000 + k, kB=synthetic.KB_EV)
+        out.append(dict(n=int(n), box=box, kind="lj", positions=pos, velocities=v, masses=m, charges=q, eps=0.01,
+                        sigma=2.8, rc=9.0))
     return out
 
 

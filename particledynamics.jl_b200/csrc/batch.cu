@@ -21,6 +21,11 @@
 // Rows live in cell order (slot t of the particle at position k of the cell order at t * N + k,
 // entries are cell-order positions), so row stores and loads are contiguous per warp and the
 // neighbours' packed records of a row sit in nearby cells.
+//
+// Charged replicas (the batched ionic melts) add the real-space Coulomb polynomial to the pair kernel
+// and a mesh per replica (batch_mesh.cu): the step's force pass packs coordinates and charges once,
+// runs the pair kernel while the mesh branch (spread, batched transforms per mesh size, influence
+// multiply) runs on a second stream, and the gather joins both and applies the closing half kick.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -28,6 +33,10 @@
 #include "common.cuh"
 #include "ell_common.cuh"
 #include "internal.hpp"
+
+#include <algorithm>
+#include <numeric>
+#include <tuple>
 
 using namespace pdb;
 
@@ -302,10 +311,21 @@ struct BatchKick {
     int on;
 };
 
+// Real-space Coulomb of charged replicas, shared by every replica (one split and cutoff): the
+// cluster route's fitted polynomial (pair_force, PairFunctor.jl:127-156), f/r = C qq (r^-3 - P_f(x)),
+// e = C qq (1/r + P_e(x) - eshift), x = r^2 sx - 1, inside rc2.  Monomial coefficients, constant term
+// first, zero above the fitted degree.
+constexpr int BATCH_NP = 16;
+struct BatchCoul {
+    float C, rc2, sx, eshift;
+    float pf[BATCH_NP], pe[BATCH_NP];
+};
+
 // Row pair kernel over all replicas: the model of particle i's replica (LJ or WCA, the ELL route's
 // UniformLJ / UniformWCA arithmetic), forces stored, optional energy (half of each pair), the
 // closing half kick fused.  The packed coordinates are refreshed by the pack of the same stage.
-template <int G, bool ENERGY>
+// COUL: the packed records carry the charges (xq.w) and the pair adds the Coulomb polynomial term.
+template <int G, bool ENERGY, bool COUL>
 __global__ void __launch_bounds__(B_THREADS) k_batch_pairs(const float4 *__restrict__ xq, int n,
                                                            const int *__restrict__ rows,
                                                            const int *__restrict__ counts,
@@ -314,7 +334,8 @@ __global__ void __launch_bounds__(B_THREADS) k_batch_pairs(const float4 *__restr
                                                            const BatchRep *__restrict__ reps, float *__restrict__ fx,
                                                            float *__restrict__ fy, float *__restrict__ fz,
                                                            float *__restrict__ epot, BatchKick kick,
-                                                           long long *__restrict__ st, int advance) {
+                                                           long long *__restrict__ st, int advance,
+                                                           const __grid_constant__ BatchCoul cp) {
     if (st[E_VALID] == 0) return;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = tid / G, lane = tid % G;   // position in cell order
@@ -328,6 +349,7 @@ __global__ void __launch_bounds__(B_THREADS) k_batch_pairs(const float4 *__restr
         const float eoff = R.kind == PD_PAIR_WCA ? R.eps : -R.eshift;
         const float4 pi = xq[k];
         const int cnt = counts[k];
+        const float cqi = COUL ? cp.C * pi.w : 0.f;
         auto pair = [&](float4 pj) {
             const float dx = periodic_delta(pi.x, pj.x, hLx, Lx);
             const float dy = periodic_delta(pi.y, pj.y, hLy, Ly);
@@ -343,6 +365,25 @@ __global__ void __launch_bounds__(B_THREADS) k_batch_pairs(const float4 *__restr
                 a[1] += fr * dy;
                 a[2] += fr * dz;
                 if (ENERGY) e += 0.5f * (4.f * eps * (s12 - s6) + eoff);
+            }
+            if (COUL && r2 > 0.f && r2 < cp.rc2) {
+                const float rinv = rsqrtf(r2);
+                const float rinv2 = rinv * rinv;
+                const float x = fmaf(r2, cp.sx, -1.f);
+                float pf = cp.pf[BATCH_NP - 1];
+#pragma unroll
+                for (int t = BATCH_NP - 2; t >= 0; --t) pf = fmaf(pf, x, cp.pf[t]);
+                const float cq = cqi * pj.w;
+                const float fq = cq * (rinv * rinv2 - pf);
+                a[0] = fmaf(fq, dx, a[0]);
+                a[1] = fmaf(fq, dy, a[1]);
+                a[2] = fmaf(fq, dz, a[2]);
+                if (ENERGY) {
+                    float pe = cp.pe[BATCH_NP - 1];
+#pragma unroll
+                    for (int t = BATCH_NP - 2; t >= 0; --t) pe = fmaf(pe, x, cp.pe[t]);
+                    e = fmaf(0.5f * cq, rinv + pe - cp.eshift, e);
+                }
             }
         };
         int slot = lane;
@@ -399,13 +440,68 @@ struct pd_batch {
     float exec_dt = 0.f;
     int exec_lanes = 0;
     cudaStream_t exec_stream = nullptr;
+    int exec_chunk = 0;
+    std::vector<double> box;          // 3 per replica, as given
+    // charged replicas: real-space Coulomb and the batched meshes
+    bool coul = false;
+    BatchCoul cp{};
+    float half_c_self = 0.f;
+    bool mesh = false;
+    int morder = 5, mchunk = 64, nchunk = 0;
+    std::vector<BMeshRep> hmreps;
+    BMeshRep *mreps = nullptr;
+    int *chunk_rep = nullptr, *slot_src = nullptr, *mid = nullptr;
+    float4 *mq = nullptr;
+    float *gridA = nullptr, *gridB = nullptr, *G = nullptr;
+    float2 *spec = nullptr;
+    long long total_nodes = 0, total_modes = 0;
+    struct FftGroup {
+        int K1, K2, K3, count;
+        long long grid, modes;
+        cufftHandle fwd, bwd;
+    };
+    std::vector<FftGroup> groups;
+    void *fft_work = nullptr;
+    cudaStream_t mesh_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 namespace pdb {
 
+static void batch_free_chunks(pd_batch *b) {
+    dfree(b->chunk_rep);
+    dfree(b->slot_src);
+    dfree(b->mid);
+    dfree(b->mq);
+    b->nchunk = 0;
+}
+
+static void batch_free_mesh(pd_batch *b) {
+    for (auto &g : b->groups) {
+        if (g.fwd) cufftDestroy(g.fwd);
+        if (g.bwd) cufftDestroy(g.bwd);
+    }
+    b->groups.clear();
+    batch_free_chunks(b);
+    dfree(b->mreps);
+    dfree(b->gridA);
+    dfree(b->gridB);
+    dfree(b->G);
+    dfree(b->spec);
+    if (b->fft_work) cudaFree(b->fft_work);
+    b->fft_work = nullptr;
+    if (b->mesh_stream) cudaStreamDestroy(b->mesh_stream);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
+    b->mesh_stream = nullptr;
+    b->ev_fork = b->ev_join = nullptr;
+    b->mesh = false;
+}
+
 static void batch_free(pd_batch *b) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     b->exec = nullptr;
+    batch_free_mesh(b);
     if (b->body) cudaStreamDestroy(b->body);
     b->body = nullptr;
     dfree(b->reps);
@@ -442,22 +538,20 @@ static int batch_rebuild_launch(pd_batch *b, const float *x, const float *y, con
     return PD_OK;
 }
 
-static int batch_pairs_launch(pd_batch *b, const float *x, const float *y, const float *z, float *fx, float *fy,
-                              float *fz, float *epot, int energy, BatchKick kick, int advance, cudaStream_t s) {
-    k_batch_pack<<<(b->n + B_THREADS - 1) / B_THREADS, B_THREADS, 0, s>>>(x, y, z, b->sorted, b->n, b->xq,
-                                                                          b->st);
-    PD_LAUNCHED();
+template <bool COUL>
+static void launch_batch_pairs(pd_batch *b, float *fx, float *fy, float *fz, float *epot, int energy,
+                               const BatchKick &kick, int advance, cudaStream_t s) {
     const int G = b->lanes;
     const int blocks = (int)(((long long)b->n * G + B_THREADS - 1) / B_THREADS);
 #define PD_BP(GG)                                                                                                      \
     if (energy)                                                                                                        \
-        k_batch_pairs<GG, true><<<blocks, B_THREADS, 0, s>>>(b->xq, b->n, b->rows, b->counts, b->sorted, b->rep_of, \
-                                                              b->reps, fx, \
-                                                              fy, fz, epot, kick, b->st, advance);                     \
+        k_batch_pairs<GG, true, COUL><<<blocks, B_THREADS, 0, s>>>(b->xq, b->n, b->rows, b->counts, b->sorted,       \
+                                                                    b->rep_of, b->reps, fx, fy, fz, epot, kick, b->st, \
+                                                                    advance, b->cp);                                   \
     else                                                                                                               \
-        k_batch_pairs<GG, false><<<blocks, B_THREADS, 0, s>>>(b->xq, b->n, b->rows, b->counts, b->sorted, b->rep_of, \
-                                                               b->reps, fx, \
-                                                               fy, fz, epot, kick, b->st, advance);
+        k_batch_pairs<GG, false, COUL><<<blocks, B_THREADS, 0, s>>>(b->xq, b->n, b->rows, b->counts, b->sorted,      \
+                                                                     b->rep_of, b->reps, fx, fy, fz, epot, kick,       \
+                                                                     b->st, advance, b->cp);
     switch (G) {
         case 1: PD_BP(1) break;
         case 2: PD_BP(2) break;
@@ -465,8 +559,85 @@ static int batch_pairs_launch(pd_batch *b, const float *x, const float *y, const
         default: PD_BP(8) break;
     }
 #undef PD_BP
-    PD_LAUNCHED();
+}
+
+static BMeshView batch_mesh_view(const pd_batch *b) {
+    BMeshView v;
+    v.order = b->morder;
+    v.chunk = b->mchunk;
+    v.nchunk = b->nchunk;
+    v.nrep = b->nrep;
+    v.reps = b->mreps;
+    v.chunk_rep = b->chunk_rep;
+    v.slot_src = b->slot_src;
+    v.mq = b->mq;
+    v.mid = b->mid;
+    v.gridA = b->gridA;
+    v.gridB = b->gridB;
+    v.spec = b->spec;
+    v.G = b->G;
+    v.total_nodes = b->total_nodes;
+    v.total_modes = b->total_modes;
+    return v;
+}
+
+// The mesh branch of charged replicas: spread, the batched forward transforms (one per mesh size),
+// the influence multiply, the batched inverse transforms.
+static int batch_mesh_transform(pd_batch *b, cudaStream_t s) {
+    const BMeshView v = batch_mesh_view(b);
+    int rc;
+    if ((rc = bmesh_spread_launch(v, b->st, s))) return rc;
+    for (auto &g : b->groups) {
+        PD_CHECK(cufftSetStream(g.fwd, s) == CUFFT_SUCCESS, PD_ECUFFT, "batched mesh: cufftSetStream failed");
+        PD_CHECK(cufftExecR2C(g.fwd, b->gridA + g.grid, reinterpret_cast<cufftComplex *>(b->spec + g.modes)) ==
+                     CUFFT_SUCCESS,
+                 PD_ECUFFT, "batched mesh: forward transform failed");
+    }
+    if ((rc = bmesh_solve_launch(v, b->st, s))) return rc;
+    for (auto &g : b->groups) {
+        PD_CHECK(cufftSetStream(g.bwd, s) == CUFFT_SUCCESS, PD_ECUFFT, "batched mesh: cufftSetStream failed");
+        PD_CHECK(cufftExecC2R(g.bwd, reinterpret_cast<cufftComplex *>(b->spec + g.modes), b->gridB + g.grid) ==
+                     CUFFT_SUCCESS,
+                 PD_ECUFFT, "batched mesh: inverse transform failed");
+    }
     return PD_OK;
+}
+
+// The force pass: pack, then the row pair kernel; with charges and meshes the pair kernel runs on s
+// while the mesh branch runs on the batch's mesh stream (forked and joined by events, so the same
+// code is captured into the step graph), and the gather joins both and applies the closing kick.
+static int batch_pairs_launch(pd_batch *b, const float *x, const float *y, const float *z, float *fx, float *fy,
+                              float *fz, float *epot, int energy, BatchKick kick, int advance, cudaStream_t s) {
+    if (!b->coul) {
+        k_batch_pack<<<(b->n + B_THREADS - 1) / B_THREADS, B_THREADS, 0, s>>>(x, y, z, b->sorted, b->n, b->xq,
+                                                                              b->st);
+        PD_LAUNCHED();
+        launch_batch_pairs<false>(b, fx, fy, fz, epot, energy, kick, advance, s);
+        PD_LAUNCHED();
+        return PD_OK;
+    }
+    PD_CHECK(b->mesh && b->bound && b->state.q, PD_ESTATE,
+             "charged replicas need their meshes (pd_batch_set_mesh) and a bound state with charges");
+    const BMeshView v = batch_mesh_view(b);
+    int rc;
+    if ((rc = bmesh_pack_launch(v, x, y, z, b->state.q, b->sorted, b->xq, b->st, s))) return rc;
+    PD_CUDA(cudaEventRecord(b->ev_fork, s));
+    PD_CUDA(cudaStreamWaitEvent(b->mesh_stream, b->ev_fork, 0));
+    if ((rc = batch_mesh_transform(b, b->mesh_stream))) return rc;
+    PD_CUDA(cudaEventRecord(b->ev_join, b->mesh_stream));
+    BatchKick nokick = kick;
+    nokick.on = 0;
+    launch_batch_pairs<true>(b, fx, fy, fz, epot, energy, nokick, advance, s);
+    PD_LAUNCHED();
+    PD_CUDA(cudaStreamWaitEvent(s, b->ev_join, 0));
+    BMeshKick mk;
+    mk.vx = kick.vx;
+    mk.vy = kick.vy;
+    mk.vz = kick.vz;
+    mk.inv_mass = kick.inv_mass;
+    mk.half_dt = kick.half_dt;
+    mk.on = kick.on;
+    return bmesh_gather_launch(v, fx, fy, fz, epot, energy, mk, b->half_c_self, b->st, s);
 }
 
 static int batch_enqueue_step(pd_batch *b, float dt, cudaStream_t s, int cond) {
@@ -560,6 +731,7 @@ int pd_batch_create(pd_batch **out, const pd_batch_replica *reps, int nrep, floa
         h.rc2 = R.rc2;
         h.eshift = R.eshift;
         b->hreps.push_back(h);
+        b->box.insert(b->box.end(), R.box, R.box + 3);
         b->first.push_back(b->n);
         b->n += R.n;
         const int nc = ng[0] * ng[1] * ng[2];
@@ -696,7 +868,8 @@ int pd_batch_step(pd_batch *b, int nsteps, float dt, int use_graph, pd_stream_t 
             if (rc) return rc;
             continue;
         }
-        if (!b->exec || b->exec_dt != dt || b->exec_stream != s || b->exec_lanes != b->lanes) {
+        if (!b->exec || b->exec_dt != dt || b->exec_stream != s || b->exec_lanes != b->lanes ||
+            b->exec_chunk != b->mchunk) {
             if (b->exec) {
                 cudaGraphExecDestroy(b->exec);
                 b->exec = nullptr;
@@ -722,9 +895,218 @@ int pd_batch_step(pd_batch *b, int nsteps, float dt, int use_graph, pd_stream_t 
             b->exec_dt = dt;
             b->exec_stream = s;
             b->exec_lanes = b->lanes;
+            b->exec_chunk = b->mchunk;
         }
         PD_CUDA(cudaGraphLaunch(b->exec, s));
     }
+    return PD_OK;
+}
+
+int pd_batch_set_coulomb(pd_batch *b, const pd_batch_coulomb *c) {
+    PD_CHECK(b && c, PD_EINVAL, "pd_batch_set_coulomb: null argument");
+    PD_CHECK(std::isfinite(c->C) && c->C > 0.f && c->rc2 > 0.f && std::isfinite(c->sx) && std::isfinite(c->selfc),
+             PD_EINVAL, "pd_batch_set_coulomb: C, rc2, sx and selfc must be finite and C, rc2 positive");
+    PD_CHECK(c->ne >= 1 && c->nf >= 1 && c->ne <= BATCH_NP && c->nf <= BATCH_NP, PD_EINVAL,
+             "pd_batch_set_coulomb: the polynomials hold 1..%d coefficients", BATCH_NP);
+    PD_CHECK(c->rc2 <= b->rl2, PD_EINVAL, "pd_batch_set_coulomb: the Coulomb cutoff exceeds the list radius %g "
+             "(create the batch with a van der Waals cutoff covering it)", std::sqrt((double)b->rl2));
+    BatchCoul cp{};
+    cp.C = c->C;
+    cp.rc2 = c->rc2;
+    cp.sx = c->sx;
+    cp.eshift = c->eshift;
+    for (int k = 0; k < c->nf; ++k) cp.pf[k] = c->pf[k];
+    for (int k = 0; k < c->ne; ++k) cp.pe[k] = c->pe[k];
+    b->cp = cp;
+    b->half_c_self = 0.5f * c->C * c->selfc;
+    b->coul = true;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+    return PD_OK;
+}
+
+// Tiles of the batched meshes: replica r's cell-order positions are [first_r, first_r + N_r) (its
+// cells are contiguous in the global cell order), cut into tiles of `chunk` positions; the last
+// tile of a replica is padded (slot_src = -1).
+static int batch_layout_chunks(pd_batch *b, int chunk) {
+    batch_free_chunks(b);
+    std::vector<int> crep, src;
+    for (int r = 0; r < b->nrep; ++r) {
+        const int first = b->first[(size_t)r];
+        const int nr = (r + 1 < b->nrep ? b->first[(size_t)r + 1] : b->n) - first;
+        const int nc = (nr + chunk - 1) / chunk;
+        for (int c = 0; c < nc; ++c) {
+            crep.push_back(r);
+            for (int p = 0; p < chunk; ++p) {
+                const int k = c * chunk + p;
+                src.push_back(k < nr ? first + k : -1);
+            }
+        }
+    }
+    b->nchunk = (int)crep.size();
+    int rc;
+    if ((rc = dalloc(&b->chunk_rep, crep.size())) || (rc = dalloc(&b->slot_src, src.size())) ||
+        (rc = dalloc(&b->mid, src.size())) || (rc = dalloc(&b->mq, src.size())))
+        return rc;
+    PD_CUDA(cudaMemcpy(b->chunk_rep, crep.data(), sizeof(int) * crep.size(), cudaMemcpyHostToDevice));
+    PD_CUDA(cudaMemcpy(b->slot_src, src.data(), sizeof(int) * src.size(), cudaMemcpyHostToDevice));
+    PD_CUDA(cudaMemset(b->mid, 0xff, sizeof(int) * src.size()));
+    PD_CUDA(cudaMemset(b->mq, 0, sizeof(float4) * src.size()));
+    b->mchunk = chunk;
+    return PD_OK;
+}
+
+static int batch_set_mesh(pd_batch *b, int kind, int order, double alpha, double C, const int *meshes) {
+    const int nrep = b->nrep;
+    std::vector<int> idx((size_t)nrep);
+    std::iota(idx.begin(), idx.end(), 0);
+    auto key = [&](int r) { return std::make_tuple(meshes[3 * r + 2], meshes[3 * r + 1], meshes[3 * r]); };
+    std::stable_sort(idx.begin(), idx.end(), [&](int a, int c) { return key(a) < key(c); });
+    b->hmreps.assign((size_t)nrep, BMeshRep{});
+    long long grid = 0, modes = 0;
+    for (size_t a = 0; a < idx.size();) {
+        size_t e = a;
+        while (e < idx.size() && key(idx[e]) == key(idx[a])) ++e;
+        const int r0 = idx[a];
+        pd_batch::FftGroup g{};
+        g.K1 = meshes[3 * r0];
+        g.K2 = meshes[3 * r0 + 1];
+        g.K3 = meshes[3 * r0 + 2];
+        g.count = (int)(e - a);
+        grid = (grid + 63) & ~63ll;     // each group starts on a 256-byte boundary
+        modes = (modes + 31) & ~31ll;
+        g.grid = grid;
+        g.modes = modes;
+        const int K1h = g.K1 / 2 + 1;
+        const long long nn = (long long)g.K1 * g.K2 * g.K3, nm = (long long)K1h * g.K2 * g.K3;
+        for (size_t j = a; j < e; ++j) {
+            const int r = idx[j];
+            BMeshRep &R = b->hmreps[(size_t)r];
+            R.K1 = g.K1;
+            R.K2 = g.K2;
+            R.K3 = g.K3;
+            R.K1h = K1h;
+            R.Lx = b->hreps[(size_t)r].L[0];
+            R.Ly = b->hreps[(size_t)r].L[1];
+            R.Lz = b->hreps[(size_t)r].L[2];
+            R.nmodes = (int)nm;
+            R.grid = grid;
+            R.modes = modes;
+            grid += nn;
+            modes += nm;
+        }
+        g.fwd = g.bwd = 0;
+        b->groups.push_back(g);
+        a = e;
+    }
+    b->total_nodes = grid;
+    b->total_modes = modes;
+    PD_CHECK(2 * modes >= grid, PD_EINVAL, "batched mesh: the modes do not cover the grids");
+    int rc;
+    if ((rc = dalloc(&b->gridA, (size_t)grid)) || (rc = dalloc(&b->gridB, (size_t)grid)) ||
+        (rc = dalloc(&b->spec, (size_t)modes)) || (rc = dalloc(&b->G, (size_t)modes)) ||
+        (rc = dalloc(&b->mreps, (size_t)nrep)))
+        return rc;
+    PD_CUDA(cudaMemset(b->gridA, 0, sizeof(float) * (size_t)grid));
+    PD_CUDA(cudaMemset(b->gridB, 0, sizeof(float) * (size_t)grid));
+    PD_CUDA(cudaMemset(b->spec, 0, sizeof(float2) * (size_t)modes));
+    PD_CUDA(cudaMemset(b->G, 0, sizeof(float) * (size_t)modes));
+    PD_CUDA(cudaMemcpy(b->mreps, b->hmreps.data(), sizeof(BMeshRep) * nrep, cudaMemcpyHostToDevice));
+    // every replica's influence function from the single-system mesh setup (FP64, Influence.jl)
+    for (int r = 0; r < nrep; ++r) {
+        const BMeshRep &R = b->hmreps[(size_t)r];
+        pd_mesh_params mp;
+        memset(&mp, 0, sizeof mp);
+        mp.kind = kind;
+        mp.order = order;
+        mp.alias_order = 2;
+        mp.mesh[0] = R.K1;
+        mp.mesh[1] = R.K2;
+        mp.mesh[2] = R.K3;
+        mp.alpha = alpha;
+        mp.C = C;
+        const int first = b->first[(size_t)r];
+        mp.nmax = std::max(1, (r + 1 < nrep ? b->first[(size_t)r + 1] : b->n) - first);
+        pd_mesh *m = nullptr;
+        if ((rc = pd_mesh_create(&m, &mp, &b->box[3 * (size_t)r]))) return rc;
+        cudaError_t err = cudaDeviceSynchronize();
+        if (err == cudaSuccess)
+            err = cudaMemcpy(b->G + R.modes, m->G, sizeof(float) * (size_t)R.nmodes, cudaMemcpyDeviceToDevice);
+        pd_mesh_destroy(m);
+        PD_CHECK(err == cudaSuccess, PD_ECUDA, "batched mesh: influence copy failed: %s", cudaGetErrorString(err));
+    }
+    size_t wmax = 0;
+    for (auto &g : b->groups) {
+        int n[3] = {g.K3, g.K2, g.K1};
+        const int K1h = g.K1 / 2 + 1;
+        const int nn = g.K1 * g.K2 * g.K3, nm = K1h * g.K2 * g.K3;
+        size_t w1 = 0, w2 = 0;
+        PD_CHECK(cufftCreate(&g.fwd) == CUFFT_SUCCESS && cufftCreate(&g.bwd) == CUFFT_SUCCESS, PD_ECUFFT,
+                 "batched mesh: cufftCreate failed");
+        PD_CHECK(cufftSetAutoAllocation(g.fwd, 0) == CUFFT_SUCCESS && cufftSetAutoAllocation(g.bwd, 0) == CUFFT_SUCCESS,
+                 PD_ECUFFT, "batched mesh: cufftSetAutoAllocation failed");
+        PD_CHECK(cufftMakePlanMany(g.fwd, 3, n, nullptr, 1, nn, nullptr, 1, nm, CUFFT_R2C, g.count, &w1) ==
+                         CUFFT_SUCCESS &&
+                     cufftMakePlanMany(g.bwd, 3, n, nullptr, 1, nm, nullptr, 1, nn, CUFFT_C2R, g.count, &w2) ==
+                         CUFFT_SUCCESS,
+                 PD_ECUFFT, "batched mesh: plan of %d meshes %dx%dx%d failed", g.count, g.K1, g.K2, g.K3);
+        wmax = std::max(wmax, std::max(w1, w2));
+    }
+    if (wmax > 0) {
+        PD_CUDA(cudaMalloc(&b->fft_work, wmax));
+        for (auto &g : b->groups)
+            PD_CHECK(cufftSetWorkArea(g.fwd, b->fft_work) == CUFFT_SUCCESS &&
+                         cufftSetWorkArea(g.bwd, b->fft_work) == CUFFT_SUCCESS,
+                     PD_ECUFFT, "batched mesh: cufftSetWorkArea failed");
+    }
+    PD_CUDA(cudaStreamCreateWithFlags(&b->mesh_stream, cudaStreamNonBlocking));
+    PD_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+    PD_CUDA(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
+    if ((rc = batch_layout_chunks(b, b->mchunk))) return rc;
+    b->morder = order;
+    b->mesh = true;
+    return PD_OK;
+}
+
+int pd_batch_set_mesh(pd_batch *b, int kind, int order, double alpha, double C, const int *meshes) {
+    PD_CHECK(b && meshes, PD_EINVAL, "pd_batch_set_mesh: null argument");
+    PD_CHECK(b->coul, PD_ESTATE, "pd_batch_set_mesh: set the real-space Coulomb terms first (pd_batch_set_coulomb)");
+    PD_CHECK(kind == PD_MESH_SPME || kind == PD_MESH_P3M_AD, PD_ENOTSUP,
+             "pd_batch_set_mesh: batched meshes take SPME or P3M-AD (analytic differentiation)");
+    PD_CHECK(order >= 4 && order <= 6, PD_ENOTSUP, "pd_batch_set_mesh: batched meshes take orders 4, 5 and 6");
+    PD_CHECK(std::isfinite(alpha) && alpha > 0 && std::isfinite(C) && C > 0, PD_EINVAL,
+             "pd_batch_set_mesh: alpha and C must be finite and positive");
+    for (int r = 0; r < b->nrep; ++r)
+        for (int d = 0; d < 3; ++d)
+            PD_CHECK(meshes[3 * r + d] >= order && meshes[3 * r + d] <= 1024, PD_EINVAL,
+                     "pd_batch_set_mesh: replica %d mesh dimension %d is %d (order %d .. 1024)", r, d,
+                     meshes[3 * r + d], order);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+    batch_free_mesh(b);
+    const int rc = batch_set_mesh(b, kind, order, alpha, C, meshes);
+    if (rc != PD_OK) batch_free_mesh(b);
+    return rc;
+}
+
+int pd_batch_set_spread_tile(pd_batch *b, int chunk) {
+    PD_CHECK(b, PD_EINVAL, "pd_batch_set_spread_tile: null handle");
+    PD_CHECK(chunk == 32 || chunk == 64, PD_EINVAL, "pd_batch_set_spread_tile: 32 or 64 particles per tile");
+    if (!b->mesh) {
+        b->mchunk = chunk;
+        return PD_OK;
+    }
+    if (chunk == b->mchunk) return PD_OK;
+    return batch_layout_chunks(b, chunk);
+}
+
+int pd_batch_mesh_info(pd_batch *b, int *groups, long long *nodes, long long *modes, int *chunk, int *nchunk) {
+    PD_CHECK(b, PD_EINVAL, "pd_batch_mesh_info: null handle");
+    if (groups) *groups = (int)b->groups.size();
+    if (nodes) *nodes = b->total_nodes;
+    if (modes) *modes = b->total_modes;
+    if (chunk) *chunk = b->mchunk;
+    if (nchunk) *nchunk = b->nchunk;
     return PD_OK;
 }
 

@@ -228,6 +228,51 @@ const float4 *learned_radial(const pd_learned *h);
 int ell_sort_cells_launch(const int *cell_of, int n, int ncell, int *cell_count, int *cell_off, int *sorted, int *tmp,
                           long long *st, cudaStream_t s);
 
+// Batched meshes of charged replicas (batch_mesh.cu).  Replica r's real grids start at float
+// `grid` of the concatenated grids and its half spectrum (and influence function) at complex mode
+// `modes`; replicas of one mesh size are adjacent, so one batched cuFFT plan transforms them all.
+struct BMeshRep {
+    int K1, K2, K3, K1h;
+    float Lx, Ly, Lz;
+    int nmodes;
+    long long grid;
+    long long modes;
+};
+
+// What the batched mesh kernels read and write.  Particles are processed in chunks of `chunk`
+// consecutive cell-order positions of one replica (padded slots: slot_src = -1).
+struct BMeshView {
+    int order, chunk, nchunk, nrep;
+    const BMeshRep *reps;
+    const int *chunk_rep;        // nchunk
+    const int *slot_src;         // nchunk * chunk: cell-order position or -1
+    float4 *mq;                  // nchunk * chunk: (x, y, z, q) of the slot's particle
+    int *mid;                    // nchunk * chunk: particle index or -1
+    float *gridA, *gridB;        // charge grids (zero between steps), potential grids
+    float2 *spec;
+    const float *G;
+    long long total_nodes, total_modes;
+};
+
+struct BMeshKick {
+    float *vx, *vy, *vz;
+    const float *inv_mass;
+    float half_dt;
+    int on;
+};
+
+// Pack the step's coordinates and charges: xq (cell order, for the pair kernel) and the padded
+// chunk slots of the mesh.  Skipped while the rows are invalid (st[E_VALID] == 0).
+int bmesh_pack_launch(const BMeshView &v, const float *x, const float *y, const float *z, const float *q,
+                      const int *sorted, float4 *xq, const long long *st, cudaStream_t s);
+int bmesh_spread_launch(const BMeshView &v, const long long *st, cudaStream_t s);
+// spec *= G over every replica's modes; clears the charge grids for the next spread.
+int bmesh_solve_launch(const BMeshView &v, const long long *st, cudaStream_t s);
+// AD gather joined with the pair forces already stored in f: f += mesh force, the closing half kick
+// when kick.on, and with energy epot += q phi / 2 - half_c_self q^2.
+int bmesh_gather_launch(const BMeshView &v, float *fx, float *fy, float *fz, float *epot, int energy,
+                        const BMeshKick &kick, float half_c_self, const long long *st, cudaStream_t s);
+
 // Append an IF node on handle h to the graph being captured on s, capture body(cs) into its body
 // graph on the helper stream cs, and continue s after the node.
 template <typename F>

@@ -161,7 +161,8 @@ struct Brick {
 
 constexpr int ROWS_MAX = 512;   // brick rows tabulated in shared memory
 
-template <int P>
+// NT: threads of the CTA that moves the brick (two per particle of the chunk).
+template <int P, int NT = MESH_THREADS>
 __device__ __forceinline__ void chunk_brick(bool valid, int k1, int k2, int k3, int K1, int K2, int K3, int &d1,
                                             int &d2, int &d3, Brick &b, int *sm /* >= 10 ints */,
                                             unsigned *rowbase) {
@@ -210,7 +211,7 @@ __device__ __forceinline__ void chunk_brick(bool valid, int k1, int k2, int k3, 
         b.e2 = sm[8] - sm[5] + P;
         b.e3 = sm[9] - sm[6] + P;
         const long long nodes = (long long)b.e1 * b.e2 * b.e3;
-        b.fits = nodes <= TILE_MAX && b.e1 <= MESH_THREADS && (!b.vec || b.e1 <= K1) &&
+        b.fits = nodes <= TILE_MAX && b.e1 <= NT && (!b.vec || b.e1 <= K1) &&
                  (long long)b.e2 * b.e3 <= ROWS_MAX;
         if (valid) {
             d1 += shift - sm[4];
@@ -236,12 +237,12 @@ __device__ __forceinline__ void chunk_brick(bool valid, int k1, int k2, int k3, 
 // (row, x vector) with MESH_THREADS / nv rows in flight, nv = vectors (or nodes)
 // per row; visit(tile_element, global_node) gets the first node of each
 // 4-node vector (vec) or single node.
-template <typename F>
+template <int NT = MESH_THREADS, typename F>
 __device__ __forceinline__ void for_brick(const Brick &b, const unsigned *rowbase, int K1, F &&visit) {
     const int per = b.vec ? 4 : 1;
     const int nv = b.e1 / per;
     if (nv == 0) return;
-    const int rpi = MESH_THREADS / nv;
+    const int rpi = NT / nv;
     const int t = threadIdx.x;
     const int r0 = t / nv, v = t - r0 * nv;
     if (r0 >= rpi) return;
@@ -250,22 +251,18 @@ __device__ __forceinline__ void for_brick(const Brick &b, const unsigned *rowbas
     for (int r = r0; r < nrows; r += rpi) visit(r * nv + v, (size_t)rowbase[r] + x0);
 }
 
-// Spread of chunks of packed (x, y, z, q) particles (the charge assignment of
-// _spread_lines_kernel!, MeshKernels.jl:247-276).  nchunk_dev (optional) holds
-// the number of active chunks (the cluster list's super-cluster count).
-template <int P, int WIN>
-__global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_spread(const float4 *__restrict__ xq, int nchunks,
-                                                         const int *__restrict__ nchunk_dev, float *__restrict__ grid,
-                                                         int K1, int K2, int K3, float Lx, float Ly, float Lz,
-                                                         WindowPoly wp) {
-    const int c = blockIdx.x;
-    if (nchunk_dev && c >= *nchunk_dev) return;
-    if (c >= nchunks) return;
+// Spread of one chunk of CH packed (x, y, z, q) particles into `grid` (the charge assignment of
+// _spread_lines_kernel!, MeshKernels.jl:247-276), by a CTA of 2 CH threads: each particle's two
+// threads take the two halves of its z stencil.
+template <int P, int WIN, int CH>
+__device__ __forceinline__ void spread_chunk(const float4 *__restrict__ chunk, float *__restrict__ grid, int K1,
+                                             int K2, int K3, float Lx, float Ly, float Lz, const WindowPoly &wp) {
+    constexpr int NT = 2 * CH;
     __shared__ __align__(16) float tile[TILE_MAX];
     __shared__ unsigned rowbase[ROWS_MAX];
     __shared__ int sm[10];
-    const int t = threadIdx.x, p = t & (MESH_CHUNK - 1), h = t >> 6;
-    const float4 v = xq[c * MESH_CHUNK + p];
+    const int t = threadIdx.x, p = t & (CH - 1), h = t / CH;
+    const float4 v = chunk[p];
     const bool valid = v.w != 0.f && isfinite(v.x) && isfinite(v.y) && isfinite(v.z);
     float w1[P], w2[P], w3[P];
     int k1 = 0, k2 = 0, k3 = 0;
@@ -277,7 +274,7 @@ __global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_spread(const
     int d1 = 0, d2 = 0, d3 = 0;
     Brick b;
     // both halves of a particle take part (their min/max contributions are identical)
-    chunk_brick<P>(valid, k1, k2, k3, K1, K2, K3, d1, d2, d3, b, sm, rowbase);
+    chunk_brick<P, NT>(valid, k1, k2, k3, K1, K2, K3, d1, d2, d3, b, sm, rowbase);
     constexpr int PH = (P + 1) / 2;
 
     if (b.fits) {
@@ -286,7 +283,7 @@ __global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_spread(const
         // on the order of its atomics.  The window weights lie in [0, 1], so no node of the brick
         // exceeds the chunk's sum of |q| in magnitude; the scale is the largest power of two that
         // keeps that sum below 2^30.  Each contribution rounds to a step of at most sum|q| / 2^30.
-        __shared__ float s_qabs[MESH_THREADS / 32];
+        __shared__ float s_qabs[NT / 32];
         float qa = (valid && h == 0) ? fabsf(v.w) : 0.f;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) qa += __shfl_xor_sync(0xffffffffu, qa, off);
@@ -294,9 +291,12 @@ __global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_spread(const
         const int nb4 = (b.e1 * b.e2 * b.e3 + 3) >> 2;
         int4 *itile4 = reinterpret_cast<int4 *>(tile);
         int *itile = reinterpret_cast<int *>(tile);
-        for (int k = t; k < nb4; k += MESH_THREADS) itile4[k] = make_int4(0, 0, 0, 0);
+        for (int k = t; k < nb4; k += NT) itile4[k] = make_int4(0, 0, 0, 0);
         __syncthreads();
-        const float qsum = fmaxf(s_qabs[0] + s_qabs[1] + s_qabs[2] + s_qabs[3], 1e-30f);
+        float qsum = 0.f;
+#pragma unroll
+        for (int k = 0; k < NT / 32; ++k) qsum += s_qabs[k];
+        qsum = fmaxf(qsum, 1e-30f);
         const int ex = min(30 - (int)ceilf(log2f(qsum)), 126);   // qsum * 2^ex <= 2^30, 2^ex finite
         const float scale = ldexpf(1.f, ex), inv_scale = ldexpf(1.f, -ex);
         if (valid) {
@@ -316,14 +316,14 @@ __global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_spread(const
         }
         __syncthreads();
         if (b.vec) {
-            for_brick(b, rowbase, K1, [&](int kt, size_t kg) {
+            for_brick<NT>(b, rowbase, K1, [&](int kt, size_t kg) {
                 const int4 iv = itile4[kt];
                 if (iv.x != 0 || iv.y != 0 || iv.z != 0 || iv.w != 0)
                     red_add_v4(grid + kg, (float)iv.x * inv_scale, (float)iv.y * inv_scale, (float)iv.z * inv_scale,
                                (float)iv.w * inv_scale);
             });
         } else {
-            for_brick(b, rowbase, K1, [&](int kt, size_t kg) {
+            for_brick<NT>(b, rowbase, K1, [&](int kt, size_t kg) {
                 const int iv = itile[kt];
                 if (iv != 0) red_add(grid + kg, (float)iv * inv_scale);
             });
@@ -344,6 +344,19 @@ __global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_spread(const
             }
         }
     }
+}
+
+// Spread of chunks of packed (x, y, z, q) particles.  nchunk_dev (optional) holds the number of
+// active chunks (the cluster list's super-cluster count).
+template <int P, int WIN>
+__global__ void __launch_bounds__(MESH_THREADS, MESH_CTAS_PER_SM) k_spread(const float4 *__restrict__ xq, int nchunks,
+                                                         const int *__restrict__ nchunk_dev, float *__restrict__ grid,
+                                                         int K1, int K2, int K3, float Lx, float Ly, float Lz,
+                                                         WindowPoly wp) {
+    const int c = blockIdx.x;
+    if (nchunk_dev && c >= *nchunk_dev) return;
+    if (c >= nchunks) return;
+    spread_chunk<P, WIN, MESH_CHUNK>(xq + (size_t)c * MESH_CHUNK, grid, K1, K2, K3, Lx, Ly, Lz, wp);
 }
 
 // AD gather of chunks (the sums of _gather_ad_lines_sums, MeshKernels.jl:281-311,
