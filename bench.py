@@ -866,7 +866,7 @@ def melts_sizes(nmelts: int, rank: int = 0):
     return [n + (n % 2) for n in ns]
 
 
-def melts_measure(pd, ns, steps, warmup, skin, buffer, prune, world=1, compare=True):
+def melts_measure(pd, ns, steps, warmup, skin, buffer, prune, world=1, compare=True, shape=None):
     """The charged melts as one batch (one launch per force stage, the step one captured graph, lanes per row
     and spread tile by the autotuner), and, with ``compare``, each melt's own captured single-system step
     replayed concurrently on 16 streams and one after another.  Returns the result dict (ms per step,
@@ -877,9 +877,31 @@ def melts_measure(pd, ns, steps, warmup, skin, buffer, prune, world=1, compare=T
     systems = pd.batch.melt_systems(ns, rho=RHO, T=T_INIT, seed=SEED)
     alpha = pd.splits.alpha_from_tolerance(RC, 1e-5)
     el = dict(alpha=alpha, C=pd.synthetic.COULOMB_EV_A, rc=RC, order=5, kind="spme", spacing=1.0)
-    batch = pd.batch.BatchedReplicas(systems, skin=skin, electrostatics=el)
-    batch.evaluate()
-    tuned = batch.autotune(dt)
+    if shape is None:
+        # autotuner: row-list skin (longer rows against fewer partial rebuilds), then lanes per row x spread
+        # tile on whole captured steps of the batch itself
+        trials = {}
+        for sk in ((skin,) if skin is not None else (0.8, 1.2, 1.6)):
+            bt = pd.batch.BatchedReplicas(systems, skin=sk, electrostatics=el)
+            bt.evaluate()
+            tb = bt.autotune(dt)
+            trials[sk] = (min(tb["ms"].values()), tb)
+            bt.close()
+            del bt
+            torch.cuda.empty_cache()
+        skin = min(trials, key=lambda k: trials[k][0])
+        tuned = dict(trials[skin][1], skin=skin, skin_trials_ms={str(k): v[0] for k, v in trials.items()})
+        batch = pd.batch.BatchedReplicas(systems, skin=skin, electrostatics=el)
+        batch.evaluate()
+        batch.set_lanes(tuned["lanes"])
+        batch.set_spread_tile(tuned["spread_tile"])
+    else:   # a fixed (lanes per row, spread tile), e.g. the autotuner's earlier choice for a launch list
+        skin = 1.0 if skin is None else skin
+        batch = pd.batch.BatchedReplicas(systems, skin=skin, electrostatics=el)
+        batch.evaluate()
+        batch.set_lanes(shape[0])
+        batch.set_spread_tile(shape[1])
+        tuned = {"lanes": shape[0], "spread_tile": shape[1], "skin": skin, "fixed": True}
     batch.step(warmup, dt)
     torch.cuda.synchronize()
     s0 = batch.stream
@@ -963,8 +985,9 @@ def run_melts_workload(pd, args, world, rank):
     """64 independent charged melts (the 64 000-ion melt's density, LJ and SPME settings, 1 A mesh, order 5)
     as one batch, against each melt's own captured step replayed concurrently and one after another."""
     ns = melts_sizes(args.melts, rank)
+    shape = None if args.melt_shape is None else tuple(int(v) for v in args.melt_shape.split("x"))
     res = melts_measure(pd, ns, args.steps, args.warmup, args.melt_skin, args.buffer, args.prune, world=world,
-                        compare=not args.no_compare)
+                        compare=not args.no_compare, shape=shape)
     if rank == 0:
         line = {"metric": res.pop("metric"), "value": res.pop("value"), "unit": res.pop("unit"), "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": res.pop("ms_per_step"),
@@ -1022,7 +1045,10 @@ def main():
     ap.add_argument("--prune", type=float, default=PRUNE, help="prune buffer (Angstrom)")
     ap.add_argument("--replicas", type=int, default=512, help="replicas of the batch512 workload")
     ap.add_argument("--melts", type=int, default=64, help="charged melts of the melts64 workload")
-    ap.add_argument("--melt-skin", type=float, default=1.0, help="row-list skin of the batched melts (Angstrom)")
+    ap.add_argument("--melt-skin", type=float, default=None,
+                    help="row-list skin of the batched melts (Angstrom); default: the autotuner's choice")
+    ap.add_argument("--melt-shape", default=None,
+                    help="melts64: lanes per row x spread tile, e.g. 4x64, instead of the autotuner's choice")
     ap.add_argument("--no-compare", action="store_true",
                     help="melts64: time the batched path only (no single-system replays), e.g. for a launch list")
     ap.add_argument("--workload", default="melt64k",
@@ -1220,7 +1246,7 @@ def main():
                    "config1a_lj1m": ell_config(pd, "lj1m", 30, args.warmup, peaks),
                    "config1b_wca2d1m": ell_config(pd, "wca2d1m", 30, args.warmup, peaks),
                    "config4_batch512": batch_config(pd, 30, args.warmup, peaks),
-                   "config4_melts64": melts_measure(pd, melts_sizes(64), 20, args.warmup, 1.0, args.buffer,
+                   "config4_melts64": melts_measure(pd, melts_sizes(64), 20, args.warmup, None, args.buffer,
                                                     args.prune)}
         for c in configs.values():
             c["value"] = world * c["value"]

@@ -461,7 +461,13 @@ struct pd_batch {
         cufftHandle fwd, bwd;
     };
     std::vector<FftGroup> groups;
-    void *fft_work = nullptr;
+    // the mesh sizes' transforms run on NFFT streams at once, group g on stream g % NFFT with that
+    // stream's own cuFFT work area
+    static constexpr int NFFT = 4;
+    void *fft_work[NFFT] = {nullptr, nullptr, nullptr, nullptr};
+    cudaStream_t fft_stream[NFFT] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev_fft[NFFT] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev_fft_fork = nullptr;
     cudaStream_t mesh_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
@@ -488,8 +494,16 @@ static void batch_free_mesh(pd_batch *b) {
     dfree(b->gridB);
     dfree(b->G);
     dfree(b->spec);
-    if (b->fft_work) cudaFree(b->fft_work);
-    b->fft_work = nullptr;
+    for (int k = 0; k < pd_batch::NFFT; ++k) {
+        if (b->fft_work[k]) cudaFree(b->fft_work[k]);
+        if (b->fft_stream[k]) cudaStreamDestroy(b->fft_stream[k]);
+        if (b->ev_fft[k]) cudaEventDestroy(b->ev_fft[k]);
+        b->fft_work[k] = nullptr;
+        b->fft_stream[k] = nullptr;
+        b->ev_fft[k] = nullptr;
+    }
+    if (b->ev_fft_fork) cudaEventDestroy(b->ev_fft_fork);
+    b->ev_fft_fork = nullptr;
     if (b->mesh_stream) cudaStreamDestroy(b->mesh_stream);
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     if (b->ev_join) cudaEventDestroy(b->ev_join);
@@ -583,24 +597,40 @@ static BMeshView batch_mesh_view(const pd_batch *b) {
 
 // The mesh branch of charged replicas: spread, the batched forward transforms (one per mesh size),
 // the influence multiply, the batched inverse transforms.
+// Transforms of every mesh size, forked from s onto the FFT streams and joined back into s.
+static int batch_fft_all(pd_batch *b, bool forward, cudaStream_t s) {
+    const int ns = std::min<int>(pd_batch::NFFT, (int)b->groups.size());
+    PD_CUDA(cudaEventRecord(b->ev_fft_fork, s));
+    for (int k = 0; k < ns; ++k) PD_CUDA(cudaStreamWaitEvent(b->fft_stream[k], b->ev_fft_fork, 0));
+    for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+        auto &g = b->groups[gi];
+        cudaStream_t fs = b->fft_stream[gi % pd_batch::NFFT];
+        if (forward) {
+            PD_CHECK(cufftSetStream(g.fwd, fs) == CUFFT_SUCCESS, PD_ECUFFT, "batched mesh: cufftSetStream failed");
+            PD_CHECK(cufftExecR2C(g.fwd, b->gridA + g.grid, reinterpret_cast<cufftComplex *>(b->spec + g.modes)) ==
+                         CUFFT_SUCCESS,
+                     PD_ECUFFT, "batched mesh: forward transform failed");
+        } else {
+            PD_CHECK(cufftSetStream(g.bwd, fs) == CUFFT_SUCCESS, PD_ECUFFT, "batched mesh: cufftSetStream failed");
+            PD_CHECK(cufftExecC2R(g.bwd, reinterpret_cast<cufftComplex *>(b->spec + g.modes), b->gridB + g.grid) ==
+                         CUFFT_SUCCESS,
+                     PD_ECUFFT, "batched mesh: inverse transform failed");
+        }
+    }
+    for (int k = 0; k < ns; ++k) {
+        PD_CUDA(cudaEventRecord(b->ev_fft[k], b->fft_stream[k]));
+        PD_CUDA(cudaStreamWaitEvent(s, b->ev_fft[k], 0));
+    }
+    return PD_OK;
+}
+
 static int batch_mesh_transform(pd_batch *b, cudaStream_t s) {
     const BMeshView v = batch_mesh_view(b);
     int rc;
     if ((rc = bmesh_spread_launch(v, b->st, s))) return rc;
-    for (auto &g : b->groups) {
-        PD_CHECK(cufftSetStream(g.fwd, s) == CUFFT_SUCCESS, PD_ECUFFT, "batched mesh: cufftSetStream failed");
-        PD_CHECK(cufftExecR2C(g.fwd, b->gridA + g.grid, reinterpret_cast<cufftComplex *>(b->spec + g.modes)) ==
-                     CUFFT_SUCCESS,
-                 PD_ECUFFT, "batched mesh: forward transform failed");
-    }
+    if ((rc = batch_fft_all(b, true, s))) return rc;
     if ((rc = bmesh_solve_launch(v, b->st, s))) return rc;
-    for (auto &g : b->groups) {
-        PD_CHECK(cufftSetStream(g.bwd, s) == CUFFT_SUCCESS, PD_ECUFFT, "batched mesh: cufftSetStream failed");
-        PD_CHECK(cufftExecC2R(g.bwd, reinterpret_cast<cufftComplex *>(b->spec + g.modes), b->gridB + g.grid) ==
-                     CUFFT_SUCCESS,
-                 PD_ECUFFT, "batched mesh: inverse transform failed");
-    }
-    return PD_OK;
+    return batch_fft_all(b, false, s);
 }
 
 // The force pass: pack, then the row pair kernel; with charges and meshes the pair kernel runs on s
@@ -1052,12 +1082,17 @@ static int batch_set_mesh(pd_batch *b, int kind, int order, double alpha, double
                  PD_ECUFFT, "batched mesh: plan of %d meshes %dx%dx%d failed", g.count, g.K1, g.K2, g.K3);
         wmax = std::max(wmax, std::max(w1, w2));
     }
-    if (wmax > 0) {
-        PD_CUDA(cudaMalloc(&b->fft_work, wmax));
-        for (auto &g : b->groups)
-            PD_CHECK(cufftSetWorkArea(g.fwd, b->fft_work) == CUFFT_SUCCESS &&
-                         cufftSetWorkArea(g.bwd, b->fft_work) == CUFFT_SUCCESS,
-                     PD_ECUFFT, "batched mesh: cufftSetWorkArea failed");
+    for (int k = 0; k < pd_batch::NFFT; ++k) {
+        PD_CUDA(cudaMalloc(&b->fft_work[k], std::max<size_t>(wmax, 256)));
+        PD_CUDA(cudaStreamCreateWithFlags(&b->fft_stream[k], cudaStreamNonBlocking));
+        PD_CUDA(cudaEventCreateWithFlags(&b->ev_fft[k], cudaEventDisableTiming));
+    }
+    PD_CUDA(cudaEventCreateWithFlags(&b->ev_fft_fork, cudaEventDisableTiming));
+    for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+        auto &g = b->groups[gi];
+        void *w = b->fft_work[gi % pd_batch::NFFT];
+        PD_CHECK(cufftSetWorkArea(g.fwd, w) == CUFFT_SUCCESS && cufftSetWorkArea(g.bwd, w) == CUFFT_SUCCESS,
+                 PD_ECUFFT, "batched mesh: cufftSetWorkArea failed");
     }
     PD_CUDA(cudaStreamCreateWithFlags(&b->mesh_stream, cudaStreamNonBlocking));
     PD_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));

@@ -9,7 +9,9 @@
 // chunk of cell-sorted particles lies in about two cells, so its B-spline stencils cover a small
 // brick that the spread accumulates in shared memory (32-bit fixed point, as the single-system
 // spread) and the gather stages before every particle reads its P^3 nodes.  The chunk size (32 or
-// 64 particles, 64 or 128 threads) is the autotuner's spread tile.
+// 64 particles, 64 or 128 threads) is the autotuner's spread tile.  The transforms of the mesh sizes
+// run on several streams at once (each size's batched plan is small; one after another they would
+// leave most of the GPU idle).
 //
 // Stages: k_bmesh_pack (coordinates and charges of the step, for the pair kernel and the chunks),
 // k_bspread, the batched R2C transforms (one cuFFT plan per mesh size, outside this file), k_bsolve
@@ -20,6 +22,12 @@
 #include "mesh_kernels.cuh"
 
 namespace pdb {
+
+// Shared brick of the batched spread and gather (45 KB of static shared memory): a tile of cell-sorted
+// ions spans one or two cells of at least the list radius, a larger brick than a single system's
+// super-cluster, so the batched kernels trade occupancy (4 CTAs per SM) for bricks that fit.
+constexpr int BTILE = 11264;
+constexpr int BMESH_CTAS_PER_SM = 4;
 
 __global__ void k_bmesh_pack(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
                              const float *__restrict__ q, const int *__restrict__ sorted,
@@ -42,7 +50,7 @@ __global__ void k_bmesh_pack(const float *__restrict__ x, const float *__restric
 }
 
 template <int P, int CH>
-__global__ void __launch_bounds__(2 * CH, MESH_CTAS_PER_SM) k_bspread(const float4 *__restrict__ mq,
+__global__ void __launch_bounds__(2 * CH, BMESH_CTAS_PER_SM) k_bspread(const float4 *__restrict__ mq,
                                                                       const int *__restrict__ chunk_rep,
                                                                       const BMeshRep *__restrict__ reps,
                                                                       float *__restrict__ gridA,
@@ -50,7 +58,7 @@ __global__ void __launch_bounds__(2 * CH, MESH_CTAS_PER_SM) k_bspread(const floa
     if (st[E_VALID] == 0) return;
     const int c = blockIdx.x;
     const BMeshRep R = reps[chunk_rep[c]];
-    spread_chunk<P, WIN_BSPLINE, CH>(mq + (size_t)c * CH, gridA + R.grid, R.K1, R.K2, R.K3, R.Lx, R.Ly, R.Lz,
+    spread_chunk<P, WIN_BSPLINE, CH, BTILE>(mq + (size_t)c * CH, gridA + R.grid, R.K1, R.K2, R.K3, R.Lx, R.Ly, R.Lz,
                                      WindowPoly{nullptr, 0});
 }
 
@@ -79,7 +87,7 @@ __global__ void __launch_bounds__(256) k_bsolve(float2 *__restrict__ spec, const
 // _gather_ad_lines_kernel!, :313-333) from the replica's potential grid, joined with the pair force
 // already stored for the particle: F = F_pair - q grad(phi) K / L, then the closing half kick.
 template <int P, int CH, bool ENERGY>
-__global__ void __launch_bounds__(2 * CH, MESH_CTAS_PER_SM) k_bgather(const float4 *__restrict__ mq,
+__global__ void __launch_bounds__(2 * CH, BMESH_CTAS_PER_SM) k_bgather(const float4 *__restrict__ mq,
                                                                       const int *__restrict__ mid,
                                                                       const int *__restrict__ chunk_rep,
                                                                       const BMeshRep *__restrict__ reps,
@@ -95,7 +103,7 @@ __global__ void __launch_bounds__(2 * CH, MESH_CTAS_PER_SM) k_bgather(const floa
     const BMeshRep R = reps[chunk_rep[c]];
     const float *grid = gridB + R.grid;
     const int K1 = R.K1, K2 = R.K2, K3 = R.K3;
-    __shared__ __align__(16) float tile[TILE_MAX];
+    __shared__ __align__(16) float tile[BTILE];
     __shared__ unsigned rowbase[ROWS_MAX];
     __shared__ int sm[10];
     __shared__ float part[CH][4];
@@ -127,7 +135,7 @@ __global__ void __launch_bounds__(2 * CH, MESH_CTAS_PER_SM) k_bgather(const floa
     }
     int d1 = 0, d2 = 0, d3 = 0;
     Brick b;
-    chunk_brick<P, NT>(charged, k1, k2, k3, K1, K2, K3, d1, d2, d3, b, sm, rowbase);
+    chunk_brick<P, NT, BTILE>(charged, k1, k2, k3, K1, K2, K3, d1, d2, d3, b, sm, rowbase);
     constexpr int PH = (P + 1) / 2;
     float phi = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
     if (b.fits) {

@@ -161,8 +161,9 @@ struct Brick {
 
 constexpr int ROWS_MAX = 512;   // brick rows tabulated in shared memory
 
-// NT: threads of the CTA that moves the brick (two per particle of the chunk).
-template <int P, int NT = MESH_THREADS>
+// NT: threads of the CTA that moves the brick (two per particle of the chunk); TILE: floats of the
+// shared brick.
+template <int P, int NT = MESH_THREADS, int TILE = TILE_MAX>
 __device__ __forceinline__ void chunk_brick(bool valid, int k1, int k2, int k3, int K1, int K2, int K3, int &d1,
                                             int &d2, int &d3, Brick &b, int *sm /* >= 10 ints */,
                                             unsigned *rowbase) {
@@ -211,7 +212,7 @@ __device__ __forceinline__ void chunk_brick(bool valid, int k1, int k2, int k3, 
         b.e2 = sm[8] - sm[5] + P;
         b.e3 = sm[9] - sm[6] + P;
         const long long nodes = (long long)b.e1 * b.e2 * b.e3;
-        b.fits = nodes <= TILE_MAX && b.e1 <= NT && (!b.vec || b.e1 <= K1) &&
+        b.fits = nodes <= TILE && b.e1 <= NT && (!b.vec || b.e1 <= K1) &&
                  (long long)b.e2 * b.e3 <= ROWS_MAX;
         if (valid) {
             d1 += shift - sm[4];
@@ -254,11 +255,11 @@ __device__ __forceinline__ void for_brick(const Brick &b, const unsigned *rowbas
 // Spread of one chunk of CH packed (x, y, z, q) particles into `grid` (the charge assignment of
 // _spread_lines_kernel!, MeshKernels.jl:247-276), by a CTA of 2 CH threads: each particle's two
 // threads take the two halves of its z stencil.
-template <int P, int WIN, int CH>
+template <int P, int WIN, int CH, int TILE = TILE_MAX>
 __device__ __forceinline__ void spread_chunk(const float4 *__restrict__ chunk, float *__restrict__ grid, int K1,
                                              int K2, int K3, float Lx, float Ly, float Lz, const WindowPoly &wp) {
     constexpr int NT = 2 * CH;
-    __shared__ __align__(16) float tile[TILE_MAX];
+    __shared__ __align__(16) float tile[TILE];
     __shared__ unsigned rowbase[ROWS_MAX];
     __shared__ int sm[10];
     const int t = threadIdx.x, p = t & (CH - 1), h = t / CH;
@@ -274,7 +275,7 @@ __device__ __forceinline__ void spread_chunk(const float4 *__restrict__ chunk, f
     int d1 = 0, d2 = 0, d3 = 0;
     Brick b;
     // both halves of a particle take part (their min/max contributions are identical)
-    chunk_brick<P, NT>(valid, k1, k2, k3, K1, K2, K3, d1, d2, d3, b, sm, rowbase);
+    chunk_brick<P, NT, TILE>(valid, k1, k2, k3, K1, K2, K3, d1, d2, d3, b, sm, rowbase);
     constexpr int PH = (P + 1) / 2;
 
     if (b.fits) {
