@@ -986,6 +986,26 @@ def run_melts_workload(pd, args, world, rank):
     as one batch, against each melt's own captured step replayed concurrently and one after another."""
     ns = melts_sizes(args.melts, rank)
     shape = None if args.melt_shape is None else tuple(int(v) for v in args.melt_shape.split("x"))
+    if args.profile:
+        # eager steps (no graph) so that a profiler sees every launch: set-up, one force evaluation with its
+        # full build, then warm-up and timed steps of the same batch and shape
+        import torch
+        shape = (1, 64) if shape is None else shape
+        systems = pd.batch.melt_systems(ns, rho=RHO, T=T_INIT, seed=SEED)
+        el = dict(alpha=pd.splits.alpha_from_tolerance(RC, 1e-5), C=pd.synthetic.COULOMB_EV_A, rc=RC, order=5,
+                  kind="spme", spacing=1.0)
+        b = pd.batch.BatchedReplicas(systems, skin=1.2 if args.melt_skin is None else args.melt_skin,
+                                     lanes=shape[0], electrostatics=el)
+        b.set_spread_tile(shape[1])
+        b.evaluate()
+        dt = DT_FS / pd.synthetic.TIME_UNIT_FS
+        b.step(args.warmup, dt, use_graph=False)
+        b.step(args.steps, dt, use_graph=False)
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"profile": "melts64 eager steps", "steps": args.steps, "shape": shape,
+                              "rows": b.status(), "mesh": b.mesh_info()}))
+        return
     res = melts_measure(pd, ns, args.steps, args.warmup, args.melt_skin, args.buffer, args.prune, world=world,
                         compare=not args.no_compare, shape=shape)
     if rank == 0:

@@ -187,14 +187,19 @@ __global__ void k_batch_bin(const float *__restrict__ x, const float *__restrict
 }
 
 // Rows, one warp per global cell: the replica's stencil (same visiting order as the single-system
-// row kernels) staged in shared memory, each lane a particle of the cell.  Rows, their lengths and
-// their entries are in cell order (positions in `sorted`), so the row stores of a warp and the pair
-// kernel's row loads are contiguous and neighbours' packed records sit close together.
+// row kernels) staged in shared memory once per cell, each lane taking up to M particles of the cell
+// (lane, lane + 32, ...), so a cell of up to 32 M particles stages its candidates once.
+// The candidates come from the packed coordinates in cell order (xq, packed after the sort of this
+// rebuild), so a stencil row's candidates are one contiguous, coalesced float4 run.  Rows, their
+// lengths and their entries are in cell order (positions in `sorted`), so the row stores of a warp and
+// the pair kernel's row loads are contiguous and neighbours' packed records sit close together; a
+// particle's entries are appended in the candidates' visiting order, as in the single-system kernels.
+template <int M>   // particles per lane (1, 2 or 4), from the batch's mean cell occupancy
 __global__ void __launch_bounds__(32 * BROWS_WARPS) k_batch_rows(
-    const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z, int n, int ncell,
-    const int *__restrict__ cell_rep, const BatchRep *__restrict__ reps, const int *__restrict__ rep_flag,
-    const int *__restrict__ sorted, const int *__restrict__ cell_off, float rl2, int cap, int *__restrict__ rows,
-    int *__restrict__ counts, float4 *__restrict__ ref, long long *__restrict__ st) {
+    const float4 *__restrict__ xq, int n, int ncell, const int *__restrict__ cell_rep,
+    const BatchRep *__restrict__ reps, const int *__restrict__ rep_flag, const int *__restrict__ sorted,
+    const int *__restrict__ cell_off, float rl2, int cap, int *__restrict__ rows, int *__restrict__ counts,
+    float4 *__restrict__ ref, long long *__restrict__ st) {
     if (!ell_requested(st)) return;
     extern __shared__ float4 batch_stage[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -212,44 +217,44 @@ __global__ void __launch_bounds__(32 * BROWS_WARPS) k_batch_rows(
         const int lc = c - base;
         const int cx = lc % nx, tmp = lc / nx, cy = tmp % ny, cz = tmp / ny;
         const int p0 = cell_off[c], pn = cell_off[c + 1] - p0;
-        for (int pg = 0; pg < pn; pg += 32) {
-            const bool has = pg + lane < pn;
-            const int kp = p0 + pg + lane;   // this lane's particle: its position in cell order
-            const int i = has ? sorted[kp] : -1;
-            const float xi = has ? x[i] : 0.f, yi = has ? y[i] : 0.f, zi = has ? z[i] : 0.f;
-            int found = 0;
+        for (int pg = 0; pg < pn; pg += 32 * M) {
+            int kp[M], found[M];
+            bool has[M];
+            float xi[M], yi[M], zi[M];
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                has[m] = pg + lane + 32 * m < pn;
+                kp[m] = p0 + pg + lane + 32 * m;   // this lane's m-th particle: its position in cell order
+                const float4 v = has[m] ? xq[kp[m]] : make_float4(0.f, 0.f, 0.f, 0.f);
+                xi[m] = v.x;
+                yi[m] = v.y;
+                zi[m] = v.z;
+                found[m] = 0;
+            }
             int fill = 0;
-            auto scan = [&]() {
-                __syncwarp();
-                if (has) {
-                    for (int t = 0; t < fill; ++t) {
-                        const float4 cj = sw[t];
-                        const int kc = __float_as_int(cj.w);
-                        if (kc == kp) continue;
-                        const float dx = mic_fast(cj.x - xi, hLx, Lx);
-                        const float dy = mic_fast(cj.y - yi, hLy, Ly);
-                        const float dz = mic_fast(cj.z - zi, hLz, Lz);
-                        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                        if (r2 <= rl2) {
-                            if (found < cap) rows[(size_t)found * n + kp] = kc;
-                            ++found;
-                        }
-                    }
-                }
-                __syncwarp();
-                fill = 0;
-            };
-            auto stage = [&](int ka, int kb) {
-                for (int k0 = ka; k0 < kb; k0 += 32) {
-                    const int cnt = min(32, kb - k0);
-                    if (fill + cnt > BROWS_CAP) scan();
-                    if (lane < cnt) {
-                        const int j = sorted[k0 + lane];
-                        sw[fill + lane] = make_float4(x[j], y[j], z[j], __int_as_float(k0 + lane));
-                    }
-                    fill += cnt;
-                }
-            };
+            // scan of the staged candidates by every particle of the lane (one body, expanded where a
+            // full stage buffer is flushed and at the end, so the per-particle counters stay in registers)
+#define PD_BATCH_ROWS_SCAN                                                            \
+    do {                                                                              \
+        __syncwarp();                                                                 \
+        for (int t = 0; t < fill; ++t) {                                              \
+            const float4 cj = sw[t];                                                  \
+            const int kc = __float_as_int(cj.w);                                      \
+            _Pragma("unroll") for (int m = 0; m < M; ++m) {                           \
+                if (!has[m] || kc == kp[m]) continue;                                 \
+                const float dx = mic_fast(cj.x - xi[m], hLx, Lx);                     \
+                const float dy = mic_fast(cj.y - yi[m], hLy, Ly);                     \
+                const float dz = mic_fast(cj.z - zi[m], hLz, Lz);                     \
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));                 \
+                if (r2 <= rl2) {                                                      \
+                    if (found[m] < cap) rows[(size_t)found[m] * n + kp[m]] = kc;      \
+                    ++found[m];                                                       \
+                }                                                                     \
+            }                                                                         \
+        }                                                                             \
+        __syncwarp();                                                                 \
+        fill = 0;                                                                     \
+    } while (0)
             for (int oz = -Sz; oz <= Sz; ++oz) {
                 int cz2 = cz + oz;
                 cz2 -= cz2 >= nz ? nz : 0;
@@ -265,16 +270,32 @@ __global__ void __launch_bounds__(32 * BROWS_WARPS) k_batch_rows(
                     const int row = base + (cz2 * ny + cy2) * nx;
                     int a1, b1, a2, b2;
                     ell_row_ranges(cx, g2, rl2, hx, Sx, nx, a1, b1, a2, b2);
-                    stage(cell_off[row + a1], cell_off[row + b1 + 1]);
-                    if (a2 <= b2) stage(cell_off[row + a2], cell_off[row + b2 + 1]);
+                    for (int part = 0; part < 2; ++part) {
+                        if (part == 1 && a2 > b2) break;
+                        const int ka = cell_off[row + (part ? a2 : a1)], kb = cell_off[row + (part ? b2 : b1) + 1];
+                        for (int k0 = ka; k0 < kb; k0 += 32) {
+                            const int cnt = min(32, kb - k0);
+                            if (fill + cnt > BROWS_CAP) PD_BATCH_ROWS_SCAN;
+                            if (lane < cnt) {
+                                float4 v = xq[k0 + lane];
+                                v.w = __int_as_float(k0 + lane);
+                                sw[fill + lane] = v;
+                            }
+                            fill += cnt;
+                        }
+                    }
                 }
             }
-            scan();
-            if (has) {
-                counts[kp] = found;
-                ref[i] = make_float4(xi, yi, zi, 0.f);
+            PD_BATCH_ROWS_SCAN;
+#undef PD_BATCH_ROWS_SCAN
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                if (has[m]) {
+                    counts[kp[m]] = found[m];
+                    ref[sorted[kp[m]]] = make_float4(xi[m], yi[m], zi[m], 0.f);
+                }
+                fmax = max(fmax, (unsigned)found[m]);
             }
-            fmax = max(fmax, (unsigned)found);
         }
     }
     if (ell_block_max_last(fmax, st, E_RMAX, E_TICKET_R)) {
@@ -293,15 +314,18 @@ __global__ void __launch_bounds__(32 * BROWS_WARPS) k_batch_rows(
     }
 }
 
-// Packed coordinates in cell order: xq[k] = (x, y, z) of particle sorted[k].
+// Packed coordinates (and charges, when q is given) in cell order: xq[k] = (x, y, z, q) of particle
+// sorted[k].  REBUILD: the pack that feeds the row build of a rebuild (runs while the rows are being
+// rebuilt); otherwise the pack of the pair pass (skipped while the rows are invalid).
+template <bool REBUILD>
 __global__ void k_batch_pack(const float *__restrict__ x, const float *__restrict__ y, const float *__restrict__ z,
-                             const int *__restrict__ sorted, int n, float4 *__restrict__ xq,
-                             const long long *__restrict__ st) {
-    if (st[E_VALID] == 0) return;   // no rows: the pair kernel will not read the packed records
+                             const float *__restrict__ q, const int *__restrict__ sorted, int n,
+                             float4 *__restrict__ xq, const long long *__restrict__ st) {
+    if (REBUILD ? !ell_requested(st) : st[E_VALID] == 0) return;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const int i = sorted[k];
-    xq[k] = make_float4(x[i], y[i], z[i], 0.f);
+    xq[k] = make_float4(x[i], y[i], z[i], q ? q[i] : 0.f);
 }
 
 struct BatchKick {
@@ -324,8 +348,10 @@ struct BatchCoul {
 // Row pair kernel over all replicas: the model of particle i's replica (LJ or WCA, the ELL route's
 // UniformLJ / UniformWCA arithmetic), forces stored, optional energy (half of each pair), the
 // closing half kick fused.  The packed coordinates are refreshed by the pack of the same stage.
-// COUL: the packed records carry the charges (xq.w) and the pair adds the Coulomb polynomial term.
-template <int G, bool ENERGY, bool COUL>
+// COUL: the packed records carry the charges (xq.w) and the pair adds the Coulomb polynomial term,
+// evaluated with NP coefficients (the fitted ones, zeros above them); one reciprocal square root
+// serves both terms.
+template <int G, bool ENERGY, bool COUL, int NP = BATCH_NP>
 __global__ void __launch_bounds__(B_THREADS) k_batch_pairs(const float4 *__restrict__ xq, int n,
                                                            const int *__restrict__ rows,
                                                            const int *__restrict__ counts,
@@ -350,11 +376,43 @@ __global__ void __launch_bounds__(B_THREADS) k_batch_pairs(const float4 *__restr
         const float4 pi = xq[k];
         const int cnt = counts[k];
         const float cqi = COUL ? cp.C * pi.w : 0.f;
+        const float cut2 = COUL ? fmaxf(rc2, cp.rc2) : rc2;
         auto pair = [&](float4 pj) {
             const float dx = periodic_delta(pi.x, pj.x, hLx, Lx);
             const float dy = periodic_delta(pi.y, pj.y, hLy, Ly);
             const float dz = periodic_delta(pi.z, pj.z, hLz, Lz);
             const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            if (COUL) {
+                if (!(r2 > 0.f && r2 < cut2)) return;
+                const float rinv = rsqrtf(r2);
+                const float ir2 = rinv * rinv;
+                float fr = 0.f;
+                if (r2 < rc2) {
+                    const float s2 = sig2 * ir2;
+                    const float s6 = s2 * s2 * s2;
+                    const float s12 = s6 * s6;
+                    fr = 24.f * eps * (2.f * s12 - s6) * ir2;
+                    if (ENERGY) e += 0.5f * (4.f * eps * (s12 - s6) + eoff);
+                }
+                if (r2 < cp.rc2) {
+                    const float x = fmaf(r2, cp.sx, -1.f);
+                    float pf = cp.pf[NP - 1];
+#pragma unroll
+                    for (int t = NP - 2; t >= 0; --t) pf = fmaf(pf, x, cp.pf[t]);
+                    const float cq = cqi * pj.w;
+                    fr = fmaf(cq, rinv * ir2 - pf, fr);
+                    if (ENERGY) {
+                        float pe = cp.pe[NP - 1];
+#pragma unroll
+                        for (int t = NP - 2; t >= 0; --t) pe = fmaf(pe, x, cp.pe[t]);
+                        e = fmaf(0.5f * cq, rinv + pe - cp.eshift, e);
+                    }
+                }
+                a[0] = fmaf(fr, dx, a[0]);
+                a[1] = fmaf(fr, dy, a[1]);
+                a[2] = fmaf(fr, dz, a[2]);
+                return;
+            }
             if (r2 > 0.f && r2 < rc2) {
                 const float ir2 = 1.f / r2;
                 const float s2 = sig2 * ir2;
@@ -365,25 +423,6 @@ __global__ void __launch_bounds__(B_THREADS) k_batch_pairs(const float4 *__restr
                 a[1] += fr * dy;
                 a[2] += fr * dz;
                 if (ENERGY) e += 0.5f * (4.f * eps * (s12 - s6) + eoff);
-            }
-            if (COUL && r2 > 0.f && r2 < cp.rc2) {
-                const float rinv = rsqrtf(r2);
-                const float rinv2 = rinv * rinv;
-                const float x = fmaf(r2, cp.sx, -1.f);
-                float pf = cp.pf[BATCH_NP - 1];
-#pragma unroll
-                for (int t = BATCH_NP - 2; t >= 0; --t) pf = fmaf(pf, x, cp.pf[t]);
-                const float cq = cqi * pj.w;
-                const float fq = cq * (rinv * rinv2 - pf);
-                a[0] = fmaf(fq, dx, a[0]);
-                a[1] = fmaf(fq, dy, a[1]);
-                a[2] = fmaf(fq, dz, a[2]);
-                if (ENERGY) {
-                    float pe = cp.pe[BATCH_NP - 1];
-#pragma unroll
-                    for (int t = BATCH_NP - 2; t >= 0; --t) pe = fmaf(pe, x, cp.pe[t]);
-                    e = fmaf(0.5f * cq, rinv + pe - cp.eshift, e);
-                }
             }
         };
         int slot = lane;
@@ -445,6 +484,7 @@ struct pd_batch {
     // charged replicas: real-space Coulomb and the batched meshes
     bool coul = false;
     BatchCoul cp{};
+    int coul_ne = 0, coul_nf = 0;
     float half_c_self = 0.f;
     bool mesh = false;
     int morder = 5, mchunk = 64, nchunk = 0;
@@ -544,28 +584,40 @@ static int batch_rebuild_launch(pd_batch *b, const float *x, const float *y, con
     if ((rc = ell_sort_cells_launch(b->cell_of, b->n, b->ncell, b->cell_count, b->cell_off, b->sorted, b->tmp, b->st,
                                     s)))
         return rc;
-    k_batch_rows<<<(b->ncell + BROWS_WARPS - 1) / BROWS_WARPS, 32 * BROWS_WARPS,
-                   sizeof(float4) * BROWS_WARPS * BROWS_CAP, s>>>(x, y, z, b->n, b->ncell, b->cell_rep, b->reps,
-                                                                  b->rep_flag, b->sorted, b->cell_off, b->rl2, b->cap,
-                                                                  b->rows, b->counts, b->ref, b->st);
+    k_batch_pack<true><<<(b->n + B_THREADS - 1) / B_THREADS, B_THREADS, 0, s>>>(x, y, z, nullptr, b->sorted, b->n,
+                                                                                b->xq, b->st);
+    PD_LAUNCHED();
+    // particles per lane: enough lanes for a cell of 1.3x the mean occupancy
+    const double occ = 1.3 * (double)b->n / (double)std::max(b->ncell, 1);
+    const dim3 grid((b->ncell + BROWS_WARPS - 1) / BROWS_WARPS), block(32 * BROWS_WARPS);
+    const size_t shm = sizeof(float4) * BROWS_WARPS * BROWS_CAP;
+    if (occ <= 32.0)
+        k_batch_rows<1><<<grid, block, shm, s>>>(b->xq, b->n, b->ncell, b->cell_rep, b->reps, b->rep_flag, b->sorted,
+                                                 b->cell_off, b->rl2, b->cap, b->rows, b->counts, b->ref, b->st);
+    else if (occ <= 64.0)
+        k_batch_rows<2><<<grid, block, shm, s>>>(b->xq, b->n, b->ncell, b->cell_rep, b->reps, b->rep_flag, b->sorted,
+                                                 b->cell_off, b->rl2, b->cap, b->rows, b->counts, b->ref, b->st);
+    else
+        k_batch_rows<4><<<grid, block, shm, s>>>(b->xq, b->n, b->ncell, b->cell_rep, b->reps, b->rep_flag, b->sorted,
+                                                 b->cell_off, b->rl2, b->cap, b->rows, b->counts, b->ref, b->st);
     PD_LAUNCHED();
     return PD_OK;
 }
 
-template <bool COUL>
+template <bool COUL, int NP = BATCH_NP>
 static void launch_batch_pairs(pd_batch *b, float *fx, float *fy, float *fz, float *epot, int energy,
                                const BatchKick &kick, int advance, cudaStream_t s) {
     const int G = b->lanes;
     const int blocks = (int)(((long long)b->n * G + B_THREADS - 1) / B_THREADS);
 #define PD_BP(GG)                                                                                                      \
     if (energy)                                                                                                        \
-        k_batch_pairs<GG, true, COUL><<<blocks, B_THREADS, 0, s>>>(b->xq, b->n, b->rows, b->counts, b->sorted,       \
-                                                                    b->rep_of, b->reps, fx, fy, fz, epot, kick, b->st, \
-                                                                    advance, b->cp);                                   \
+        k_batch_pairs<GG, true, COUL, NP><<<blocks, B_THREADS, 0, s>>>(b->xq, b->n, b->rows, b->counts, b->sorted,   \
+                                                                        b->rep_of, b->reps, fx, fy, fz, epot, kick,    \
+                                                                        b->st, advance, b->cp);                        \
     else                                                                                                               \
-        k_batch_pairs<GG, false, COUL><<<blocks, B_THREADS, 0, s>>>(b->xq, b->n, b->rows, b->counts, b->sorted,      \
-                                                                     b->rep_of, b->reps, fx, fy, fz, epot, kick,       \
-                                                                     b->st, advance, b->cp);
+        k_batch_pairs<GG, false, COUL, NP><<<blocks, B_THREADS, 0, s>>>(b->xq, b->n, b->rows, b->counts, b->sorted,  \
+                                                                         b->rep_of, b->reps, fx, fy, fz, epot, kick,   \
+                                                                         b->st, advance, b->cp);
     switch (G) {
         case 1: PD_BP(1) break;
         case 2: PD_BP(2) break;
@@ -639,8 +691,8 @@ static int batch_mesh_transform(pd_batch *b, cudaStream_t s) {
 static int batch_pairs_launch(pd_batch *b, const float *x, const float *y, const float *z, float *fx, float *fy,
                               float *fz, float *epot, int energy, BatchKick kick, int advance, cudaStream_t s) {
     if (!b->coul) {
-        k_batch_pack<<<(b->n + B_THREADS - 1) / B_THREADS, B_THREADS, 0, s>>>(x, y, z, b->sorted, b->n, b->xq,
-                                                                              b->st);
+        k_batch_pack<false><<<(b->n + B_THREADS - 1) / B_THREADS, B_THREADS, 0, s>>>(x, y, z, nullptr, b->sorted, b->n,
+                                                                                     b->xq, b->st);
         PD_LAUNCHED();
         launch_batch_pairs<false>(b, fx, fy, fz, epot, energy, kick, advance, s);
         PD_LAUNCHED();
@@ -657,7 +709,11 @@ static int batch_pairs_launch(pd_batch *b, const float *x, const float *y, const
     PD_CUDA(cudaEventRecord(b->ev_join, b->mesh_stream));
     BatchKick nokick = kick;
     nokick.on = 0;
-    launch_batch_pairs<true>(b, fx, fy, fz, epot, energy, nokick, advance, s);
+    // the polynomial's coefficient bucket: the fitted force coefficients, and the energy's with energy
+    if (std::max(b->coul_nf, energy ? b->coul_ne : 0) <= 14)
+        launch_batch_pairs<true, 14>(b, fx, fy, fz, epot, energy, nokick, advance, s);
+    else
+        launch_batch_pairs<true, BATCH_NP>(b, fx, fy, fz, epot, energy, nokick, advance, s);
     PD_LAUNCHED();
     PD_CUDA(cudaStreamWaitEvent(s, b->ev_join, 0));
     BMeshKick mk;
@@ -948,6 +1004,8 @@ int pd_batch_set_coulomb(pd_batch *b, const pd_batch_coulomb *c) {
     for (int k = 0; k < c->nf; ++k) cp.pf[k] = c->pf[k];
     for (int k = 0; k < c->ne; ++k) cp.pe[k] = c->pe[k];
     b->cp = cp;
+    b->coul_ne = c->ne;
+    b->coul_nf = c->nf;
     b->half_c_self = 0.5f * c->C * c->selfc;
     b->coul = true;
     if (b->exec) cudaGraphExecDestroy(b->exec);
