@@ -231,6 +231,32 @@ __global__ void __launch_bounds__(32 * BROWS_WARPS) k_batch_rows(
                 zi[m] = v.z;
                 found[m] = 0;
             }
+            // bounding box of this group's particles: a candidate farther than the list radius from the
+            // box is farther from every particle of the group, so it is not staged (a conservative
+            // margin keeps rounding from dropping a candidate that the exact test would accept)
+            float blo[3] = {INFINITY, INFINITY, INFINITY}, bhi[3] = {-INFINITY, -INFINITY, -INFINITY};
+#pragma unroll
+            for (int m = 0; m < M; ++m) {
+                if (!has[m]) continue;
+                blo[0] = fminf(blo[0], xi[m]);
+                blo[1] = fminf(blo[1], yi[m]);
+                blo[2] = fminf(blo[2], zi[m]);
+                bhi[0] = fmaxf(bhi[0], xi[m]);
+                bhi[1] = fmaxf(bhi[1], yi[m]);
+                bhi[2] = fmaxf(bhi[2], zi[m]);
+            }
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) {
+                    blo[d] = fminf(blo[d], __shfl_xor_sync(0xffffffffu, blo[d], off));
+                    bhi[d] = fmaxf(bhi[d], __shfl_xor_sync(0xffffffffu, bhi[d], off));
+                }
+            }
+            const float bcx = 0.5f * (blo[0] + bhi[0]), bcy = 0.5f * (blo[1] + bhi[1]), bcz = 0.5f * (blo[2] + bhi[2]);
+            const float bhx = 0.5f * (bhi[0] - blo[0]), bhy = 0.5f * (bhi[1] - blo[1]), bhz = 0.5f * (bhi[2] - blo[2]);
+            const float rbox = rl * 1.0001f + 1e-3f;
+            const float rbox2 = rbox * rbox;
             int fill = 0;
             // scan of the staged candidates by every particle of the lane (one body, expanded where a
             // full stage buffer is flushed and at the end, so the per-particle counters stay in registers)
@@ -274,14 +300,20 @@ __global__ void __launch_bounds__(32 * BROWS_WARPS) k_batch_rows(
                         if (part == 1 && a2 > b2) break;
                         const int ka = cell_off[row + (part ? a2 : a1)], kb = cell_off[row + (part ? b2 : b1) + 1];
                         for (int k0 = ka; k0 < kb; k0 += 32) {
-                            const int cnt = min(32, kb - k0);
-                            if (fill + cnt > BROWS_CAP) PD_BATCH_ROWS_SCAN;
-                            if (lane < cnt) {
-                                float4 v = xq[k0 + lane];
+                            const bool in = lane < kb - k0;
+                            float4 v = in ? xq[k0 + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+                            const float ex = fmaxf(fabsf(mic_fast(v.x - bcx, hLx, Lx)) - bhx, 0.f);
+                            const float ey = fmaxf(fabsf(mic_fast(v.y - bcy, hLy, Ly)) - bhy, 0.f);
+                            const float ez = fmaxf(fabsf(mic_fast(v.z - bcz, hLz, Lz)) - bhz, 0.f);
+                            const bool keep = in && fmaf(ex, ex, fmaf(ey, ey, ez * ez)) <= rbox2;
+                            const unsigned bal = __ballot_sync(0xffffffffu, keep);
+                            const int nk = __popc(bal);
+                            if (fill + nk > BROWS_CAP) PD_BATCH_ROWS_SCAN;
+                            if (keep) {   // staged in the candidates' order
                                 v.w = __int_as_float(k0 + lane);
-                                sw[fill + lane] = v;
+                                sw[fill + __popc(bal & ((1u << lane) - 1u))] = v;
                             }
-                            fill += cnt;
+                            fill += nk;
                         }
                     }
                 }

@@ -301,6 +301,23 @@ __global__ void __launch_bounds__(32 * ROWS_WARPS) k_ell_rows_cells(
             const bool has = pg + lane < pn;
             const int i = has ? sorted[p0 + pg + lane] : -1;
             const float xi = has ? x[i] : 0.f, yi = has ? y[i] : 0.f, zi = (has && D == 3) ? z[i] : 0.f;
+            // bounding box of this group's particles: a candidate farther than the list radius from the
+            // box is farther from every particle of the group and is not staged (a conservative margin
+            // keeps rounding from dropping a candidate that the exact test below would accept)
+            float bl[3] = {has ? xi : INFINITY, has ? yi : INFINITY, has ? zi : INFINITY};
+            float bh[3] = {has ? xi : -INFINITY, has ? yi : -INFINITY, has ? zi : -INFINITY};
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) {
+                    bl[d] = fminf(bl[d], __shfl_xor_sync(0xffffffffu, bl[d], off));
+                    bh[d] = fmaxf(bh[d], __shfl_xor_sync(0xffffffffu, bh[d], off));
+                }
+            }
+            const float bcx = 0.5f * (bl[0] + bh[0]), bcy = 0.5f * (bl[1] + bh[1]), bcz = 0.5f * (bl[2] + bh[2]);
+            const float bhx = 0.5f * (bh[0] - bl[0]), bhy = 0.5f * (bh[1] - bl[1]), bhz = 0.5f * (bh[2] - bl[2]);
+            const float rbox = rl * 1.0001f + 1e-3f;
+            const float rbox2 = rbox * rbox;
             int found = 0;
             int fill = 0;
             auto scan = [&]() {
@@ -330,13 +347,19 @@ __global__ void __launch_bounds__(32 * ROWS_WARPS) k_ell_rows_cells(
             };
             auto stage = [&](int ka, int kb) {
                 for (int k0 = ka; k0 < kb; k0 += 32) {
-                    const int cnt = min(32, kb - k0);
-                    if (fill + cnt > ROWS_CAP) scan();
-                    if (lane < cnt) {
-                        const int j = sorted[k0 + lane];
-                        sw[fill + lane] = make_float4(x[j], y[j], D == 3 ? z[j] : 0.f, __int_as_float(j));
-                    }
-                    fill += cnt;
+                    const bool in = lane < kb - k0;
+                    const int j = in ? sorted[k0 + lane] : 0;
+                    const float cx3 = in ? x[j] : 0.f, cy3 = in ? y[j] : 0.f, cz3 = (in && D == 3) ? z[j] : 0.f;
+                    const float ex = fmaxf(fabsf(mic_fast(cx3 - bcx, hLx, Lx)) - bhx, 0.f);
+                    const float ey = fmaxf(fabsf(mic_fast(cy3 - bcy, hLy, Ly)) - bhy, 0.f);
+                    const float ez = D == 3 ? fmaxf(fabsf(mic_fast(cz3 - bcz, hLz, Lz)) - bhz, 0.f) : 0.f;
+                    const bool keep = in && fmaf(ex, ex, fmaf(ey, ey, ez * ez)) <= rbox2;
+                    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+                    const int nk = __popc(bal);
+                    if (fill + nk > ROWS_CAP) scan();
+                    if (keep)   // staged in the candidates' order
+                        sw[fill + __popc(bal & ((1u << lane) - 1u))] = make_float4(cx3, cy3, cz3, __int_as_float(j));
+                    fill += nk;
                 }
             };
             for (int oz = -Sz; oz <= Sz; ++oz) {
