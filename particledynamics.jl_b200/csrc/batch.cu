@@ -1063,7 +1063,6 @@ static int batch_layout_chunks(pd_batch *b, int chunk) {
             }
         }
     }
-    b->nchunk = (int)crep.size();
     int rc;
     if ((rc = dalloc(&b->chunk_rep, crep.size())) || (rc = dalloc(&b->slot_src, src.size())) ||
         (rc = dalloc(&b->mid, src.size())) || (rc = dalloc(&b->mq, src.size())))
@@ -1072,6 +1071,7 @@ static int batch_layout_chunks(pd_batch *b, int chunk) {
     PD_CUDA(cudaMemcpy(b->slot_src, src.data(), sizeof(int) * src.size(), cudaMemcpyHostToDevice));
     PD_CUDA(cudaMemset(b->mid, 0xff, sizeof(int) * src.size()));
     PD_CUDA(cudaMemset(b->mq, 0, sizeof(float4) * src.size()));
+    b->nchunk = (int)crep.size();   // only a complete layout is used
     b->mchunk = chunk;
     return PD_OK;
 }
@@ -1222,7 +1222,9 @@ int pd_batch_set_spread_tile(pd_batch *b, int chunk) {
         return PD_OK;
     }
     if (chunk == b->mchunk) return PD_OK;
-    return batch_layout_chunks(b, chunk);
+    const int rc = batch_layout_chunks(b, chunk);
+    if (rc != PD_OK) batch_free_mesh(b);   // a batch without its tiles takes no charged step (PD_ESTATE)
+    return rc;
 }
 
 int pd_batch_mesh_info(pd_batch *b, int *groups, long long *nodes, long long *modes, int *chunk, int *nchunk) {
