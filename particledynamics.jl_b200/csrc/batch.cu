@@ -536,9 +536,9 @@ struct pd_batch {
     // the mesh sizes' transforms run on NFFT streams at once, group g on stream g % NFFT with that
     // stream's own cuFFT work area
     static constexpr int NFFT = 4;
-    void *fft_work[NFFT] = {nullptr, nullptr, nullptr, nullptr};
-    cudaStream_t fft_stream[NFFT] = {nullptr, nullptr, nullptr, nullptr};
-    cudaEvent_t ev_fft[NFFT] = {nullptr, nullptr, nullptr, nullptr};
+    void *fft_work[NFFT] = {};
+    cudaStream_t fft_stream[NFFT] = {};
+    cudaEvent_t ev_fft[NFFT] = {};
     cudaEvent_t ev_fft_fork = nullptr;
     cudaStream_t mesh_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -999,7 +999,9 @@ int pd_batch_step(pd_batch *b, int nsteps, float dt, int use_graph, pd_stream_t 
                 PD_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
                 const int rc = batch_enqueue_step(b, dt, s, cond);
                 cudaError_t err = cudaStreamEndCapture(s, &g);
-                if (rc == PD_OK && err == cudaSuccess) err = cudaGraphInstantiate(&b->exec, g, 0);
+                // node priorities kept, so the charged batches' mesh branch keeps its streams' high priority
+                if (rc == PD_OK && err == cudaSuccess)
+                    err = cudaGraphInstantiateWithFlags(&b->exec, g, cudaGraphInstantiateFlagUseNodePriority);
                 if (g) cudaGraphDestroy(g);
                 if (rc == PD_OK && err == cudaSuccess) break;
                 b->exec = nullptr;
@@ -1172,9 +1174,13 @@ static int batch_set_mesh(pd_batch *b, int kind, int order, double alpha, double
                  PD_ECUFFT, "batched mesh: plan of %d meshes %dx%dx%d failed", g.count, g.K1, g.K2, g.K3);
         wmax = std::max(wmax, std::max(w1, w2));
     }
+    // the mesh branch is the longer of the two branches of the force pass: its streams get the high
+    // priority, so its kernels' blocks are scheduled ahead of the pair kernel's
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
     for (int k = 0; k < pd_batch::NFFT; ++k) {
         PD_CUDA(cudaMalloc(&b->fft_work[k], std::max<size_t>(wmax, 256)));
-        PD_CUDA(cudaStreamCreateWithFlags(&b->fft_stream[k], cudaStreamNonBlocking));
+        PD_CUDA(cudaStreamCreateWithPriority(&b->fft_stream[k], cudaStreamNonBlocking, prio_hi));
         PD_CUDA(cudaEventCreateWithFlags(&b->ev_fft[k], cudaEventDisableTiming));
     }
     PD_CUDA(cudaEventCreateWithFlags(&b->ev_fft_fork, cudaEventDisableTiming));
@@ -1184,7 +1190,7 @@ static int batch_set_mesh(pd_batch *b, int kind, int order, double alpha, double
         PD_CHECK(cufftSetWorkArea(g.fwd, w) == CUFFT_SUCCESS && cufftSetWorkArea(g.bwd, w) == CUFFT_SUCCESS,
                  PD_ECUFFT, "batched mesh: cufftSetWorkArea failed");
     }
-    PD_CUDA(cudaStreamCreateWithFlags(&b->mesh_stream, cudaStreamNonBlocking));
+    PD_CUDA(cudaStreamCreateWithPriority(&b->mesh_stream, cudaStreamNonBlocking, prio_hi));
     PD_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
     PD_CUDA(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
     if ((rc = batch_layout_chunks(b, b->mchunk))) return rc;
