@@ -861,9 +861,8 @@ def run_batch_workload(pd, args, world, rank):
 
 def melts_sizes(nmelts: int, rank: int = 0):
     """Sizes of the batched charged melts: N log-uniform in [2 000, 32 000], even (half +1, half -1)."""
-    rng = np.random.default_rng(SEED + 64 + rank)
-    ns = [int(round(math.exp(rng.uniform(math.log(2000), math.log(32000))))) for _ in range(nmelts)]
-    return [n + (n % 2) for n in ns]
+    import __graft_entry__ as ge
+    return ge.load_package().batch.melt_sizes(nmelts, SEED + 64 + rank)
 
 
 def melts_measure(pd, ns, steps, warmup, skin, buffer, prune, world=1, compare=True, shape=None):

@@ -228,6 +228,14 @@ def make_systems(specs, mass: float = 1.0):
     return out
 
 
+def melt_sizes(nmelts: int, seed: int, n_lo: int = 2000, n_hi: int = 32000):
+    """Sizes of a set of charged melts: N log-uniform in [n_lo, n_hi], rounded to even (half +1, half -1)."""
+    import math
+    rng = np.random.default_rng(seed)
+    ns = [int(round(math.exp(rng.uniform(math.log(n_lo), math.log(n_hi))))) for _ in range(nmelts)]
+    return [n + (n % 2) for n in ns]
+
+
 def melt_systems(ns, rho: float = 0.0375, T: float = 1200.0, seed: int = 0, min_sep: float = 2.2):
     """Charged melts of the given sizes (half +1, half -1) at number density rho, seeded rejection
     placement with min_sep, Na/Cl masses, Maxwell-Boltzmann velocities at T (eV units, A/fs scaled by

@@ -34,13 +34,8 @@ def test_melt_meshes_follow_the_box(pd):
     assert meshes[0] != meshes[1]
 
 
-def test_bench_melt_sizes():
-    import importlib.util
-    from pathlib import Path
-    spec = importlib.util.spec_from_file_location("bench_mod", Path(__file__).resolve().parent.parent / "bench.py")
-    bench = importlib.util.module_from_spec(spec)
-    spec.loader.exec_module(bench)
-    ns = bench.melts_sizes(64)
+def test_melt_sizes(pd):
+    ns = pd.batch.melt_sizes(64, 2090)
     assert len(ns) == 64 and all(n % 2 == 0 for n in ns)
     assert min(ns) >= 2000 and max(ns) <= 32002
-    assert ns == bench.melts_sizes(64)
+    assert ns == pd.batch.melt_sizes(64, 2090) and ns != pd.batch.melt_sizes(64, 2091)

@@ -130,3 +130,39 @@ def test_batched_melt_errors(pd, cuda):
     systems[0]["charges"][0] += 1.0
     with pytest.raises(ValueError, match="net charge"):
         pd.batch.BatchedReplicas(systems, skin=1.0, electrostatics=dict(alpha=alpha, C=14.4, rc=RC, spacing=1.0))
+
+
+@pytest.mark.slow
+def test_the_64_melt_set_at_full_size(pd, ora, cuda):
+    """The benchmark's 64 melts (760 278 ions) as one batch: every melt's forces equal its own
+    single-system engine's (cluster list + SPME at the same mesh) within 1e-5 relative RMS, and the
+    smallest, a middle and the largest melt equal the FP64 oracle's PME sum within 1e-5."""
+    ns = pd.batch.melt_sizes(64, 2026 + 64)
+    systems = pd.batch.melt_systems(ns, seed=2026)
+    alpha = pd.splits.alpha_from_tolerance(RC, ALPHA_TOL)
+    el = dict(alpha=alpha, C=pd.synthetic.COULOMB_EV_A, rc=RC, order=5, kind="spme", spacing=1.0)
+    b = pd.batch.BatchedReplicas(systems, skin=1.2, lanes=1, electrostatics=el)
+    b.evaluate()
+    assert b.status()["error"] == 0 and b.mesh_info()["groups"] == len({tuple(m) for m in b.meshes})
+    for k, s in enumerate(systems):
+        F = np.stack([b.replica(k, t).cpu().numpy() for t in (b.fx, b.fy, b.fz)], 1).astype(float)
+        system = pd.ParticleSystem(s["positions"], s["box"], types=["Na", "Cl"],
+                                   typeids=np.where(s["charges"] > 0, 1, 2), masses=s["masses"],
+                                   charges=s["charges"], velocities=s["velocities"])
+        lj = pd.LennardJones(epsilon=0.01, sigma=2.8, cutoff=RC, pairs="neighborlist",
+                             neighborlist=pd.ClusterPairList(buffer=1.0, prune_buffer=0.3))
+        pme = pd.PME(coulomb_prefactor=pd.synthetic.COULOMB_EV_A, real_cutoff=RC, alpha=alpha, mesh=b.meshes[k],
+                     order=5)
+        sim = pd.Simulation(system, pd.Integrator(dt=1.0 / pd.synthetic.TIME_UNIT_FS, forces=[lj, pme]))
+        pd.evaluate_forces_into_f(sim)
+        Fs = sim.state.forces()
+        rel = np.linalg.norm(F - Fs) / np.linalg.norm(Fs)
+        assert rel < 1e-5, (k, s["n"], rel)
+        del sim
+    order = np.argsort(ns)
+    for k in (order[0], order[len(order) // 2], order[-1]):
+        s = systems[k]
+        pos = np.stack([b.replica(k, t).cpu().numpy() for t in (b.x, b.y, b.z)], 1).astype(float)
+        F = np.stack([b.replica(k, t).cpu().numpy() for t in (b.fx, b.fy, b.fz)], 1).astype(float)
+        ref = _oracle(pd, ora, s, b.meshes[k], alpha, pos)
+        assert np.linalg.norm(F - ref["F"]) / np.linalg.norm(ref["F"]) < 1e-5, (k, s["n"])
