@@ -893,14 +893,14 @@ def melts_measure(pd, ns, steps, warmup, skin, buffer, prune, world=1, compare=T
         batch = pd.batch.BatchedReplicas(systems, skin=skin, electrostatics=el)
         batch.evaluate()
         batch.set_lanes(tuned["lanes"])
-        batch.set_spread_tile(tuned["spread_tile"])
+        batch.set_spread_tile(*tuned["spread_tile"])
     else:   # a fixed (lanes per row, spread tile), e.g. the autotuner's earlier choice for a launch list
         skin = 1.0 if skin is None else skin
         batch = pd.batch.BatchedReplicas(systems, skin=skin, electrostatics=el)
         batch.evaluate()
         batch.set_lanes(shape[0])
-        batch.set_spread_tile(shape[1])
-        tuned = {"lanes": shape[0], "spread_tile": shape[1], "skin": skin, "fixed": True}
+        batch.set_spread_tile(*shape[1:])
+        tuned = {"lanes": shape[0], "spread_tile": list(shape[1:]), "skin": skin, "fixed": True}
     batch.step(warmup, dt)
     torch.cuda.synchronize()
     s0 = batch.stream
@@ -995,7 +995,7 @@ def run_melts_workload(pd, args, world, rank):
                   kind="spme", spacing=1.0)
         b = pd.batch.BatchedReplicas(systems, skin=1.2 if args.melt_skin is None else args.melt_skin,
                                      lanes=shape[0], electrostatics=el)
-        b.set_spread_tile(shape[1])
+        b.set_spread_tile(*shape[1:])
         b.evaluate()
         dt = DT_FS / pd.synthetic.TIME_UNIT_FS
         b.step(args.warmup, dt, use_graph=False)
@@ -1067,7 +1067,8 @@ def main():
     ap.add_argument("--melt-skin", type=float, default=None,
                     help="row-list skin of the batched melts (Angstrom); default: the autotuner's choice")
     ap.add_argument("--melt-shape", default=None,
-                    help="melts64: lanes per row x spread tile, e.g. 4x64, instead of the autotuner's choice")
+                    help="melts64: lanes per row x ions per spread tile [x threads per ion], e.g. 1x64x4, "
+                         "instead of the autotuner's choice")
     ap.add_argument("--no-compare", action="store_true",
                     help="melts64: time the batched path only (no single-system replays), e.g. for a launch list")
     ap.add_argument("--workload", default="melt64k",

@@ -557,8 +557,9 @@ int pd_batch_set_coulomb(pd_batch *b, const pd_batch_coulomb *c);
  * all replicas.  Neutral replicas only (net_charge = :error).  Host boundary: allocates. */
 int pd_batch_set_mesh(pd_batch *b, int kind, int order, double alpha, double C, const int *meshes);
 /* Spread tile of the batched meshes, the autotuner's choice: 32 or 64 particles (cell-order
- * neighbours of one replica) per spread / gather CTA.  Host boundary: may reallocate. */
-int pd_batch_set_spread_tile(pd_batch *b, int chunk);
+ * neighbours of one replica) per spread / gather CTA, with 2 threads per ion sharing its stencil's
+ * z planes, or 4 (tiles of 64).  Host boundary: may reallocate. */
+int pd_batch_set_spread_tile(pd_batch *b, int chunk, int threads_per_ion);
 /* Batched-mesh sizes: FFT plan groups (mesh sizes), grid nodes and modes of all replicas, the tile
  * size and the number of tiles. */
 int pd_batch_mesh_info(pd_batch *b, int *groups, long long *nodes, long long *modes, int *chunk, int *nchunk);

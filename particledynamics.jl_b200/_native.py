@@ -248,7 +248,7 @@ _SIGS = {
     "pd_batch_step": (C.c_int, [_p, C.c_int, C.c_float, C.c_int, _p]),
     "pd_batch_set_coulomb": (C.c_int, [_p, C.POINTER(BatchCoulomb)]),
     "pd_batch_set_mesh": (C.c_int, [_p, C.c_int, C.c_int, C.c_double, C.c_double, C.POINTER(C.c_int)]),
-    "pd_batch_set_spread_tile": (C.c_int, [_p, C.c_int]),
+    "pd_batch_set_spread_tile": (C.c_int, [_p, C.c_int, C.c_int]),
     "pd_batch_mesh_info": (C.c_int, [_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                      C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "pd_ewald_oracle": (C.c_int, [C.c_int, _fp, C.POINTER(C.c_double), C.c_double, C.c_double, C.c_double, C.c_int,

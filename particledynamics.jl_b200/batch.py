@@ -88,7 +88,7 @@ class BatchedReplicas:
         self.lanes = int(lanes)
         self.stream = torch.cuda.Stream(device=device)
         self.electrostatics = None
-        self.spread_tile = 64
+        self.spread_tile = (64, 2)
         if electrostatics is not None:
             self._set_electrostatics(electrostatics)
 
@@ -119,9 +119,10 @@ class BatchedReplicas:
         self.meshes = meshes
         self.electrostatics = dict(el, order=order, meshes=meshes)
 
-    def set_spread_tile(self, tile: int):
-        N.call("pd_batch_set_spread_tile", self.handle, int(tile))
-        self.spread_tile = int(tile)
+    def set_spread_tile(self, tile: int, threads_per_ion: int = 2):
+        """Ions per spread / gather CTA (32 or 64) and threads per ion (2, or 4 with 64)."""
+        N.call("pd_batch_set_spread_tile", self.handle, int(tile), int(threads_per_ion))
+        self.spread_tile = (int(tile), int(threads_per_ion))
 
     def mesh_info(self) -> dict:
         g, ch, nc = C.c_int(), C.c_int(), C.c_int()
@@ -184,10 +185,10 @@ class BatchedReplicas:
         return {"lanes": best, "ms": times}
 
 
-    def autotune(self, dt: float, lanes=(1, 2, 4, 8), tiles=(32, 64), steps: int = 10) -> dict:
+    def autotune(self, dt: float, lanes=(1, 2, 4, 8), tiles=((32, 2), (64, 2), (64, 4)), steps: int = 10) -> dict:
         """Time the captured step for every (lanes per row, spread tile) pair on this batch and keep the
-        fastest (the step's pair pass and mesh branch overlap, so whole steps are timed).  The state is
-        restored afterwards."""
+        fastest (the step's pair pass and mesh branch overlap, so whole steps are timed); a spread tile is
+        (ions per CTA, threads per ion).  The state is restored afterwards."""
         saved = [t.clone() for t in (self.x, self.y, self.z, self.vx, self.vy, self.vz, self.fx, self.fy, self.fz)]
         s = self.stream
         times = {}
@@ -195,7 +196,7 @@ class BatchedReplicas:
             for tile in (tiles if self.electrostatics is not None else (self.spread_tile,)):
                 self.set_lanes(g)
                 if self.electrostatics is not None:
-                    self.set_spread_tile(tile)
+                    self.set_spread_tile(*tile)
                 self.step(2, dt)
                 a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 with torch.cuda.stream(s):
@@ -207,13 +208,15 @@ class BatchedReplicas:
         best = min(times, key=times.get)
         self.set_lanes(best[0])
         if self.electrostatics is not None:
-            self.set_spread_tile(best[1])
+            self.set_spread_tile(*best[1])
         torch.cuda.synchronize()
         for t, v in zip((self.x, self.y, self.z, self.vx, self.vy, self.vz, self.fx, self.fy, self.fz), saved):
             t.copy_(v)
         torch.cuda.synchronize()
         self.evaluate()
-        return {"lanes": best[0], "spread_tile": best[1], "ms": {f"{k[0]}x{k[1]}": v for k, v in times.items()}}
+        tag = lambda k: f"lanes {k[0]}, tile {k[1][0]}x{k[1][1]}" if isinstance(k[1], tuple) else f"lanes {k[0]}"
+        return {"lanes": best[0], "spread_tile": list(best[1]) if isinstance(best[1], tuple) else best[1],
+                "ms": {tag(k): v for k, v in times.items()}}
 
 
 def make_systems(specs, mass: float = 1.0):

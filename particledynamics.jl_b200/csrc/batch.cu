@@ -519,7 +519,7 @@ struct pd_batch {
     int coul_ne = 0, coul_nf = 0;
     float half_c_self = 0.f;
     bool mesh = false;
-    int morder = 5, mchunk = 64, nchunk = 0;
+    int morder = 5, mchunk = 64, nchunk = 0, mtpi = 2;
     std::vector<BMeshRep> hmreps;
     BMeshRep *mreps = nullptr;
     int *chunk_rep = nullptr, *slot_src = nullptr, *mid = nullptr;
@@ -663,6 +663,7 @@ static BMeshView batch_mesh_view(const pd_batch *b) {
     BMeshView v;
     v.order = b->morder;
     v.chunk = b->mchunk;
+    v.tpi = b->mtpi;
     v.nchunk = b->nchunk;
     v.nrep = b->nrep;
     v.reps = b->mreps;
@@ -987,7 +988,7 @@ int pd_batch_step(pd_batch *b, int nsteps, float dt, int use_graph, pd_stream_t 
             continue;
         }
         if (!b->exec || b->exec_dt != dt || b->exec_stream != s || b->exec_lanes != b->lanes ||
-            b->exec_chunk != b->mchunk) {
+            b->exec_chunk != b->mchunk * 8 + b->mtpi) {
             if (b->exec) {
                 cudaGraphExecDestroy(b->exec);
                 b->exec = nullptr;
@@ -1015,7 +1016,7 @@ int pd_batch_step(pd_batch *b, int nsteps, float dt, int use_graph, pd_stream_t 
             b->exec_dt = dt;
             b->exec_stream = s;
             b->exec_lanes = b->lanes;
-            b->exec_chunk = b->mchunk;
+            b->exec_chunk = b->mchunk * 8 + b->mtpi;
         }
         PD_CUDA(cudaGraphLaunch(b->exec, s));
     }
@@ -1220,9 +1221,12 @@ int pd_batch_set_mesh(pd_batch *b, int kind, int order, double alpha, double C, 
     return rc;
 }
 
-int pd_batch_set_spread_tile(pd_batch *b, int chunk) {
+int pd_batch_set_spread_tile(pd_batch *b, int chunk, int threads_per_ion) {
     PD_CHECK(b, PD_EINVAL, "pd_batch_set_spread_tile: null handle");
     PD_CHECK(chunk == 32 || chunk == 64, PD_EINVAL, "pd_batch_set_spread_tile: 32 or 64 particles per tile");
+    PD_CHECK(threads_per_ion == 2 || (threads_per_ion == 4 && chunk == 64), PD_EINVAL,
+             "pd_batch_set_spread_tile: 2 threads per ion, or 4 with tiles of 64");
+    b->mtpi = threads_per_ion;
     if (!b->mesh) {
         b->mchunk = chunk;
         return PD_OK;

@@ -8,8 +8,8 @@
 // cell, replica by replica), cut into chunks of `chunk` consecutive positions of one replica; a
 // chunk of cell-sorted particles lies in about two cells, so its B-spline stencils cover a small
 // brick that the spread accumulates in shared memory (32-bit fixed point, as the single-system
-// spread) and the gather stages before every particle reads its P^3 nodes.  The chunk size (32 or
-// 64 particles, 64 or 128 threads) is the autotuner's spread tile.  The transforms of the mesh sizes
+// spread) and the gather stages before every particle reads its P^3 nodes.  The tile (32 or 64
+// particles, with 2 or 4 threads per particle sharing its z planes) is the autotuner's spread tile.  The transforms of the mesh sizes
 // run on several streams at once (each size's batched plan is small; one after another they would
 // leave most of the GPU idle).
 //
@@ -49,8 +49,8 @@ __global__ void k_bmesh_pack(const float *__restrict__ x, const float *__restric
     mid[s] = i;
 }
 
-template <int P, int CH>
-__global__ void __launch_bounds__(2 * CH, BMESH_CTAS_PER_SM) k_bspread(const float4 *__restrict__ mq,
+template <int P, int CH, int TP>
+__global__ void __launch_bounds__(TP * CH, BMESH_CTAS_PER_SM) k_bspread(const float4 *__restrict__ mq,
                                                                       const int *__restrict__ chunk_rep,
                                                                       const BMeshRep *__restrict__ reps,
                                                                       float *__restrict__ gridA,
@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(2 * CH, BMESH_CTAS_PER_SM) k_bspread(const flo
     if (st[E_VALID] == 0) return;
     const int c = blockIdx.x;
     const BMeshRep R = reps[chunk_rep[c]];
-    spread_chunk<P, WIN_BSPLINE, CH, BTILE>(mq + (size_t)c * CH, gridA + R.grid, R.K1, R.K2, R.K3, R.Lx, R.Ly, R.Lz,
+    spread_chunk<P, WIN_BSPLINE, CH, BTILE, TP>(mq + (size_t)c * CH, gridA + R.grid, R.K1, R.K2, R.K3, R.Lx, R.Ly, R.Lz,
                                      WindowPoly{nullptr, 0});
 }
 
@@ -85,9 +85,10 @@ __global__ void __launch_bounds__(256) k_bsolve(float2 *__restrict__ spec, const
 
 // AD gather of one chunk (the sums of _gather_ad_lines_sums, MeshKernels.jl:281-311, and
 // _gather_ad_lines_kernel!, :313-333) from the replica's potential grid, joined with the pair force
-// already stored for the particle: F = F_pair - q grad(phi) K / L, then the closing half kick.
-template <int P, int CH, bool ENERGY>
-__global__ void __launch_bounds__(2 * CH, BMESH_CTAS_PER_SM) k_bgather(const float4 *__restrict__ mq,
+// already stored for the particle: F = F_pair - q grad(phi) K / L, then the closing half kick.  Each
+// particle's TP threads share the z planes of its stencil.
+template <int P, int CH, int TP, bool ENERGY>
+__global__ void __launch_bounds__(TP * CH, BMESH_CTAS_PER_SM) k_bgather(const float4 *__restrict__ mq,
                                                                       const int *__restrict__ mid,
                                                                       const int *__restrict__ chunk_rep,
                                                                       const BMeshRep *__restrict__ reps,
@@ -98,7 +99,7 @@ __global__ void __launch_bounds__(2 * CH, BMESH_CTAS_PER_SM) k_bgather(const flo
                                                                       float half_c_self,
                                                                       const long long *__restrict__ st) {
     if (st[E_VALID] == 0) return;
-    constexpr int NT = 2 * CH;
+    constexpr int NT = TP * CH;
     const int c = blockIdx.x;
     const BMeshRep R = reps[chunk_rep[c]];
     const float *grid = gridB + R.grid;
@@ -106,7 +107,6 @@ __global__ void __launch_bounds__(2 * CH, BMESH_CTAS_PER_SM) k_bgather(const flo
     __shared__ __align__(16) float tile[BTILE];
     __shared__ unsigned rowbase[ROWS_MAX];
     __shared__ int sm[10];
-    __shared__ float part[CH][4];
     const int t = threadIdx.x, p = t & (CH - 1), h = t / CH;
     const int e = c * CH + p;
     const float4 v = mq[e];
@@ -136,7 +136,6 @@ __global__ void __launch_bounds__(2 * CH, BMESH_CTAS_PER_SM) k_bgather(const flo
     int d1 = 0, d2 = 0, d3 = 0;
     Brick b;
     chunk_brick<P, NT, BTILE>(charged, k1, k2, k3, K1, K2, K3, d1, d2, d3, b, sm, rowbase);
-    constexpr int PH = (P + 1) / 2;
     float phi = 0.f, gx = 0.f, gy = 0.f, gz = 0.f;
     if (b.fits) {
         if (b.vec) {
@@ -150,8 +149,8 @@ __global__ void __launch_bounds__(2 * CH, BMESH_CTAS_PER_SM) k_bgather(const flo
         __syncthreads();
         if (charged) {
 #pragma unroll
-            for (int j3 = 0; j3 < P; ++j3) {   // this half's z nodes only (warp-uniform test)
-                if ((j3 < PH) != (h == 0)) continue;
+            for (int j3 = 0; j3 < P; ++j3) {   // this thread's z planes only (warp-uniform test)
+                if (!my_plane<P, TP>(j3, h)) continue;
                 float s0 = 0.f, s1 = 0.f, s2 = 0.f;
 #pragma unroll
                 for (int j2 = 0; j2 < P; ++j2) {
@@ -176,7 +175,7 @@ __global__ void __launch_bounds__(2 * CH, BMESH_CTAS_PER_SM) k_bgather(const flo
     } else if (charged) {
 #pragma unroll
         for (int j3 = 0; j3 < P; ++j3) {
-            if ((j3 < PH) != (h == 0)) continue;
+            if (!my_plane<P, TP>(j3, h)) continue;
             const int n3 = wrap_node(k3 + j3, K3);
             float s0 = 0.f, s1 = 0.f, s2 = 0.f;
 #pragma unroll
@@ -199,18 +198,20 @@ __global__ void __launch_bounds__(2 * CH, BMESH_CTAS_PER_SM) k_bgather(const flo
             gy = fmaf(w3[j3], s2, gy);
         }
     }
-    if (h == 1) {
-        part[p][0] = phi;
-        part[p][1] = gx;
-        part[p][2] = gy;
-        part[p][3] = gz;
-    }
+    // the partial sums of threads h > 0 meet in the brick's shared memory once every thread is done with it
     __syncthreads();
-    if (h == 1 || id < 0) return;
-    phi += part[p][0];
-    gx += part[p][1];
-    gy += part[p][2];
-    gz += part[p][3];
+    float4 *part = reinterpret_cast<float4 *>(tile);   // (TP - 1) x CH, far below the brick's size
+    if (h > 0) part[(h - 1) * CH + p] = make_float4(phi, gx, gy, gz);
+    __syncthreads();
+    if (h > 0 || id < 0) return;
+#pragma unroll
+    for (int k = 0; k < TP - 1; ++k) {
+        const float4 o = part[k * CH + p];
+        phi += o.x;
+        gx += o.y;
+        gy += o.z;
+        gz += o.w;
+    }
     const float qi = v.w;
     float Fx = fpx, Fy = fpy, Fz = fpz;
     if (charged) {
@@ -241,9 +242,11 @@ int bmesh_pack_launch(const BMeshView &v, const float *x, const float *y, const 
 template <int P>
 static void spread_p(const BMeshView &v, const long long *st, cudaStream_t s) {
     if (v.chunk == 32)
-        k_bspread<P, 32><<<v.nchunk, 64, 0, s>>>(v.mq, v.chunk_rep, v.reps, v.gridA, st);
+        k_bspread<P, 32, 2><<<v.nchunk, 64, 0, s>>>(v.mq, v.chunk_rep, v.reps, v.gridA, st);
+    else if (v.tpi == 4)
+        k_bspread<P, 64, 4><<<v.nchunk, 256, 0, s>>>(v.mq, v.chunk_rep, v.reps, v.gridA, st);
     else
-        k_bspread<P, 64><<<v.nchunk, 128, 0, s>>>(v.mq, v.chunk_rep, v.reps, v.gridA, st);
+        k_bspread<P, 64, 2><<<v.nchunk, 128, 0, s>>>(v.mq, v.chunk_rep, v.reps, v.gridA, st);
 }
 
 int bmesh_spread_launch(const BMeshView &v, const long long *st, cudaStream_t s) {
@@ -265,24 +268,26 @@ int bmesh_solve_launch(const BMeshView &v, const long long *st, cudaStream_t s) 
     return PD_OK;
 }
 
-template <int P, int CH>
+template <int P, int CH, int TP>
 static void gather_pc(const BMeshView &v, float *fx, float *fy, float *fz, float *epot, int energy,
                       const BMeshKick &kick, float half_c_self, const long long *st, cudaStream_t s) {
     if (energy)
-        k_bgather<P, CH, true><<<v.nchunk, 2 * CH, 0, s>>>(v.mq, v.mid, v.chunk_rep, v.reps, v.gridB, fx, fy, fz, epot,
-                                                           kick, half_c_self, st);
+        k_bgather<P, CH, TP, true><<<v.nchunk, TP * CH, 0, s>>>(v.mq, v.mid, v.chunk_rep, v.reps, v.gridB, fx, fy,
+                                                                fz, epot, kick, half_c_self, st);
     else
-        k_bgather<P, CH, false><<<v.nchunk, 2 * CH, 0, s>>>(v.mq, v.mid, v.chunk_rep, v.reps, v.gridB, fx, fy, fz,
-                                                            epot, kick, half_c_self, st);
+        k_bgather<P, CH, TP, false><<<v.nchunk, TP * CH, 0, s>>>(v.mq, v.mid, v.chunk_rep, v.reps, v.gridB, fx, fy,
+                                                                 fz, epot, kick, half_c_self, st);
 }
 
 template <int P>
 static void gather_p(const BMeshView &v, float *fx, float *fy, float *fz, float *epot, int energy,
                      const BMeshKick &kick, float half_c_self, const long long *st, cudaStream_t s) {
     if (v.chunk == 32)
-        gather_pc<P, 32>(v, fx, fy, fz, epot, energy, kick, half_c_self, st, s);
+        gather_pc<P, 32, 2>(v, fx, fy, fz, epot, energy, kick, half_c_self, st, s);
+    else if (v.tpi == 4)
+        gather_pc<P, 64, 4>(v, fx, fy, fz, epot, energy, kick, half_c_self, st, s);
     else
-        gather_pc<P, 64>(v, fx, fy, fz, epot, energy, kick, half_c_self, st, s);
+        gather_pc<P, 64, 2>(v, fx, fy, fz, epot, energy, kick, half_c_self, st, s);
 }
 
 int bmesh_gather_launch(const BMeshView &v, float *fx, float *fy, float *fz, float *epot, int energy,

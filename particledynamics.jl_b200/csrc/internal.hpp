@@ -243,6 +243,7 @@ struct BMeshRep {
 // consecutive cell-order positions of one replica (padded slots: slot_src = -1).
 struct BMeshView {
     int order, chunk, nchunk, nrep;
+    int tpi;                     // threads per particle of the spread and gather CTAs (2 or 4)
     const BMeshRep *reps;
     const int *chunk_rep;        // nchunk
     const int *slot_src;         // nchunk * chunk: cell-order position or -1

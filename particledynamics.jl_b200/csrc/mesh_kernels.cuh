@@ -252,13 +252,20 @@ __device__ __forceinline__ void for_brick(const Brick &b, const unsigned *rowbas
     for (int r = r0; r < nrows; r += rpi) visit(r * nv + v, (size_t)rowbase[r] + x0);
 }
 
+// z planes of a particle's stencil taken by its thread h of TP: the two halves of the stencil (TP = 2),
+// or every TP-th plane (TP = 4).
+template <int P, int TP>
+__device__ __forceinline__ bool my_plane(int j3, int h) {
+    return TP == 2 ? ((j3 < (P + 1) / 2) == (h == 0)) : (j3 % TP == h);
+}
+
 // Spread of one chunk of CH packed (x, y, z, q) particles into `grid` (the charge assignment of
-// _spread_lines_kernel!, MeshKernels.jl:247-276), by a CTA of 2 CH threads: each particle's two
-// threads take the two halves of its z stencil.
-template <int P, int WIN, int CH, int TILE = TILE_MAX>
+// _spread_lines_kernel!, MeshKernels.jl:247-276), by a CTA of TP CH threads: each particle's TP
+// threads share the z planes of its stencil.
+template <int P, int WIN, int CH, int TILE = TILE_MAX, int TP = 2>
 __device__ __forceinline__ void spread_chunk(const float4 *__restrict__ chunk, float *__restrict__ grid, int K1,
                                              int K2, int K3, float Lx, float Ly, float Lz, const WindowPoly &wp) {
-    constexpr int NT = 2 * CH;
+    constexpr int NT = TP * CH;
     __shared__ __align__(16) float tile[TILE];
     __shared__ unsigned rowbase[ROWS_MAX];
     __shared__ int sm[10];
@@ -276,7 +283,6 @@ __device__ __forceinline__ void spread_chunk(const float4 *__restrict__ chunk, f
     Brick b;
     // both halves of a particle take part (their min/max contributions are identical)
     chunk_brick<P, NT, TILE>(valid, k1, k2, k3, K1, K2, K3, d1, d2, d3, b, sm, rowbase);
-    constexpr int PH = (P + 1) / 2;
 
     if (b.fits) {
         // The brick accumulates in 32-bit fixed point: integer shared-memory reductions are native
@@ -304,7 +310,7 @@ __device__ __forceinline__ void spread_chunk(const float4 *__restrict__ chunk, f
             const float qs = v.w * scale;
 #pragma unroll
             for (int j3 = 0; j3 < P; ++j3) {   // this half's z nodes only (warp-uniform test)
-            if ((j3 < PH) != (h == 0)) continue;
+            if (!my_plane<P, TP>(j3, h)) continue;
                 const float q3 = qs * w3[j3];
 #pragma unroll
                 for (int j2 = 0; j2 < P; ++j2) {
@@ -332,7 +338,7 @@ __device__ __forceinline__ void spread_chunk(const float4 *__restrict__ chunk, f
     } else if (valid) {
 #pragma unroll
         for (int j3 = 0; j3 < P; ++j3) {   // this half's z nodes only (warp-uniform test)
-            if ((j3 < PH) != (h == 0)) continue;
+            if (!my_plane<P, TP>(j3, h)) continue;
             const int n3 = wrap_node(k3 + j3, K3);
             const float q3 = v.w * w3[j3];
 #pragma unroll

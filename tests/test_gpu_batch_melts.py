@@ -50,9 +50,9 @@ def test_batched_melts_match_the_oracle(pd, ora, cuda, kind):
 def test_spread_tiles_and_lanes_agree(pd, cuda):
     b, systems, _ = _batch(pd, [800, 1700, 2500], seed=9)
     results = []
-    for lanes, tile in ((1, 32), (4, 64), (8, 32), (2, 64)):
+    for lanes, tile in ((1, (32, 2)), (4, (64, 2)), (8, (32, 2)), (2, (64, 4)), (1, (64, 4))):
         b.set_lanes(lanes)
-        b.set_spread_tile(tile)
+        b.set_spread_tile(*tile)
         b.evaluate(energy=True)
         results.append((np.stack([t.cpu().numpy() for t in (b.fx, b.fy, b.fz)], 1), b.epot.double().sum().item()))
     F0, E0 = results[0]
@@ -126,6 +126,8 @@ def test_batched_melt_errors(pd, cuda):
         pd._native.call("pd_batch_set_mesh", b.handle, 1, 5, alpha, 14.4, arr)
     with pytest.raises(pd._native.NativeError, match="32 or 64"):
         b.set_spread_tile(48)
+    with pytest.raises(pd._native.NativeError, match="4 with tiles of 64"):
+        b.set_spread_tile(32, 4)
     systems[0]["charges"] = systems[0]["charges"].copy()
     systems[0]["charges"][0] += 1.0
     with pytest.raises(ValueError, match="net charge"):
